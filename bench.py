@@ -1,0 +1,363 @@
+"""Benchmark of the match_template search on B200.
+
+Workload (the reference's metric configuration that fits one GPU): a
+4096 x 4096 micrograph (80 Gaussian-atom particles, SNR 0.03, defocus
+12,000 A, 300 kV, Cs 2.7 mm, A 0.07) searched with a 256^3 template at
+1.0 A/px (120,000 atoms, 110 A radius) on the C1 grid of 2.5 deg
+out-of-plane / 1.5 deg in-plane steps (1,595,420 orientations).  All inputs
+are seeded synthetic data.  A step is one tm_run_plane call over a contiguous
+chunk of that grid (successive steps take successive chunks).
+
+metric: search points/s = original micrograph pixels x orientations / time.
+value : device time (CUDA events on the library's stream) of K steps with
+        prepared inputs resident in HBM.
+e2e   : the same steps through the C ABI with host buffers: per step the
+        prepared spectra and filter are copied host->device (pinned memory),
+        the plane is searched, and MIP / best angles / sums / histogram are
+        copied device->host and decoded; timed by the host clock.
+
+--impl reference times the reference CPU algorithm (the FP32 build of the
+oracle's restatement, all host threads) on a bounded sample of the same
+workload; the reference itself cannot be built here (it needs wxWidgets and
+FFTW).  With --gpus N > 1 every rank runs an independent replica (the search
+has no data-path exchange on one micrograph) and the job value is the sum
+over ranks, timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "search points/s (original micrograph pixels x orientations)"
+UNIT = "points/s"
+
+WORKLOAD = dict(name="4096x4096 micrograph, 256^3 template @1.0 A/px, C1 2.5/1.5 deg grid",
+                nx=4096, ny=4096, T=256, pixel_size=1.0, n_atoms=120000, radius_A=110.0, particles=80,
+                snr=0.03, defocus=12000.0, angular_step=2.5, psi_step=1.5)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_inputs(seed=20261204):
+    """Synthetic micrograph and template, prepared as the reference's
+    DoCalculation prepares them (whitening, template spectrum, CTF filter)."""
+    from cistem_downstream_bah_b200 import prep, synthetic
+    w = WORKLOAD
+    vol = synthetic.template_volume(w["T"], w["pixel_size"], w["n_atoms"], w["radius_A"], seed=seed)
+    mic, _ = synthetic.micrograph(w["ny"], w["nx"], w["pixel_size"], w["n_atoms"], w["radius_A"], w["particles"],
+                                  w["snr"], w["defocus"], seed=seed + 1, atom_seed=seed)
+    X = prep.factorize_dimension(w["nx"], w["T"])
+    Y = prep.factorize_dimension(w["ny"], w["T"])
+    assert (X, Y) == (w["nx"], w["ny"])
+    ispec, curve = prep.whiten(mic)
+    tspec = prep.template_spectrum(vol)
+    filt = prep.projection_filter(w["T"], curve, kv=300.0, cs_mm=2.7, amplitude_contrast=0.07,
+                                  defocus1=w["defocus"], defocus2=w["defocus"], pixel_size=w["pixel_size"])
+    grid = prep.search_grid(w["angular_step"])
+    from cistem_downstream_bah_b200.core import orientation_list
+    angles = orientation_list(grid, 0.0, w["psi_step"], 360.0)
+    hmin, hstep = prep.histogram_scaled(X, Y)
+    return dict(X=X, Y=Y, T=w["T"], ispec=ispec, tspec=tspec, filt=filt, angles=angles, hmin=hmin, hstep=hstep)
+
+
+def pinned_copy(a):
+    """numpy array in page-locked host memory (torch is used only as the allocator)."""
+    import torch
+    t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+    out = t.numpy().view(a.dtype).reshape(a.shape)
+    out[...] = a
+    out._keepalive = t  # noqa: SLF001
+    return out
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def max_over_ranks(world, v):
+    if world <= 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_ours(args):
+    world, rank, local = dist_init(args)
+    from cistem_downstream_bah_b200 import core
+    inp = make_inputs()
+    X, Y, T = inp["X"], inp["Y"], inp["T"]
+    per_step = args.orientations_per_step
+    n_orient_total = len(inp["angles"])
+    npix_orig = WORKLOAD["nx"] * WORKLOAD["ny"]
+    sc = core.SearchCore(X, Y, T, histogram_min_scaled=inp["hmin"], histogram_step_scaled=inp["hstep"],
+                         orientation_batch=args.batch, device=local)
+    sc.set_template(inp["tspec"])
+    sc.set_image(inp["ispec"])
+
+    def chunk(i):
+        a = (i * per_step) % n_orient_total
+        return inp["angles"][a:a + per_step]
+
+    # ---- device-resident timing
+    for i in range(args.warmup):
+        sc.run_plane(inp["filt"], chunk(i))
+    barrier(world)
+    dev_ms = 0.0
+    b_ms = c_ms = prep_ms = 0.0
+    n_done = 0
+    t_wall0 = time.perf_counter()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            ang = chunk(args.warmup + i)
+            sc.run_plane(inp["filt"], ang)
+            t = sc.last_timing()
+            dev_ms += t["total_ms"]
+            b_ms += t["pass_b_ms"]
+            c_ms += t["pass_c_ms"]
+            prep_ms += t["prep_ms"]
+            n_done += len(ang)
+    barrier(world)
+    wall_ms = (time.perf_counter() - t_wall0) * 1e3
+    dev_ms_max = max_over_ranks(world, dev_ms)
+    value = world * npix_orig * n_done / (dev_ms_max * 1e-3)
+
+    # ---- end to end through the C ABI with pinned host buffers
+    ispec_h, tspec_h, filt_h = pinned_copy(inp["ispec"]), pinned_copy(inp["tspec"]), pinned_copy(inp["filt"])
+    n = X * Y
+    outs = {k: pinned_copy(np.zeros(n, np.float32)) for k in ("mip", "psi", "theta", "phi", "defocus", "pixel")}
+    sum_h, sq_h = pinned_copy(np.zeros(n, np.float64)), pinned_copy(np.zeros(n, np.float64))
+    hist_h = np.zeros(512, np.int64)
+    L = sc.L
+    ptr = core._ptr
+    barrier(world)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        ang = chunk(args.warmup + i)
+        sc._check(L.tm_set_image(sc.h, ptr(ispec_h), X, Y))
+        sc._check(L.tm_set_template(sc.h, ptr(tspec_h), T))
+        sc.reset()
+        sc.run_plane(filt_h, ang)
+        sc._check(L.tm_get_results(sc.h, ptr(outs["mip"]), ptr(outs["psi"]), ptr(outs["theta"]), ptr(outs["phi"]),
+                                   ptr(outs["defocus"]), ptr(outs["pixel"]), ptr(sum_h), ptr(sq_h), ptr(hist_h)))
+    barrier(world)
+    e2e_s = max_over_ranks(world, time.perf_counter() - t0)
+    e2e = world * npix_orig * n_done / e2e_s
+    h2d = ispec_h.nbytes + tspec_h.nbytes + filt_h.nbytes + per_step * 12
+    d2h = n * 4 + n * 4 + 2 * n * 8 + 512 * 8   # mip, best index, sum, sum of squares, histogram
+
+    # ---- roofline for the dominant kernel (per launch = one orientation batch)
+    hbm_peak, peak_kind = peaks()
+    N = X * Y
+    nb = sc_batch = (args.batch or 32)
+    n_launch = n_done / nb
+    b_launch_ms = b_ms / max(n_launch, 1)
+    c_launch_ms = c_ms / max(n_launch, 1)
+    # algorithmic bytes per point: pass B reads the half spectrum (4 B) and
+    # writes the intermediate (4 B); pass C reads the intermediate (4 B)
+    dominant = "k_pass_b" if b_ms >= c_ms else "k_pass_c"
+    alg_b = 8.0 * N * nb
+    alg_c = 4.0 * N * nb
+    if dominant == "k_pass_b":
+        ach = alg_b / (b_launch_ms * 1e-3) / 1e9
+        traffic = args.traffic_b
+    else:
+        ach = alg_c / (c_launch_ms * 1e-3) / 1e9
+        traffic = args.traffic_c
+
+    cpu = cpu_baseline(inp, sample=args.cpu_sample) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
+    sc.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD["name"], "micrograph": [WORKLOAD["nx"], WORKLOAD["ny"]],
+                       "padded": [X, Y], "template": T, "orientations_per_step": per_step,
+                       "grid_orientations": n_orient_total, "orientation_batch": nb,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2: each batch writes a %.1f GB intermediate" % (nb * Y * (X // 2 + 4) * 8 / 1e9)},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(6 * np.ceil(per_step / nb) * args.steps),
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": ach / hbm_peak, "traffic": traffic, "peak_source": peak_kind,
+                         "ms_per_launch": {"k_pass_b": b_launch_ms, "k_pass_c": c_launch_ms,
+                                           "prep_kernels": prep_ms / max(n_launch, 1)}},
+            "clocks": clk.summary(),
+            "wall_ms_timed_region": wall_ms,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def _oracle_sample(inp, n_orient, bits=32):
+    from oracle import oracle as O
+    st = O.SearchState(inp["X"], inp["Y"])
+    ang = inp["angles"][:n_orient]
+    t0 = time.perf_counter()
+    O.search(st, inp["tspec"].astype(np.complex64 if bits == 32 else np.complex128), inp["ispec"], inp["filt"], ang,
+             hist_min_scaled=inp["hmin"], hist_step_scaled=inp["hstep"], bits=bits)
+    return time.perf_counter() - t0
+
+
+def _cpu_threads():
+    """Host threads for the CPU legs (each thread holds ~0.6 GB of 4096^2 buffers)."""
+    threads = min(os.cpu_count() or 1, 32)
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    return int(os.environ["OMP_NUM_THREADS"])
+
+
+def cpu_baseline(inp, sample=None):
+    threads = _cpu_threads()
+    n = sample or max(threads, 8)
+    secs = _oracle_sample(inp, n)
+    pts = WORKLOAD["nx"] * WORKLOAD["ny"] * n / secs
+    return {"value": pts, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {n} orientations of the grid on the full 4096^2 micrograph, FP32 oracle build, "
+                      f"{threads} OpenMP threads, {secs:.1f} s"}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    inp = make_inputs()
+    threads = _cpu_threads()
+    n = args.cpu_sample or max(threads, 8)
+    for _ in range(args.warmup):
+        _oracle_sample(inp, min(n, threads))
+    total = 0.0
+    for _ in range(args.steps):
+        total += _oracle_sample(inp, n)
+    pts = WORKLOAD["nx"] * WORKLOAD["ny"] * n * args.steps / total
+    line = {"impl": "reference", "metric": METRIC, "value": pts, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD["name"], "orientations_per_step": n},
+            "cpu_baseline": {"value": pts, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{n} orientations per step on the full micrograph, FP32 oracle build "
+                                       "(reference CPU algorithm restated; the reference needs wxWidgets/FFTW)"},
+            "e2e": {"value": pts, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--orientations-per-step", type=int, default=1024)
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--cpu-sample", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--traffic-b", type=float, default=None, help="ncu DRAM bytes per pass-B launch")
+    ap.add_argument("--traffic-c", type=float, default=None, help="ncu DRAM bytes per pass-C launch")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("note: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,61 @@
+"""Build recipe for the native libraries (in-tree, sm_100a).
+
+``build()`` compiles ``lib/libtm_b200.so`` (the CUDA search core behind the C
+ABI in include/tm_b200.h).  nvcc cross-compiles without a GPU, so this runs on
+any machine with CUDA 12.9.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+LIB_DIR = os.path.join(PKG, "lib")
+CSRC = os.path.join(PKG, "csrc")
+CORE_LIB = os.path.join(LIB_DIR, "libtm_b200.so")
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17", "--extended-lambda",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+    "-shared",
+]
+
+
+def _nvcc():
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return "nvcc"
+
+
+def _sources():
+    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))] + [os.path.join(ROOT, "include", "tm_b200.h")]
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build_core(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(LIB_DIR, exist_ok=True)
+    if force or _stale(CORE_LIB, _sources()):
+        cmd = [_nvcc(), *NVCC_FLAGS, "-o", CORE_LIB, os.path.join(CSRC, "tm_capi.cu")]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+    return CORE_LIB
+
+
+def build(force: bool = False, verbose: bool = False) -> None:
+    build_core(force=force, verbose=verbose)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)

@@ -1,0 +1,234 @@
+"""ctypes bindings of the search core's C ABI (include/tm_b200.h).
+
+``SearchCore`` is a thin object over one ``tm_ctx``; ``TemplateMatchingCore``
+mirrors the reference class of the same name (src/gpu/TemplateMatchingCore.h:
+55-179): ``Init`` takes the prepared template and micrograph spectra and the
+search ranges, ``RunInnerLoop`` runs one (pixel size, defocus) plane over the
+orientation range ``[first_search_position, last_search_position]`` x psi, and
+the results are read back like the reference's device images.
+
+The library must exist and load: there is no fallback.  Building it needs only
+nvcc (``python -m cistem_downstream_bah_b200.build``); running it needs a GPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+TM_OK = 0
+TM_ERR_INVALID = -1
+TM_ERR_CUDA = -2
+TM_ERR_UNSUPPORTED = -3
+TM_ERR_OOM = -4
+TM_ERR_TIMEOUT = -5
+TM_ERR_CANCELLED = -6
+
+EXPORTED = [
+    "tm_create", "tm_set_template", "tm_set_image", "tm_reset_results", "tm_run_plane",
+    "tm_get_results", "tm_correlations_computed", "tm_last_timing", "tm_destroy", "tm_last_error", "tm_version",
+]
+
+
+class TmDims(ctypes.Structure):
+    _fields_ = [
+        ("image_x", ctypes.c_int), ("image_y", ctypes.c_int), ("template_size", ctypes.c_int),
+        ("histogram_bins", ctypes.c_int),
+        ("histogram_min_scaled", ctypes.c_double), ("histogram_step_scaled", ctypes.c_double),
+        ("orientation_batch", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
+PROGRESS_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_void_p)
+
+_LIB = None
+
+
+class TmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"tm error {code}: {msg}")
+        self.code = code
+
+
+def library_path() -> str:
+    return _build.CORE_LIB
+
+
+def load(build_if_missing: bool = True) -> ctypes.CDLL:
+    """Loads libtm_b200.so (building it first when missing)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not os.path.exists(path):
+        if not build_if_missing:
+            raise OSError(f"{path} is missing; run python -m cistem_downstream_bah_b200.build")
+        _build.build_core()
+    L = ctypes.CDLL(path)
+    vp, ip, fp = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    L.tm_create.argtypes = [ctypes.POINTER(TmDims), ctypes.POINTER(vp)]
+    L.tm_set_template.argtypes = [vp, vp, ip]
+    L.tm_set_image.argtypes = [vp, vp, ip, ip]
+    L.tm_reset_results.argtypes = [vp]
+    L.tm_run_plane.argtypes = [vp, vp, vp, ip, fp, fp, PROGRESS_FN, vp]
+    L.tm_get_results.argtypes = [vp] + [vp] * 9
+    L.tm_correlations_computed.argtypes = [vp]
+    L.tm_correlations_computed.restype = ctypes.c_longlong
+    L.tm_last_timing.argtypes = [vp] + [ctypes.POINTER(ctypes.c_double)] * 4
+    L.tm_destroy.argtypes = [vp]
+    L.tm_last_error.argtypes = [vp]
+    L.tm_last_error.restype = ctypes.c_char_p
+    L.tm_version.restype = ctypes.c_char_p
+    _LIB = L
+    return L
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+class SearchCore:
+    """One search context on one GPU (tm_create ... tm_destroy)."""
+
+    def __init__(self, image_x, image_y, template_size, *, histogram_min_scaled, histogram_step_scaled,
+                 histogram_bins=512, orientation_batch=0, device=0):
+        self.L = load()
+        self.X, self.Y, self.T = image_x, image_y, template_size
+        self.hist_bins = histogram_bins
+        d = TmDims(image_x, image_y, template_size, histogram_bins, histogram_min_scaled, histogram_step_scaled,
+                   orientation_batch, device)
+        h = ctypes.c_void_p()
+        rc = self.L.tm_create(ctypes.byref(d), ctypes.byref(h))
+        self.h = h
+        if rc != TM_OK:
+            msg = self.L.tm_last_error(h).decode() if h.value else "tm_create failed"
+            if h.value:
+                self.L.tm_destroy(h)
+            self.h = ctypes.c_void_p()
+            raise TmError(rc, msg)
+
+    def _check(self, rc):
+        if rc != TM_OK:
+            raise TmError(rc, self.L.tm_last_error(self.h).decode())
+
+    def set_template(self, spectrum):
+        s = np.ascontiguousarray(spectrum, dtype=np.complex64)
+        assert s.shape == (self.T, self.T, self.T // 2 + 1), s.shape
+        self._check(self.L.tm_set_template(self.h, _ptr(s), self.T))
+
+    def set_image(self, spectrum):
+        s = np.ascontiguousarray(spectrum, dtype=np.complex64)
+        assert s.shape == (self.Y, self.X // 2 + 1), s.shape
+        self._check(self.L.tm_set_image(self.h, _ptr(s), self.X, self.Y))
+
+    def reset(self):
+        self._check(self.L.tm_reset_results(self.h))
+
+    def run_plane(self, projection_filter, euler_angles, defocus_offset=0.0, pixel_size_offset=0.0, progress=None):
+        f = np.ascontiguousarray(projection_filter, dtype=np.float32)
+        assert f.shape == (self.T, self.T // 2 + 1), f.shape
+        a = np.ascontiguousarray(euler_angles, dtype=np.float32).reshape(-1, 3)
+        cb = PROGRESS_FN(progress) if progress else PROGRESS_FN()
+        self._check(self.L.tm_run_plane(self.h, _ptr(f), _ptr(a), len(a), defocus_offset, pixel_size_offset, cb, None))
+
+    def results(self):
+        n = self.X * self.Y
+        out = {k: np.zeros(n, np.float32) for k in ("mip", "psi", "theta", "phi", "defocus", "pixel")}
+        s = np.zeros(n, np.float64)
+        q = np.zeros(n, np.float64)
+        h = np.zeros(self.hist_bins, np.int64)
+        self._check(self.L.tm_get_results(self.h, _ptr(out["mip"]), _ptr(out["psi"]), _ptr(out["theta"]),
+                                          _ptr(out["phi"]), _ptr(out["defocus"]), _ptr(out["pixel"]),
+                                          _ptr(s), _ptr(q), _ptr(h)))
+        out["sum"], out["sumsq"], out["hist"] = s, q, h
+        return out
+
+    def correlations_computed(self):
+        return int(self.L.tm_correlations_computed(self.h))
+
+    def last_timing(self):
+        v = [ctypes.c_double() for _ in range(4)]
+        self._check(self.L.tm_last_timing(self.h, *[ctypes.byref(x) for x in v]))
+        return {"total_ms": v[0].value, "pass_b_ms": v[1].value, "pass_c_ms": v[2].value, "prep_ms": v[3].value}
+
+    def close(self):
+        if self.h and self.h.value:
+            self.L.tm_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def orientation_list(search_positions, psi_start, psi_step, psi_max, first=0, last=None):
+    """(phi, theta, psi) in the reference's loop order for search positions
+    [first, last]: position outer, psi inner, psi accumulated in float
+    (match_template.cpp:996-1004)."""
+    pos = np.asarray(search_positions, dtype=np.float32)
+    if last is None:
+        last = len(pos) - 1
+    psis = []
+    p = np.float32(psi_start)
+    while p <= np.float32(psi_max):
+        psis.append(p)
+        p = np.float32(p + np.float32(psi_step))
+    psis = np.array(psis, dtype=np.float32)
+    sel = pos[first:last + 1]
+    out = np.zeros((len(sel) * len(psis), 3), np.float32)
+    out[:, 0] = np.repeat(sel[:, 0], len(psis))
+    out[:, 1] = np.repeat(sel[:, 1], len(psis))
+    out[:, 2] = np.tile(psis, len(sel))
+    return out
+
+
+class TemplateMatchingCore:
+    """Mirror of the reference's TemplateMatchingCore (TemplateMatchingCore.h:55-179)."""
+
+    def Init(self, template_reconstruction, input_image, pixel_size_search_range, pixel_size_step, pixel_size,
+             defocus_search_range, defocus_step, defocus1, defocus2, psi_max, psi_start, psi_step,
+             search_positions, histogram_min_scaled, histogram_step_scaled, histogram_number_of_bins,
+             max_padding, first_search_position, last_search_position, total_correlation_positions=0,
+             image_x=None, image_y=None, device=0, orientation_batch=0):
+        self.image_y = input_image.shape[0]
+        self.image_x = image_x if image_x is not None else 2 * (input_image.shape[1] - 1)
+        self.T = template_reconstruction.shape[0]
+        self.psi_max, self.psi_start, self.psi_step = psi_max, psi_start, psi_step
+        self.pixel_size_step, self.defocus_step = pixel_size_step, defocus_step
+        self.orientations = orientation_list(search_positions, psi_start, psi_step, psi_max,
+                                             first_search_position, last_search_position)
+        self.core = SearchCore(self.image_x, self.image_y, self.T, histogram_min_scaled=histogram_min_scaled,
+                               histogram_step_scaled=histogram_step_scaled, histogram_bins=histogram_number_of_bins,
+                               device=device, orientation_batch=orientation_batch)
+        self.core.set_template(template_reconstruction)
+        self.core.set_image(input_image)
+        self.total_number_of_cccs_calculated = 0
+
+    def RunInnerLoop(self, projection_filter, c_pixel, c_defocus, threadIDX=0, current_correlation_position=0):
+        """One plane; like the reference, the per-plane state starts from zero."""
+        self.core.reset()
+        self.core.run_plane(projection_filter, self.orientations,
+                            defocus_offset=float(np.float32(c_defocus) * np.float32(self.defocus_step)),
+                            pixel_size_offset=float(np.float32(c_pixel) * np.float32(self.pixel_size_step)))
+        r = self.core.results()
+        shape = (self.image_y, self.image_x)
+        self.d_max_intensity_projection = r["mip"].reshape(shape)
+        self.d_best_psi = r["psi"].reshape(shape)
+        self.d_best_theta = r["theta"].reshape(shape)
+        self.d_best_phi = r["phi"].reshape(shape)
+        self.d_sum3 = r["sum"].reshape(shape)
+        self.d_sumSq3 = r["sumsq"].reshape(shape)
+        self.histogram = r["hist"]
+        self.total_number_of_cccs_calculated = len(self.orientations)
+        return current_correlation_position + len(self.orientations)

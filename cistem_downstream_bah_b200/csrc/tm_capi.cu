@@ -1,0 +1,518 @@
+// tm_capi.cu -- C ABI of the B200 search core (declared in include/tm_b200.h).
+//
+// Owns all device memory of a search context, prepares the micrograph spectrum
+// once, and drives one (pixel size, defocus) plane as a sequence of
+// orientation batches: six kernels per batch on one stream, no host
+// synchronisation inside a plane.
+#include <cuda_runtime.h>
+#include <float.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <chrono>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/tm_b200.h"
+#include "tm_kernels.cuh"
+
+#define TM_VERSION "tm_b200 0.1 (sm_100a, fp32 search path)"
+
+namespace {
+
+struct Plane {
+    long long base;       // global index of the plane's first orientation
+    int n;                // orientations in the plane
+    int angles_id;        // index into angle_lists
+    float defocus, pixel;
+};
+
+struct Variant;
+
+}  // namespace
+
+struct tm_ctx {
+    tm_dims d{};
+    int X = 0, Y = 0, T = 0, XP = 0, TP = 0, B = 0;
+    int device = 0, nsm = 0;
+    const Variant* var = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_prep = nullptr, ev_b = nullptr, ev_c = nullptr, ev_end = nullptr;
+    // device buffers
+    float2 *tmpl = nullptr, *Ip = nullptr, *S = nullptr, *A = nullptr, *C = nullptr, *norm = nullptr, *twid = nullptr;
+    float *P = nullptr, *filter = nullptr, *rot = nullptr;
+    double* rowstat = nullptr;
+    float* mip = nullptr;
+    int* best = nullptr;
+    double *sum = nullptr, *sumsq = nullptr;
+    unsigned long long* hist = nullptr;
+    int lmax = 0;
+    long long rot_capacity = 0;
+    bool has_template = false, has_image = false;
+    // bookkeeping for decoding the argmax
+    std::vector<Plane> planes;
+    std::vector<std::vector<float>> angle_lists;
+    long long next_gidx = 0;
+    long long n_ccs = 0;
+    double last_total_ms = 0, last_b_ms = 0, last_c_ms = 0, last_prep_ms = 0;
+    std::string err;
+};
+
+namespace {
+
+int set_err(tm_ctx* c, int code, const char* fmt, ...) {
+    if (c) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        c->err = buf;
+    }
+    return code;
+}
+
+#define TM_CUDA(ctx, call)                                                                              \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            return set_err((ctx), e_ == cudaErrorMemoryAllocation ? TM_ERR_OOM : TM_ERR_CUDA, "%s: %s (%s:%d)", \
+                           #call, cudaGetErrorString(e_), __FILE__, __LINE__);                         \
+    } while (0)
+
+// ---------------------------------------------------------------------------------------------
+// Kernel variants per geometry.
+
+struct Variant {
+    int T, X, Y;
+    int (*run_batch)(tm_ctx*, tmk::BatchArgs&, bool timing);
+    int (*configure)(tm_ctx*);
+};
+
+template <int T, int X, int Y>
+struct Impl {
+    using PB = tmk::PassB<T, Y>;
+    using RC = tmk::RowC2R<T>;
+
+    static int configure(tm_ctx* c) {
+        TM_CUDA(c, cudaFuncSetAttribute(tmk::k_pass_b<T, Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB::SMEM));
+        return TM_OK;
+    }
+
+    static int run_batch(tm_ctx* c, tmk::BatchArgs& a, bool timing) {
+        cudaStream_t s = c->stream;
+        tmk::k_slice_colfft<T><<<dim3((T / 2 + 1 + 15) / 16, a.nb), T, 0, s>>>(a);
+        tmk::k_row_c2r<T><<<dim3(T / RC::ROWS, a.nb), RC::NT, 0, s>>>(a);
+        tmk::k_norm<T><<<(a.nb + 7) / 8, 256, 0, s>>>(a, (long long)X * Y);
+        tmk::k_pass_a<T, X><<<dim3(T, a.nb), X / 16, 0, s>>>(a);
+        if (timing) cudaEventRecord(c->ev_prep, s);
+        const int nchunk = c->XP / PB::W;
+        const int n_items = nchunk * a.nb;
+        const int grid = n_items < c->nsm ? n_items : c->nsm;
+        tmk::k_pass_b<T, Y><<<grid, PB::NT, PB::SMEM, s>>>(a, n_items);
+        if (timing) cudaEventRecord(c->ev_b, s);
+        tmk::k_pass_c<X><<<Y, X / 16, 0, s>>>(a, Y);
+        if (timing) cudaEventRecord(c->ev_c, s);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return set_err(c, TM_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+        return TM_OK;
+    }
+};
+
+#define TM_VARIANT(T, X, Y) {T, X, Y, &Impl<T, X, Y>::run_batch, &Impl<T, X, Y>::configure}
+
+const Variant kVariants[] = {
+    TM_VARIANT(32, 256, 256),
+    TM_VARIANT(32, 512, 256),
+    TM_VARIANT(32, 256, 512),
+    TM_VARIANT(32, 512, 512),
+    TM_VARIANT(64, 512, 512),
+    TM_VARIANT(64, 1024, 1024),
+    TM_VARIANT(128, 1024, 1024),
+    TM_VARIANT(128, 2048, 2048),
+    TM_VARIANT(256, 2048, 2048),
+    TM_VARIANT(256, 4096, 4096),
+    TM_VARIANT(64, 4096, 4096),
+};
+
+const Variant* find_variant(int T, int X, int Y) {
+    for (const Variant& v : kVariants)
+        if (v.T == T && v.X == X && v.Y == Y) return &v;
+    return nullptr;
+}
+
+template <class Tp>
+int dalloc(tm_ctx* c, Tp** p, size_t count) {
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(Tp));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return set_err(c, e == cudaErrorMemoryAllocation ? TM_ERR_OOM : TM_ERR_CUDA, "cudaMalloc(%zu bytes): %s",
+                       count * sizeof(Tp), cudaGetErrorString(e));
+    }
+    return TM_OK;
+}
+
+// Waits for the stream with a time limit; polling keeps the host responsive.
+int wait_stream(tm_ctx* c, double limit_s) {
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaStreamQuery(c->stream);
+        if (e == cudaSuccess) return TM_OK;
+        if (e != cudaErrorNotReady) return set_err(c, TM_ERR_CUDA, "device error: %s", cudaGetErrorString(e));
+        double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > limit_s) return set_err(c, TM_ERR_TIMEOUT, "stream did not finish within %.0f s", limit_s);
+        std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+}
+
+void free_all(tm_ctx* c) {
+    void* ptrs[] = {c->tmpl, c->Ip, c->S, c->A, c->C, c->norm, c->twid, c->P, c->filter, c->rot,
+                    c->rowstat, c->mip, c->best, c->sum, c->sumsq, c->hist};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    cudaEvent_t evs[] = {c->ev_start, c->ev_prep, c->ev_b, c->ev_c, c->ev_end};
+    for (cudaEvent_t e : evs)
+        if (e) cudaEventDestroy(e);
+}
+
+tmk::BatchArgs make_args(tm_ctx* c) {
+    tmk::BatchArgs a{};
+    a.tmpl = c->tmpl;
+    a.filter = c->filter;
+    a.rot = c->rot;
+    a.S = c->S;
+    a.P = c->P;
+    a.rowstat = c->rowstat;
+    a.norm = c->norm;
+    a.A = c->A;
+    a.C = c->C;
+    a.Ip = c->Ip;
+    a.mip = c->mip;
+    a.best = c->best;
+    a.sum = c->sum;
+    a.sumsq = c->sumsq;
+    a.hist = c->hist;
+    a.hist_min = (float)c->d.histogram_min_scaled;
+    a.hist_inv_step = (float)(1.0 / c->d.histogram_step_scaled);
+    a.hist_bins = c->d.histogram_bins;
+    a.XP = c->XP;
+    a.tw.tab = c->twid;
+    a.tw.lmax = c->lmax;
+    return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tm_version(void) { return TM_VERSION; }
+
+const char* tm_last_error(const tm_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int tm_create(const tm_dims* dims, tm_ctx** out) {
+    if (!dims || !out) return TM_ERR_INVALID;
+    *out = nullptr;
+    tm_ctx* c = new tm_ctx();
+    c->d = *dims;
+    c->X = dims->image_x;
+    c->Y = dims->image_y;
+    c->T = dims->template_size;
+    c->XP = c->X / 2 + 4;
+    c->TP = c->T / 2 + 1;
+    c->B = dims->orientation_batch > 0 ? dims->orientation_batch : 32;
+    if (dims->histogram_bins <= 0 || dims->histogram_bins > 1024 || !(dims->histogram_step_scaled > 0)) {
+        *out = c;
+        return set_err(c, TM_ERR_INVALID, "histogram_bins must be 1..1024 and the step positive");
+    }
+    c->var = find_variant(c->T, c->X, c->Y);
+    if (!c->var) {
+        *out = c;
+        return set_err(c, TM_ERR_UNSUPPORTED, "no kernel variant for template %d and image %d x %d", c->T, c->X, c->Y);
+    }
+    c->device = dims->device;
+    int rc;
+#define TRY(x) if ((rc = (x)) != TM_OK) { *out = c; return rc; }
+    {
+        cudaError_t e = cudaSetDevice(c->device);
+        if (e != cudaSuccess) { *out = c; return set_err(c, TM_ERR_CUDA, "cudaSetDevice(%d): %s", c->device, cudaGetErrorString(e)); }
+        e = cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device);
+        if (e != cudaSuccess) { *out = c; return set_err(c, TM_ERR_CUDA, "device query: %s", cudaGetErrorString(e)); }
+    }
+    {
+        cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreate(&c->ev_start);
+        if (e == cudaSuccess) e = cudaEventCreate(&c->ev_prep);
+        if (e == cudaSuccess) e = cudaEventCreate(&c->ev_b);
+        if (e == cudaSuccess) e = cudaEventCreate(&c->ev_c);
+        if (e == cudaSuccess) e = cudaEventCreate(&c->ev_end);
+        if (e != cudaSuccess) { *out = c; return set_err(c, TM_ERR_CUDA, "stream/event creation: %s", cudaGetErrorString(e)); }
+    }
+    const size_t T = c->T, X = c->X, Y = c->Y, XP = c->XP, TP = c->TP, B = c->B;
+    TRY(dalloc(c, &c->tmpl, T * T * TP));
+    TRY(dalloc(c, &c->Ip, Y * XP));
+    TRY(dalloc(c, &c->S, B * T * TP));
+    TRY(dalloc(c, &c->P, B * T * T));
+    TRY(dalloc(c, &c->rowstat, B * T * 4));
+    TRY(dalloc(c, &c->norm, B));
+    TRY(dalloc(c, &c->A, B * T * XP));
+    TRY(dalloc(c, &c->C, B * Y * XP));
+    TRY(dalloc(c, &c->filter, T * TP));
+    TRY(dalloc(c, &c->mip, X * Y));
+    TRY(dalloc(c, &c->best, X * Y));
+    TRY(dalloc(c, &c->sum, X * Y));
+    TRY(dalloc(c, &c->sumsq, X * Y));
+    TRY(dalloc(c, &c->hist, (size_t)1024));
+    // A's columns beyond X/2 are never written by the kernels and must read as zero
+    {
+        cudaError_t e = cudaMemsetAsync(c->A, 0, B * T * XP * sizeof(float2), c->stream);
+        if (e != cudaSuccess) { *out = c; return set_err(c, TM_ERR_CUDA, "memset: %s", cudaGetErrorString(e)); }
+    }
+    // twiddle table W_LMAX^m for the largest transform length
+    c->lmax = (int)(X > Y ? X : Y);
+    TRY(dalloc(c, &c->twid, (size_t)c->lmax));
+    {
+        std::vector<float2> tw(c->lmax);
+        for (int m = 0; m < c->lmax; m++) {
+            double ang = -2.0 * M_PI * (double)m / (double)c->lmax;
+            tw[m] = make_float2((float)cos(ang), (float)sin(ang));
+        }
+        cudaError_t e = cudaMemcpy(c->twid, tw.data(), sizeof(float2) * c->lmax, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { *out = c; return set_err(c, TM_ERR_CUDA, "twiddle upload: %s", cudaGetErrorString(e)); }
+    }
+    TRY(c->var->configure(c));
+#undef TRY
+    *out = c;
+    return tm_reset_results(c);
+}
+
+int tm_set_template(tm_ctx* c, const float* spectrum, int template_size) {
+    if (!c || !spectrum) return TM_ERR_INVALID;
+    if (template_size != c->T) return set_err(c, TM_ERR_INVALID, "template size %d differs from the context's %d", template_size, c->T);
+    TM_CUDA(c, cudaSetDevice(c->device));
+    TM_CUDA(c, cudaMemcpy(c->tmpl, spectrum, sizeof(float2) * (size_t)c->T * c->T * c->TP, cudaMemcpyHostToDevice));
+    c->has_template = true;
+    return TM_OK;
+}
+
+int tm_set_image(tm_ctx* c, const float* spectrum, int image_x, int image_y) {
+    if (!c || !spectrum) return TM_ERR_INVALID;
+    if (image_x != c->X || image_y != c->Y)
+        return set_err(c, TM_ERR_INVALID, "image %d x %d differs from the context's %d x %d", image_x, image_y, c->X, c->Y);
+    TM_CUDA(c, cudaSetDevice(c->device));
+    // I'[ky][kx] = I[ky][kx] * exp(+2 pi i (kx*x0/X + ky*y0/Y)) / N, with the
+    // projection placed at (x0, y0) = (X/2 - T/2, Y/2 - T/2); I'[0][0] = 0.
+    const int X = c->X, Y = c->Y, hc = X / 2 + 1, XP = c->XP;
+    const long long x0 = X / 2 - c->T / 2, y0 = Y / 2 - c->T / 2;
+    const double invn = 1.0 / ((double)X * (double)Y);
+    std::vector<float2> ip((size_t)Y * XP, make_float2(0.f, 0.f));
+    std::vector<double> cx(hc), sx(hc);
+    for (int kx = 0; kx < hc; kx++) {
+        double a = 2.0 * M_PI * (double)((kx * x0) % X) / (double)X;
+        cx[kx] = cos(a);
+        sx[kx] = sin(a);
+    }
+    for (int ky = 0; ky < Y; ky++) {
+        double b = 2.0 * M_PI * (double)((ky * y0) % Y) / (double)Y;
+        double cy = cos(b), sy = sin(b);
+        for (int kx = 0; kx < hc; kx++) {
+            double pr = cx[kx] * cy - sx[kx] * sy, pi = cx[kx] * sy + sx[kx] * cy;
+            double ir = spectrum[2 * ((size_t)ky * hc + kx)], ii = spectrum[2 * ((size_t)ky * hc + kx) + 1];
+            ip[(size_t)ky * XP + kx] = make_float2((float)((ir * pr - ii * pi) * invn), (float)((ir * pi + ii * pr) * invn));
+        }
+    }
+    ip[0] = make_float2(0.f, 0.f);
+    TM_CUDA(c, cudaMemcpy(c->Ip, ip.data(), sizeof(float2) * ip.size(), cudaMemcpyHostToDevice));
+    c->has_image = true;
+    return TM_OK;
+}
+
+int tm_reset_results(tm_ctx* c) {
+    if (!c) return TM_ERR_INVALID;
+    TM_CUDA(c, cudaSetDevice(c->device));
+    const size_t n = (size_t)c->X * c->Y;
+    tmk::k_reset_state<<<c->nsm * 4, 256, 0, c->stream>>>(c->mip, c->best, c->sum, c->sumsq, n);
+    TM_CUDA(c, cudaGetLastError());
+    TM_CUDA(c, cudaMemsetAsync(c->hist, 0, sizeof(unsigned long long) * 1024, c->stream));
+    int rc = wait_stream(c, 60.0);
+    if (rc != TM_OK) return rc;
+    c->planes.clear();
+    c->angle_lists.clear();
+    c->next_gidx = 0;
+    c->n_ccs = 0;
+    return TM_OK;
+}
+
+int tm_run_plane(tm_ctx* c, const float* projection_filter, const float* euler_angles, int n, float defocus_offset,
+                 float pixel_size_offset, tm_progress_fn progress, void* user) {
+    if (!c || !projection_filter || (!euler_angles && n > 0) || n < 0) return TM_ERR_INVALID;
+    if (!c->has_template || !c->has_image) return set_err(c, TM_ERR_INVALID, "template and image must be set before tm_run_plane");
+    if (c->next_gidx + n > 2147483647LL) return set_err(c, TM_ERR_INVALID, "more than 2^31 orientations since the last reset");
+    if (n == 0) return TM_OK;
+    TM_CUDA(c, cudaSetDevice(c->device));
+    // rotation table, float Euler matrices as RotationMatrix::SetToEulerRotation (matrix.cpp:490-510)
+    if (n > c->rot_capacity) {
+        if (c->rot) cudaFree(c->rot);
+        c->rot = nullptr;
+        int rc = dalloc(c, &c->rot, (size_t)6 * n);
+        if (rc != TM_OK) return rc;
+        c->rot_capacity = n;
+    }
+    std::vector<float> rot((size_t)6 * n);
+    const float pif = 3.14159265359f;
+    for (int o = 0; o < n; o++) {
+        auto d2r = [pif](float deg) { return (float)((double)(deg * pif) / 180.); };
+        const float phi = euler_angles[3 * o], theta = euler_angles[3 * o + 1], psi = euler_angles[3 * o + 2];
+        const float cphi = cosf(d2r(phi)), sphi = sinf(d2r(phi));
+        const float cth = cosf(d2r(theta)), sth = sinf(d2r(theta));
+        const float cpsi = cosf(d2r(psi)), spsi = sinf(d2r(psi));
+        float* m = rot.data() + 6 * (size_t)o;
+        m[0] = cphi * cth * cpsi - sphi * spsi;    // m[0][0]
+        m[1] = -cphi * cth * spsi - sphi * cpsi;   // m[0][1]
+        m[2] = sphi * cth * cpsi + cphi * spsi;    // m[1][0]
+        m[3] = -sphi * cth * spsi + cphi * cpsi;   // m[1][1]
+        m[4] = -sth * cpsi;                        // m[2][0]
+        m[5] = sth * spsi;                         // m[2][1]
+    }
+    TM_CUDA(c, cudaMemcpyAsync(c->rot, rot.data(), sizeof(float) * rot.size(), cudaMemcpyHostToDevice, c->stream));
+    TM_CUDA(c, cudaMemcpyAsync(c->filter, projection_filter, sizeof(float) * (size_t)c->T * c->TP, cudaMemcpyHostToDevice, c->stream));
+    // bookkeeping for decoding (reuse the previous angle list when identical)
+    Plane pl;
+    pl.base = c->next_gidx;
+    pl.n = n;
+    pl.defocus = defocus_offset;
+    pl.pixel = pixel_size_offset;
+    if (!c->angle_lists.empty() && (int)c->angle_lists.back().size() == 3 * n &&
+        memcmp(c->angle_lists.back().data(), euler_angles, sizeof(float) * 3 * (size_t)n) == 0) {
+        pl.angles_id = (int)c->angle_lists.size() - 1;
+    } else {
+        c->angle_lists.emplace_back(euler_angles, euler_angles + 3 * (size_t)n);
+        pl.angles_id = (int)c->angle_lists.size() - 1;
+    }
+    c->planes.push_back(pl);
+
+    tmk::BatchArgs a = make_args(c);
+    a.rot = c->rot;
+    TM_CUDA(c, cudaEventRecord(c->ev_start, c->stream));
+    double b_ms = 0, c_ms = 0, prep_ms = 0;
+    const int nbatch = (n + c->B - 1) / c->B;
+    for (int bi = 0; bi < nbatch; bi++) {
+        a.orient0 = bi * c->B;
+        a.nb = n - a.orient0 < c->B ? n - a.orient0 : c->B;
+        a.gidx0 = pl.base + a.orient0;
+        // time the kernel families on the first and last batch only (events
+        // cost a little; the split is for roofline accounting)
+        const bool timing = (bi == 0 || bi == nbatch - 1);
+        cudaEvent_t evb0 = nullptr;
+        if (timing) {
+            TM_CUDA(c, cudaEventRecord(c->ev_end, c->stream));
+            evb0 = c->ev_end;
+        }
+        int rc = c->var->run_batch(c, a, timing);
+        if (rc != TM_OK) return rc;
+        if (timing) {
+            int w = wait_stream(c, 600.0);
+            if (w != TM_OK) return w;
+            float t_prep = 0, t_b = 0, t_c = 0;
+            cudaEventElapsedTime(&t_prep, evb0, c->ev_prep);
+            cudaEventElapsedTime(&t_b, c->ev_prep, c->ev_b);
+            cudaEventElapsedTime(&t_c, c->ev_b, c->ev_c);
+            const double scale = (double)a.nb;
+            prep_ms += t_prep / scale;
+            b_ms += t_b / scale;
+            c_ms += t_c / scale;
+        }
+        if (progress) {
+            if (progress((long long)(a.orient0 + a.nb), (long long)n, user) != 0) {
+                int w = wait_stream(c, 600.0);
+                c->next_gidx += n;
+                return w != TM_OK ? w : set_err(c, TM_ERR_CANCELLED, "cancelled by the progress callback");
+            }
+        }
+    }
+    TM_CUDA(c, cudaEventRecord(c->ev_c, c->stream));
+    int w = wait_stream(c, 3600.0);
+    if (w != TM_OK) return w;
+    float tot = 0;
+    cudaEventElapsedTime(&tot, c->ev_start, c->ev_c);
+    // per-orientation averages of the sampled batches, scaled to the plane
+    const int sampled = nbatch > 1 ? 2 : 1;
+    c->last_total_ms = tot;
+    c->last_prep_ms = prep_ms / sampled * n;
+    c->last_b_ms = b_ms / sampled * n;
+    c->last_c_ms = c_ms / sampled * n;
+    c->next_gidx += n;
+    c->n_ccs += n;
+    return TM_OK;
+}
+
+int tm_get_results(tm_ctx* c, float* mip, float* best_psi, float* best_theta, float* best_phi, float* best_defocus,
+                   float* best_pixel_size, double* sum, double* sum_of_squares, long long* histogram) {
+    if (!c) return TM_ERR_INVALID;
+    TM_CUDA(c, cudaSetDevice(c->device));
+    const size_t n = (size_t)c->X * c->Y;
+    int rc = wait_stream(c, 3600.0);
+    if (rc != TM_OK) return rc;
+    if (mip) TM_CUDA(c, cudaMemcpy(mip, c->mip, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    if (sum) TM_CUDA(c, cudaMemcpy(sum, c->sum, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (sum_of_squares) TM_CUDA(c, cudaMemcpy(sum_of_squares, c->sumsq, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (histogram) {
+        std::vector<unsigned long long> h(c->d.histogram_bins);
+        TM_CUDA(c, cudaMemcpy(h.data(), c->hist, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < h.size(); i++) histogram[i] = (long long)h[i];
+    }
+    if (best_psi || best_theta || best_phi || best_defocus || best_pixel_size) {
+        std::vector<int> best(n);
+        TM_CUDA(c, cudaMemcpy(best.data(), c->best, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < n; i++) {
+            const int g = best[i];
+            float psi = 0, th = 0, ph = 0, df = 0, px = 0;
+            if (g >= 0) {
+                // planes are few: linear scan from the back (most recent first)
+                for (size_t k = c->planes.size(); k-- > 0;) {
+                    const Plane& p = c->planes[k];
+                    if (g >= p.base && g < p.base + p.n) {
+                        const float* ang = c->angle_lists[p.angles_id].data() + 3 * (size_t)(g - p.base);
+                        ph = ang[0];
+                        th = ang[1];
+                        psi = ang[2];
+                        df = p.defocus;
+                        px = p.pixel;
+                        break;
+                    }
+                }
+            }
+            if (best_psi) best_psi[i] = psi;
+            if (best_theta) best_theta[i] = th;
+            if (best_phi) best_phi[i] = ph;
+            if (best_defocus) best_defocus[i] = df;
+            if (best_pixel_size) best_pixel_size[i] = px;
+        }
+    }
+    return TM_OK;
+}
+
+long long tm_correlations_computed(const tm_ctx* c) { return c ? c->n_ccs : 0; }
+
+int tm_last_timing(const tm_ctx* c, double* total_ms, double* pass_b_ms, double* pass_c_ms, double* prep_ms) {
+    if (!c) return TM_ERR_INVALID;
+    if (total_ms) *total_ms = c->last_total_ms;
+    if (pass_b_ms) *pass_b_ms = c->last_b_ms;
+    if (pass_c_ms) *pass_c_ms = c->last_c_ms;
+    if (prep_ms) *prep_ms = c->last_prep_ms;
+    return TM_OK;
+}
+
+int tm_destroy(tm_ctx* c) {
+    if (!c) return TM_ERR_INVALID;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_all(c);
+    delete c;
+    return TM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,486 @@
+// tm_kernels.cuh -- the search kernels for one batch of orientations.
+//
+// Data flow per orientation (o) of a batch, T = template box, X x Y = padded
+// micrograph, XP = X/2 + 4 (row pitch of half-spectra, in complex values):
+//
+//   k_slice_colfft   Fourier slice of the 3-D template (trilinear, Hermitian
+//                    mirror; image.cpp:2450-2607, 2899-3020) x (-1)^(i+j)
+//                    (SwapRealSpaceQuadrants) x projection filter, then the
+//                    inverse FFT along y of each of the T/2+1 columns
+//   k_row_c2r        inverse c2r FFT of each row -> real T x T projection,
+//                    plus per-row sums for the edge mean and variance
+//   k_norm           per-orientation edge mean e and 1/sigma
+//                    (match_template.cpp:1060-1068)
+//   k_pass_a         (p - e)/sigma, placed at the origin of an X-wide row and
+//                    forward FFT along x using only its T non-zero samples
+//                    (X/T twiddled T-point FFTs) -> A[o][row][kx]
+//   k_pass_b         per column kx: pruned forward FFT along y of the T rows
+//                    of A, multiply by the prepared micrograph spectrum
+//                    I'[ky][kx] (whitened spectrum x conj(placement phase) / N,
+//                    DC zero), inverse FFT along y -> C[o][y][kx]
+//   k_pass_c         per row y: c2r FFT along x of C[o][y][:] and, in
+//                    registers, the MIP / argmax / sum / sum-of-squares /
+//                    histogram update of match_template.cpp:1102-1149 over the
+//                    batch; per-pixel state is read and written once per batch
+//
+// The placement of the projection at (X/2 - T/2, Y/2 - T/2)
+// (ClipIntoLargerRealSpace2D, image.cpp:8398-8465), the forward-FFT scaling
+// 1/N and the zeroed central pixel are folded into I' once per micrograph.
+#pragma once
+#include <float.h>
+#include "tm_fft.cuh"
+
+namespace tmk {
+
+using tmfft::cmul;
+using tmfft::cmul_conj;
+using tmfft::Twiddles;
+
+__host__ __device__ constexpr int round_up16(int v) { return (v + 15) / 16 * 16; }
+// region stride >= len whose value mod 16 equals `rem` (bank skew between regions)
+__host__ __device__ constexpr int skewed(int len, int rem) { return round_up16(len) + rem; }
+
+struct BatchArgs {
+    int nb;                       // orientations in this batch
+    int orient0;                  // index of the batch's first orientation within the plane
+    long long gidx0;              // global orientation index of the batch's first orientation
+    const float* rot;             // plane rotation table: 6 floats per orientation (m00 m01 m10 m11 m20 m21)
+    const float2* tmpl;           // T*T*(T/2+1) template spectrum
+    const float* filter;          // T*(T/2+1) projection filter
+    float2* S;                    // nb * T * (T/2+1)
+    float* P;                     // nb * T * T
+    double* rowstat;              // nb * T * 4
+    float2* norm;                 // nb: (edge mean, 1/sigma)
+    float2* A;                    // nb * T * XP
+    float2* C;                    // nb * Y * XP
+    const float2* Ip;             // Y * XP prepared micrograph spectrum
+    float* mip;                   // Y * X
+    int* best;                    // Y * X
+    double* sum;                  // Y * X
+    double* sumsq;                // Y * X
+    unsigned long long* hist;     // hist_bins
+    float hist_min, hist_inv_step;
+    int hist_bins;
+    int XP;                       // row pitch (complex values) of A, C and Ip
+    Twiddles tw;
+};
+
+// --------------------------------------------------------------------------------------
+// Trilinear Fourier interpolation with the reference's bounds and Hermitian rules
+// (Image::ReturnLinearInterpolatedFourier, image.cpp:2899-3020), even T.
+template <int T>
+__device__ __forceinline__ float2 interp3(const float2* __restrict__ vol, float x, float y, float z) {
+    constexpr int TP = T / 2 + 1;
+    const int lb = -(T / 2), ub = T / 2 - 1;
+    float2 acc = make_float2(0.f, 0.f);
+    if (x >= 0.f) {
+        int i0 = (int)floorf(x);
+        if (i0 + 1 > T / 2) return acc;
+        int j0 = (int)floorf(y);
+        if (j0 < lb || j0 + 1 > ub) return acc;
+        int k0 = (int)floorf(z);
+        if (k0 < lb || k0 + 1 > ub) return acc;
+        const float wx1 = x - (float)i0, wx0 = 1.f - wx1;
+#pragma unroll
+        for (int dk = 0; dk < 2; dk++) {
+            const int k = k0 + dk;
+            const int pz = k >= 0 ? k : T + k;
+            const float wz = 1.f - fabsf(z - (float)k);
+#pragma unroll
+            for (int dj = 0; dj < 2; dj++) {
+                const int j = j0 + dj;
+                const int py = j >= 0 ? j : T + j;
+                const float w = wz * (1.f - fabsf(y - (float)j));
+                const float2* row = vol + ((size_t)pz * T + py) * TP;
+                const float2 a = __ldg(row + i0), b = __ldg(row + i0 + 1);
+                acc.x = fmaf(a.x, w * wx0, acc.x);
+                acc.y = fmaf(a.y, w * wx0, acc.y);
+                acc.x = fmaf(b.x, w * wx1, acc.x);
+                acc.y = fmaf(b.y, w * wx1, acc.y);
+            }
+        }
+    } else {
+        int i0 = (int)floorf(x);
+        if (i0 < -(T / 2)) return acc;
+        int j0 = (int)floorf(y);
+        if (j0 < lb || j0 + 1 > ub) return acc;
+        int k0 = (int)floorf(z);
+        if (k0 < lb || k0 + 1 > ub) return acc;
+        const float wx1 = x - (float)i0, wx0 = 1.f - wx1;
+#pragma unroll
+        for (int dk = 0; dk < 2; dk++) {
+            const int k = k0 + dk;
+            const int pz = k > 0 ? T - k : -k;
+            const float wz = 1.f - fabsf(z - (float)k);
+#pragma unroll
+            for (int dj = 0; dj < 2; dj++) {
+                const int j = j0 + dj;
+                const int py = j > 0 ? T - j : -j;
+                const float w = wz * (1.f - fabsf(y - (float)j));
+                const float2* row = vol + ((size_t)pz * T + py) * TP;
+                // mirrored samples at x indices -i0 and -(i0+1), conjugated
+                const float2 a = __ldg(row - i0), b = __ldg(row - i0 - 1);
+                acc.x = fmaf(a.x, w * wx0, acc.x);
+                acc.y = fmaf(-a.y, w * wx0, acc.y);
+                acc.x = fmaf(b.x, w * wx1, acc.x);
+                acc.y = fmaf(-b.y, w * wx1, acc.y);
+            }
+        }
+    }
+    return acc;
+}
+
+// --------------------------------------------------------------------------------------
+// k_slice_colfft: block = 16 columns x (T/16) threads; grid = (ceil((T/2+1)/16), nb)
+template <int T>
+__global__ void __launch_bounds__(T)
+k_slice_colfft(BatchArgs a) {
+    constexpr int TP = T / 2 + 1;
+    constexpr int PT = T / 16;
+    constexpr int RS = skewed(tmfft::padded_len(T), 1);
+    __shared__ float2 sm[16 * RS];
+    const int il = threadIdx.x & 15, tp = threadIdx.x >> 4;
+    const int i = blockIdx.x * 16 + il;
+    const int o = blockIdx.y;
+    const bool valid = i <= T / 2;
+    const float* m = a.rot + 6 * (size_t)(a.orient0 + o);
+    const float m00 = __ldg(m), m01 = __ldg(m + 1), m10 = __ldg(m + 2), m11 = __ldg(m + 3), m20 = __ldg(m + 4), m21 = __ldg(m + 5);
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; r++) {
+        const int y = tp + PT * r;
+        const int j = y < T / 2 ? y : y - T;
+        float2 val = make_float2(0.f, 0.f);
+        if (valid) {
+            if (i == 0) {
+                if (j != 0) {
+                    // j > 0 and j = -T/2 interpolate at (0, j); other j < 0 mirror (0, -j)
+                    const int jj = (j > 0 || j == -(T / 2)) ? j : -j;
+                    const float fy = (float)jj;
+                    val = interp3<T>(a.tmpl, m01 * fy, m11 * fy, m21 * fy);
+                    if (jj != j) val.y = -val.y;
+                }
+            } else {
+                const float fx = (float)i, fy = (float)j;
+                val = interp3<T>(a.tmpl, fmaf(m00, fx, m01 * fy), fmaf(m10, fx, m11 * fy), fmaf(m20, fx, m21 * fy));
+            }
+            float f = __ldg(a.filter + (size_t)y * TP + i);
+            if ((i + j) & 1) f = -f;
+            val.x *= f;
+            val.y *= f;
+        }
+        v[r] = val;
+    }
+    tmfft::fft<T, 16, +1>(v, tp, sm + il * RS, a.tw, [] __device__() { __syncthreads(); });
+    if (valid) {
+        float2* out = a.S + (size_t)o * T * TP;
+#pragma unroll
+        for (int r = 0; r < 16; r++) out[(size_t)(tp + PT * r) * TP + i] = v[r];
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// k_row_c2r: each row of T/2+1 complex -> T reals via a T/2-point inverse FFT
+// (even/odd packing; imaginary parts of the DC and Nyquist terms ignored as in
+// FFTW's c2r).  block = ROWS rows x PH threads; grid = (T/ROWS, nb).
+template <int T>
+struct RowC2R {
+    static constexpr int H = T / 2;
+    static constexpr int PH = H / 16;                           // threads per row
+    static constexpr int ROWS = (256 / PH) < T ? (256 / PH) : T;  // rows per block
+    static constexpr int NT = ROWS * PH;
+    static constexpr int RS = skewed(tmfft::padded_len(H), PH % 16);
+};
+
+template <int T>
+__global__ void __launch_bounds__(RowC2R<T>::NT)
+k_row_c2r(BatchArgs a) {
+    using RC = RowC2R<T>;
+    constexpr int TP = T / 2 + 1, H = RC::H, PH = RC::PH, ROWS = RC::ROWS;
+    constexpr int RS = RC::RS;
+    __shared__ float2 sm[ROWS * RS];
+    const int t = threadIdx.x % PH, rl = threadIdx.x / PH;
+    const int y = blockIdx.x * ROWS + rl;
+    const int o = blockIdx.y;
+    const float2* Hrow = a.S + ((size_t)o * T + y) * TP;
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; r++) {
+        const int k = t + PH * r;
+        float2 hk = Hrow[k];
+        float2 hm = Hrow[H - k];
+        if (k == 0) { hk.y = 0.f; hm.y = 0.f; }
+        const float2 e = make_float2(hk.x + hm.x, hk.y - hm.y);
+        const float2 d = make_float2(hk.x - hm.x, hk.y + hm.y);
+        const float2 od = cmul(d, a.tw.template w<+1>(k, T));
+        v[r] = make_float2(e.x - od.y, e.y + od.x);
+    }
+    tmfft::fft<H, 16, +1>(v, t, sm + rl * RS, a.tw, [] __device__() { __syncthreads(); });
+    float* prow = a.P + ((size_t)o * T + y) * T;
+    float s = 0.f, q = 0.f;
+#pragma unroll
+    for (int r = 0; r < 16; r++) {
+        const int mm = t + PH * r;
+        reinterpret_cast<float2*>(prow)[mm] = v[r];
+        s += v[r].x + v[r].y;
+        q = fmaf(v[r].x, v[r].x, fmaf(v[r].y, v[r].y, q));
+    }
+    double ds = s, dq = q;
+#pragma unroll
+    for (int off = PH / 2; off > 0; off >>= 1) {
+        ds += __shfl_xor_sync(0xffffffffu, ds, off);
+        dq += __shfl_xor_sync(0xffffffffu, dq, off);
+    }
+    // edge sum: full first and last rows, else the first and last pixel
+    float e0 = 0.f, e1 = 0.f;
+    if (t == 0) e0 = v[0].x;                                   // pixel 0 = z[0].x
+    if (t == (H - 1) % PH) e1 = v[(H - 1) / PH].y;            // pixel T-1 = z[H-1].y
+    float ee = e0 + e1;
+#pragma unroll
+    for (int off = PH / 2; off > 0; off >>= 1) ee += __shfl_xor_sync(0xffffffffu, ee, off);
+    const double edge = (y == 0 || y == T - 1) ? ds : (double)ee;
+    if (t == 0) {
+        double* st = a.rowstat + ((size_t)o * T + y) * 4;
+        st[0] = ds;
+        st[1] = dq;
+        st[2] = edge;
+        st[3] = 0.0;
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// k_norm: one warp per orientation.  e = edge mean (ReturnAverageOfRealValuesOnEdges,
+// image.cpp:5907-5945); variance as match_template.cpp:1066-1067 with the
+// mean of squares and the mean of the edge-subtracted projection.
+template <int T>
+__global__ void __launch_bounds__(256)
+k_norm(BatchArgs a, long long n_image) {
+    const int lane = threadIdx.x & 31;
+    const int o = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (o >= a.nb) return;
+    double s = 0, q = 0, e = 0;
+    for (int y = lane; y < T; y += 32) {
+        const double* st = a.rowstat + ((size_t)o * T + y) * 4;
+        s += st[0];
+        q += st[1];
+        e += st[2];
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, off);
+        q += __shfl_xor_sync(0xffffffffu, q, off);
+        e += __shfl_xor_sync(0xffffffffu, e, off);
+    }
+    if (lane == 0) {
+        const double n = (double)T * T;
+        const float edge_mean = (float)(e / (double)(4 * T - 4));
+        const double em = edge_mean;
+        const double s1 = s - n * em;                 // sum of (p - e)
+        const double s2 = q - 2.0 * em * s + n * em * em;  // sum of (p - e)^2
+        const double ratio = n / (double)n_image;
+        const double var = (s2 / n) * ratio - ((s1 / n) * ratio) * ((s1 / n) * ratio);
+        a.norm[o] = make_float2(edge_mean, (float)(1.0 / sqrt(var)));
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// k_pass_a: one block per (row, orientation); X/16 threads, thread j = s + MX*t'
+template <int T, int X>
+__global__ void __launch_bounds__(X / 16)
+k_pass_a(BatchArgs a) {
+    const int XP = a.XP;
+    constexpr int MX = X / T, PT = T / 16;
+    constexpr int RS = skewed(tmfft::padded_len(T), 1);
+    __shared__ float2 sm[MX * RS];
+    __shared__ float q[T];
+    const int j = threadIdx.x;
+    const int s = j % MX, tp = j / MX;
+    const int row = blockIdx.x, o = blockIdx.y;
+    const float2 nrm = a.norm[o];
+    const float* prow = a.P + ((size_t)o * T + row) * T;
+    for (int m = j; m < T; m += X / 16) q[m] = (prow[m] - nrm.x) * nrm.y;
+    __syncthreads();
+    float2 v[16];
+    const float2 w0 = a.tw.template w<-1>(s * tp, X);
+    const float2 w1 = a.tw.template w<-1>(s * PT, X);
+    float2 w = w0;
+#pragma unroll
+    for (int r = 0; r < 16; r++) {
+        const float qv = q[tp + PT * r];
+        v[r] = make_float2(qv * w.x, qv * w.y);
+        w = cmul(w, w1);
+    }
+    tmfft::fft<T, 16, -1>(v, tp, sm + s * RS, a.tw, [] __device__() { __syncthreads(); });
+    float2* out = a.A + ((size_t)o * T + row) * XP;
+#pragma unroll
+    for (int r = 0; r < 16; r++) {
+        const int kx = j + (X / 16) * r;
+        if (kx <= X / 2) out[kx] = v[r];
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// k_pass_b: persistent; block = W columns x Y/16 threads (thread = c + W*j);
+// work item = (column chunk, orientation), orientation fastest.
+template <int T, int Y>
+struct PassB {
+    static constexpr int W = 16384 / Y;               // columns per block
+    static constexpr int NT = W * (Y / 16);           // 1024 threads
+    static constexpr int MY = Y / T, PT = T / 16;
+    static constexpr int RST = skewed(tmfft::padded_len(T), 1);
+    static constexpr int CS0 = (MY * RST > tmfft::padded_len(Y)) ? MY * RST : tmfft::padded_len(Y);
+    static constexpr int CS = round_up16(CS0) + 16 / W;  // column stride, = 16/W mod 16
+    static constexpr size_t SMEM = sizeof(float2) * ((size_t)W * CS + (size_t)T * W);
+};
+
+template <int T, int Y>
+__global__ void __launch_bounds__(1024, 1)
+k_pass_b(BatchArgs a, int n_items) {
+    using PB = PassB<T, Y>;
+    constexpr int W = PB::W, MY = PB::MY, PT = PB::PT;
+    const int XP = a.XP;
+    extern __shared__ float2 smem_b[];
+    float2* cols = smem_b;
+    float2* Asm = smem_b + (size_t)W * PB::CS;
+    const int c = threadIdx.x % W, j = threadIdx.x / W;
+    const int s = j % MY, tp = j / MY;
+    float2* colbuf = cols + (size_t)c * PB::CS;
+    float2* fwdbuf = colbuf + s * PB::RST;
+    // twiddles of the pruned forward: W_Y^(s * (tp + PT*r))
+    const float2 w0 = a.tw.template w<-1>(s * tp, Y);
+    const float2 w1 = a.tw.template w<-1>(s * PT, Y);
+    auto sync = [] __device__() { __syncthreads(); };
+    const int per = (n_items + gridDim.x - 1) / gridDim.x;
+    const int it0 = blockIdx.x * per;
+    const int it1 = min(n_items, it0 + per);
+    for (int it = it0; it < it1; it++) {
+        const int chunk = it / a.nb, o = it % a.nb;
+        const int kx0 = chunk * W;
+        __syncthreads();  // previous item finished with Asm / cols
+        const float2* Ao = a.A + (size_t)o * T * XP + kx0;
+        for (int e = threadIdx.x; e < T * W; e += PB::NT) Asm[e] = Ao[(size_t)(e / W) * XP + (e % W)];
+        __syncthreads();
+        float2 v[16];
+        float2 w = w0;
+#pragma unroll
+        for (int r = 0; r < 16; r++) {
+            v[r] = cmul(Asm[(tp + PT * r) * W + c], w);
+            w = cmul(w, w1);
+        }
+        tmfft::fft<T, 16, -1>(v, tp, fwdbuf, a.tw, sync);
+        // thread (s, tp) holds F[k], k = s + MY*(tp + PT*r) = j + (Y/16)*r
+        const float2* Ic = a.Ip + kx0 + c;
+#pragma unroll
+        for (int r = 0; r < 16; r++) {
+            const int k = j + (Y / 16) * r;
+            v[r] = cmul_conj(__ldg(Ic + (size_t)k * XP), v[r]);
+        }
+        tmfft::fft<Y, 16, +1>(v, j, colbuf, a.tw, sync);
+        float2* Co = a.C + (size_t)o * Y * XP + kx0 + c;
+#pragma unroll
+        for (int r = 0; r < 16; r++) Co[(size_t)(j + (Y / 16) * r) * XP] = v[r];
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// k_pass_c: one block per row y; X/16 threads each own 16 pixels
+// (x = 2*(t + P*r) + h); loops over the batch keeping the per-pixel state in
+// registers.
+template <int X>
+struct PassC {
+    static constexpr int H = X / 2;
+    static constexpr int R = 8;
+    static constexpr int P = H / R;                 // X/16 threads
+    static constexpr int XP = X / 2 + 4;            // row pitch used for the C buffer
+    static constexpr int RSF = tmfft::padded_len(H);
+};
+
+template <int X>
+__global__ void __launch_bounds__(X / 16, 2)
+k_pass_c(BatchArgs a, int Y) {
+    using PC = PassC<X>;
+    constexpr int H = PC::H, P = PC::P, XP = PC::XP;
+    __shared__ float2 rowbuf[XP];
+    __shared__ float2 fbuf[PC::RSF];
+    __shared__ unsigned int shist[1024];
+    const int t = threadIdx.x;
+    const int y = blockIdx.x;
+    for (int b = t; b < a.hist_bins; b += P) shist[b] = 0u;
+    float mip[16];
+    int best[16];
+    float fs[16], fq[16];
+    const size_t rowoff = (size_t)y * X;
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        const int x = 2 * (t + P * r);
+        const float2 mv = *reinterpret_cast<const float2*>(a.mip + rowoff + x);
+        const int2 bv = *reinterpret_cast<const int2*>(a.best + rowoff + x);
+        mip[2 * r] = mv.x; mip[2 * r + 1] = mv.y;
+        best[2 * r] = bv.x; best[2 * r + 1] = bv.y;
+        fs[2 * r] = 0.f; fs[2 * r + 1] = 0.f;
+        fq[2 * r] = 0.f; fq[2 * r + 1] = 0.f;
+    }
+    auto sync = [] __device__() { __syncthreads(); };
+    for (int o = 0; o < a.nb; o++) {
+        const float4* src = reinterpret_cast<const float4*>(a.C + ((size_t)o * Y + y) * XP);
+        float4* dst = reinterpret_cast<float4*>(rowbuf);
+        for (int e = t; e < XP / 2; e += P) dst[e] = __ldg(src + e);
+        __syncthreads();
+        float2 v[8];
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const int k = t + P * r;
+            float2 hk = rowbuf[k];
+            float2 hm = rowbuf[H - k];
+            if (k == 0) { hk.y = 0.f; hm.y = 0.f; }
+            const float2 e = make_float2(hk.x + hm.x, hk.y - hm.y);
+            const float2 d = make_float2(hk.x - hm.x, hk.y + hm.y);
+            const float2 od = cmul(d, a.tw.template w<+1>(k, X));
+            v[r] = make_float2(e.x - od.y, e.y + od.x);
+        }
+        tmfft::fft<H, 8, +1>(v, t, fbuf, a.tw, sync);
+        const int g = (int)(a.gidx0 + o);
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const float val = h ? v[r].y : v[r].x;
+                const int pi = 2 * r + h;
+                if (val > mip[pi]) { mip[pi] = val; best[pi] = g; }
+                fs[pi] += val;
+                fq[pi] = fmaf(val, val, fq[pi]);
+                const int bin = __float2int_rz((val - a.hist_min) * a.hist_inv_step);
+                if (bin >= 0 && bin < a.hist_bins) atomicAdd(&shist[bin], 1u);
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        const int x = 2 * (t + P * r);
+        *reinterpret_cast<float2*>(a.mip + rowoff + x) = make_float2(mip[2 * r], mip[2 * r + 1]);
+        *reinterpret_cast<int2*>(a.best + rowoff + x) = make_int2(best[2 * r], best[2 * r + 1]);
+        double2 sv = *reinterpret_cast<const double2*>(a.sum + rowoff + x);
+        double2 qv = *reinterpret_cast<const double2*>(a.sumsq + rowoff + x);
+        sv.x += (double)fs[2 * r]; sv.y += (double)fs[2 * r + 1];
+        qv.x += (double)fq[2 * r]; qv.y += (double)fq[2 * r + 1];
+        *reinterpret_cast<double2*>(a.sum + rowoff + x) = sv;
+        *reinterpret_cast<double2*>(a.sumsq + rowoff + x) = qv;
+    }
+    __syncthreads();
+    for (int b = t; b < a.hist_bins; b += P) {
+        const unsigned int cnt = shist[b];
+        if (cnt) atomicAdd(a.hist + b, (unsigned long long)cnt);
+    }
+}
+
+// --------------------------------------------------------------------------------------
+__global__ void k_reset_state(float* mip, int* best, double* sum, double* sumsq, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        mip[i] = -FLT_MAX;
+        best[i] = -1;
+        sum[i] = 0.0;
+        sumsq[i] = 0.0;
+    }
+}
+
+}  // namespace tmk

@@ -1,0 +1,130 @@
+/*
+ * tm_b200.h -- C ABI of the B200 match_template search core.
+ *
+ * The search core replaces the GPU inner loop of cisTEM's match_template:
+ * TemplateMatchingCore (src/gpu/TemplateMatchingCore.h:55-179,
+ * src/gpu/TemplateMatchingCore.cu:49-368) and the host merge that consumes its
+ * outputs (src/programs/match_template/match_template.cpp:918-986).  Unlike the
+ * reference GPU path, slice extraction, filtering, normalisation and both
+ * micrograph-size FFTs run on the device, and the numerics follow the
+ * reference CPU path (match_template.cpp:996-1166), which is the parity target.
+ *
+ * All entry points take plain pointers and sizes, return an int status
+ * (TM_OK = 0, negative on error) and never abort the process.  Host buffers
+ * belong to the caller and are copied during the call.  One context drives one
+ * GPU from one host thread.
+ */
+#ifndef TM_B200_H
+#define TM_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define TM_API __attribute__((visibility("default")))
+#else
+#define TM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TM_OK 0
+#define TM_ERR_INVALID (-1)      /* bad argument or call order */
+#define TM_ERR_CUDA (-2)         /* CUDA runtime error (message in tm_last_error) */
+#define TM_ERR_UNSUPPORTED (-3)  /* geometry without a compiled kernel variant */
+#define TM_ERR_OOM (-4)          /* device allocation failed */
+#define TM_ERR_TIMEOUT (-5)      /* a bounded wait ran out */
+#define TM_ERR_CANCELLED (-6)    /* the progress callback asked to stop */
+
+typedef struct tm_ctx tm_ctx;
+
+/* Geometry and histogram set-up.  Mirrors the sizes and histogram arguments of
+ * TemplateMatchingCore::Init (TemplateMatchingCore.h:147-171):
+ * image_x/image_y are the padded (factorised) micrograph dimensions of
+ * input_image, template_size the cubic box of template_reconstruction,
+ * histogram_min_scaled / histogram_step_scaled / histogram_bins the values of
+ * match_template.cpp:633-644. */
+typedef struct tm_dims {
+    int image_x;
+    int image_y;
+    int template_size;
+    int histogram_bins;            /* 512 in the reference */
+    double histogram_min_scaled;   /* histogram_min / sqrt(X*Y) */
+    double histogram_step_scaled;  /* histogram_step / sqrt(X*Y) */
+    int orientation_batch;         /* orientations per device pass; 0 = default */
+    int device;                    /* CUDA device ordinal */
+} tm_dims;
+
+/* Called after each device pass with the number of orientations finished in
+ * the current plane; a non-zero return cancels the plane (TM_ERR_CANCELLED). */
+typedef int (*tm_progress_fn)(long long orientations_done, long long orientations_total, void *user);
+
+/* Replaces TemplateMatchingCore::Init's device set-up (TemplateMatchingCore.cu:49-138):
+ * allocates every device buffer for the geometry.  Status TM_ERR_UNSUPPORTED
+ * if no kernel variant exists for (image_x, image_y, template_size). */
+TM_API int tm_create(const tm_dims *dims, tm_ctx **out);
+
+/* Uploads the template spectrum: the quadrant-swapped Fourier transform of the
+ * template volume exactly as match_template.cpp:842-845 leaves it in
+ * template_reconstruction (ChangePixelSize(..., return_fft=true),
+ * ZeroCentralPixel, SwapRealSpaceQuadrants).  spectrum: T*T*(T/2+1) complex
+ * values as interleaved float pairs, layout [z][y][x]. */
+TM_API int tm_set_template(tm_ctx *ctx, const float *spectrum, int template_size);
+
+/* Uploads the whitened micrograph spectrum (input_image.complex_values after
+ * match_template.cpp:703-724): image_y*(image_x/2+1) complex values as
+ * interleaved float pairs, layout [y][x]. */
+TM_API int tm_set_image(tm_ctx *ctx, const float *spectrum, int image_x, int image_y);
+
+/* Clears the running MIP (to -FLT_MAX), best-orientation, sum, sum-of-squares
+ * and histogram state, as RunInnerLoop does at entry (TemplateMatchingCore.cu:143-155). */
+TM_API int tm_reset_results(tm_ctx *ctx);
+
+/* Replaces TemplateMatchingCore::RunInnerLoop (TemplateMatchingCore.cu:140-368)
+ * for one (pixel size, defocus) plane: for every orientation in order,
+ * extract the Fourier slice, apply the projection filter (CTF x whitening,
+ * match_template.cpp:895-898; T*(T/2+1) reals, layout [y][x]), normalise,
+ * correlate with the micrograph and fold the correlation map into the running
+ * MIP / argmax / sums / histogram.  euler_angles holds n_orientations triples
+ * (phi, theta, psi) in degrees, in the reference's loop order (search
+ * position outer, psi inner).  defocus_offset / pixel_size_offset are the
+ * values recorded for pixels whose maximum comes from this plane
+ * (float(defocus_i)*defocus_step, float(size_i)*pixel_size_step).
+ * Results accumulate across planes until tm_reset_results. */
+TM_API int tm_run_plane(tm_ctx *ctx, const float *projection_filter, const float *euler_angles, int n_orientations,
+                 float defocus_offset, float pixel_size_offset, tm_progress_fn progress, void *user);
+
+/* Copies the running results to host memory (any pointer may be NULL).
+ * Maps are image_y*image_x, layout [y][x]: MIP (unscaled correlation), best
+ * psi/theta/phi (degrees), best defocus and pixel-size offsets, and the per
+ * pixel sum and sum of squares of every correlation value in double.
+ * histogram receives histogram_bins counts.  These are the outputs that
+ * match_template.cpp:918-984 reads from d_max_intensity_projection,
+ * d_best_psi/theta/phi, d_sum3, d_sumSq3 and Histogram::CopyToHostAndAdd. */
+TM_API int tm_get_results(tm_ctx *ctx, float *mip, float *best_psi, float *best_theta, float *best_phi,
+                   float *best_defocus, float *best_pixel_size, double *sum, double *sum_of_squares,
+                   long long *histogram);
+
+/* Number of correlation maps computed since the last reset
+ * (TemplateMatchingCore::total_number_of_cccs_calculated). */
+TM_API long long tm_correlations_computed(const tm_ctx *ctx);
+
+/* Device time of the last tm_run_plane call in milliseconds and its split per
+ * kernel family (for roofline accounting); any pointer may be NULL. */
+TM_API int tm_last_timing(const tm_ctx *ctx, double *total_ms, double *pass_b_ms, double *pass_c_ms, double *prep_ms);
+
+/* Frees every device buffer of the context. */
+TM_API int tm_destroy(tm_ctx *ctx);
+
+/* Message of the last error on this context (never NULL). */
+TM_API const char *tm_last_error(const tm_ctx *ctx);
+
+/* Version string of the library build. */
+TM_API const char *tm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TM_B200_H */
