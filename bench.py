@@ -133,13 +133,16 @@ def make_inputs(seed=20261204):
     return dict(X=X, Y=Y, T=w["T"], ispec=ispec, tspec=tspec, filt=filt, angles=angles, hmin=hmin, hstep=hstep)
 
 
+_PINNED = []
+
+
 def pinned_copy(a):
     """numpy array in page-locked host memory (torch is used only as the allocator)."""
     import torch
     t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+    _PINNED.append(t)
     out = t.numpy().view(a.dtype).reshape(a.shape)
     out[...] = a
-    out._keepalive = t  # noqa: SLF001
     return out
 
 

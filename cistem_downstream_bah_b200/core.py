@@ -29,7 +29,8 @@ TM_ERR_CANCELLED = -6
 
 EXPORTED = [
     "tm_create", "tm_set_template", "tm_set_image", "tm_reset_results", "tm_run_plane",
-    "tm_get_results", "tm_correlations_computed", "tm_last_timing", "tm_destroy", "tm_last_error", "tm_version",
+    "tm_get_results", "tm_correlations_computed", "tm_last_timing", "tm_debug_stage_buffers", "tm_destroy",
+    "tm_last_error", "tm_version",
 ]
 
 
@@ -78,6 +79,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.tm_correlations_computed.argtypes = [vp]
     L.tm_correlations_computed.restype = ctypes.c_longlong
     L.tm_last_timing.argtypes = [vp] + [ctypes.POINTER(ctypes.c_double)] * 4
+    L.tm_debug_stage_buffers.argtypes = [vp] * 8
     L.tm_destroy.argtypes = [vp]
     L.tm_last_error.argtypes = [vp]
     L.tm_last_error.restype = ctypes.c_char_p
@@ -153,6 +155,18 @@ class SearchCore:
         v = [ctypes.c_double() for _ in range(4)]
         self._check(self.L.tm_last_timing(self.h, *[ctypes.byref(x) for x in v]))
         return {"total_ms": v[0].value, "pass_b_ms": v[1].value, "pass_c_ms": v[2].value, "prep_ms": v[3].value}
+
+    def stage_buffers(self, projection_filter, euler_angle):
+        """Intermediates of one orientation (see tm_debug_stage_buffers)."""
+        f = np.ascontiguousarray(projection_filter, dtype=np.float32)
+        e = np.ascontiguousarray(euler_angle, dtype=np.float32).reshape(3)
+        T, hc = self.T, self.X // 2 + 1
+        out = dict(slice=np.zeros((T, T // 2 + 1), np.complex64), projection=np.zeros((T, T), np.float32),
+                   normalisation=np.zeros(2, np.float32), rows=np.zeros((T, hc), np.complex64),
+                   columns=np.zeros((self.Y, hc), np.complex64))
+        self._check(self.L.tm_debug_stage_buffers(self.h, _ptr(f), _ptr(e), _ptr(out["slice"]), _ptr(out["projection"]),
+                                                  _ptr(out["normalisation"]), _ptr(out["rows"]), _ptr(out["columns"])))
+        return out
 
     def close(self):
         if self.h and self.h.value:

@@ -90,6 +90,7 @@ struct Variant {
     int T, X, Y;
     int (*run_batch)(tm_ctx*, tmk::BatchArgs&, bool timing);
     int (*configure)(tm_ctx*);
+    int (*run_stages)(tm_ctx*, tmk::BatchArgs&);   // every kernel before the MIP epilogue
 };
 
 template <int T, int X, int Y>
@@ -99,6 +100,19 @@ struct Impl {
 
     static int configure(tm_ctx* c) {
         TM_CUDA(c, cudaFuncSetAttribute(tmk::k_pass_b<T, Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB::SMEM));
+        return TM_OK;
+    }
+
+    static int run_stages(tm_ctx* c, tmk::BatchArgs& a) {
+        cudaStream_t s = c->stream;
+        tmk::k_slice_colfft<T><<<dim3((T / 2 + 1 + 15) / 16, a.nb), T, 0, s>>>(a);
+        tmk::k_row_c2r<T><<<dim3(T / RC::ROWS, a.nb), RC::NT, 0, s>>>(a);
+        tmk::k_norm<T><<<(a.nb + 7) / 8, 256, 0, s>>>(a, (long long)X * Y);
+        tmk::k_pass_a<T, X><<<dim3(T, a.nb), X / 16, 0, s>>>(a);
+        const int n_items = (c->XP / PB::W) * a.nb;
+        tmk::k_pass_b<T, Y><<<n_items < c->nsm ? n_items : c->nsm, PB::NT, PB::SMEM, s>>>(a, n_items);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return set_err(c, TM_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
         return TM_OK;
     }
 
@@ -122,7 +136,7 @@ struct Impl {
     }
 };
 
-#define TM_VARIANT(T, X, Y) {T, X, Y, &Impl<T, X, Y>::run_batch, &Impl<T, X, Y>::configure}
+#define TM_VARIANT(T, X, Y) {T, X, Y, &Impl<T, X, Y>::run_batch, &Impl<T, X, Y>::configure, &Impl<T, X, Y>::run_stages}
 
 const Variant kVariants[] = {
     TM_VARIANT(32, 256, 256),
@@ -179,6 +193,26 @@ void free_all(tm_ctx* c) {
         if (e) cudaEventDestroy(e);
 }
 
+// The two used columns of RotationMatrix::SetToEulerRotation (matrix.cpp:490-510)
+// in float arithmetic, 6 floats per orientation: m00 m01 m10 m11 m20 m21.
+void euler_rows(const float* euler_angles, int n, float* rot) {
+    const float pif = 3.14159265359f;
+    auto d2r = [pif](float deg) { return (float)((double)(deg * pif) / 180.); };
+    for (int o = 0; o < n; o++) {
+        const float phi = euler_angles[3 * o], theta = euler_angles[3 * o + 1], psi = euler_angles[3 * o + 2];
+        const float cphi = cosf(d2r(phi)), sphi = sinf(d2r(phi));
+        const float cth = cosf(d2r(theta)), sth = sinf(d2r(theta));
+        const float cpsi = cosf(d2r(psi)), spsi = sinf(d2r(psi));
+        float* m = rot + 6 * (size_t)o;
+        m[0] = cphi * cth * cpsi - sphi * spsi;    // m[0][0]
+        m[1] = -cphi * cth * spsi - sphi * cpsi;   // m[0][1]
+        m[2] = sphi * cth * cpsi + cphi * spsi;    // m[1][0]
+        m[3] = -sphi * cth * spsi + cphi * cpsi;   // m[1][1]
+        m[4] = -sth * cpsi;                        // m[2][0]
+        m[5] = sth * spsi;                         // m[2][1]
+    }
+}
+
 tmk::BatchArgs make_args(tm_ctx* c) {
     tmk::BatchArgs a{};
     a.tmpl = c->tmpl;
@@ -221,12 +255,23 @@ int tm_create(const tm_dims* dims, tm_ctx** out) {
     c->X = dims->image_x;
     c->Y = dims->image_y;
     c->T = dims->template_size;
-    c->XP = c->X / 2 + 4;
+    {
+        // pass B processes W = 16384 / Y adjacent columns per block; the row
+        // pitch covers kx = 0 .. X/2 in whole chunks (and stays even for the
+        // 16-byte loads of pass C)
+        int W = c->Y > 0 ? 16384 / c->Y : 4;
+        if (W < 4) W = 4;
+        c->XP = (c->X / 2 + 1 + W - 1) / W * W;
+    }
     c->TP = c->T / 2 + 1;
     c->B = dims->orientation_batch > 0 ? dims->orientation_batch : 32;
     if (dims->histogram_bins <= 0 || dims->histogram_bins > 1024 || !(dims->histogram_step_scaled > 0)) {
         *out = c;
         return set_err(c, TM_ERR_INVALID, "histogram_bins must be 1..1024 and the step positive");
+    }
+    if (c->XP > c->X / 2 + 64) {
+        *out = c;
+        return set_err(c, TM_ERR_UNSUPPORTED, "image height %d too small for the column pass", c->Y);
     }
     c->var = find_variant(c->T, c->X, c->Y);
     if (!c->var) {
@@ -362,21 +407,7 @@ int tm_run_plane(tm_ctx* c, const float* projection_filter, const float* euler_a
         c->rot_capacity = n;
     }
     std::vector<float> rot((size_t)6 * n);
-    const float pif = 3.14159265359f;
-    for (int o = 0; o < n; o++) {
-        auto d2r = [pif](float deg) { return (float)((double)(deg * pif) / 180.); };
-        const float phi = euler_angles[3 * o], theta = euler_angles[3 * o + 1], psi = euler_angles[3 * o + 2];
-        const float cphi = cosf(d2r(phi)), sphi = sinf(d2r(phi));
-        const float cth = cosf(d2r(theta)), sth = sinf(d2r(theta));
-        const float cpsi = cosf(d2r(psi)), spsi = sinf(d2r(psi));
-        float* m = rot.data() + 6 * (size_t)o;
-        m[0] = cphi * cth * cpsi - sphi * spsi;    // m[0][0]
-        m[1] = -cphi * cth * spsi - sphi * cpsi;   // m[0][1]
-        m[2] = sphi * cth * cpsi + cphi * spsi;    // m[1][0]
-        m[3] = -sphi * cth * spsi + cphi * cpsi;   // m[1][1]
-        m[4] = -sth * cpsi;                        // m[2][0]
-        m[5] = sth * spsi;                         // m[2][1]
-    }
+    euler_rows(euler_angles, n, rot.data());
     TM_CUDA(c, cudaMemcpyAsync(c->rot, rot.data(), sizeof(float) * rot.size(), cudaMemcpyHostToDevice, c->stream));
     TM_CUDA(c, cudaMemcpyAsync(c->filter, projection_filter, sizeof(float) * (size_t)c->T * c->TP, cudaMemcpyHostToDevice, c->stream));
     // bookkeeping for decoding (reuse the previous angle list when identical)
@@ -503,6 +534,37 @@ int tm_last_timing(const tm_ctx* c, double* total_ms, double* pass_b_ms, double*
     if (pass_b_ms) *pass_b_ms = c->last_b_ms;
     if (pass_c_ms) *pass_c_ms = c->last_c_ms;
     if (prep_ms) *prep_ms = c->last_prep_ms;
+    return TM_OK;
+}
+
+int tm_debug_stage_buffers(tm_ctx* c, const float* projection_filter, const float* euler_angle, float* slice,
+                           float* projection, float* normalisation, float* rows, float* columns) {
+    if (!c || !projection_filter || !euler_angle) return TM_ERR_INVALID;
+    if (!c->has_template || !c->has_image) return set_err(c, TM_ERR_INVALID, "template and image must be set first");
+    TM_CUDA(c, cudaSetDevice(c->device));
+    if (c->rot_capacity < 1) {
+        int rc = dalloc(c, &c->rot, (size_t)6);
+        if (rc != TM_OK) return rc;
+        c->rot_capacity = 1;
+    }
+    float rot[6];
+    euler_rows(euler_angle, 1, rot);
+    TM_CUDA(c, cudaMemcpyAsync(c->rot, rot, sizeof rot, cudaMemcpyHostToDevice, c->stream));
+    TM_CUDA(c, cudaMemcpyAsync(c->filter, projection_filter, sizeof(float) * (size_t)c->T * c->TP, cudaMemcpyHostToDevice, c->stream));
+    tmk::BatchArgs a = make_args(c);
+    a.nb = 1;
+    a.orient0 = 0;
+    a.gidx0 = 0;
+    int rc = c->var->run_stages(c, a);
+    if (rc != TM_OK) return rc;
+    rc = wait_stream(c, 60.0);
+    if (rc != TM_OK) return rc;
+    const size_t T = c->T, TP = c->TP, XP = c->XP, hc = c->X / 2 + 1;
+    if (slice) TM_CUDA(c, cudaMemcpy(slice, c->S, sizeof(float2) * T * TP, cudaMemcpyDeviceToHost));
+    if (projection) TM_CUDA(c, cudaMemcpy(projection, c->P, sizeof(float) * T * T, cudaMemcpyDeviceToHost));
+    if (normalisation) TM_CUDA(c, cudaMemcpy(normalisation, c->norm, sizeof(float2), cudaMemcpyDeviceToHost));
+    if (rows) TM_CUDA(c, cudaMemcpy2D(rows, hc * sizeof(float2), c->A, XP * sizeof(float2), hc * sizeof(float2), T, cudaMemcpyDeviceToHost));
+    if (columns) TM_CUDA(c, cudaMemcpy2D(columns, hc * sizeof(float2), c->C, XP * sizeof(float2), hc * sizeof(float2), (size_t)c->Y, cudaMemcpyDeviceToHost));
     return TM_OK;
 }
 

@@ -1,7 +1,8 @@
 // tm_kernels.cuh -- the search kernels for one batch of orientations.
 //
 // Data flow per orientation (o) of a batch, T = template box, X x Y = padded
-// micrograph, XP = X/2 + 4 (row pitch of half-spectra, in complex values):
+// micrograph, XP = row pitch of half-spectra in complex values (X/2+1 rounded
+// up to a multiple of the pass-B column chunk):
 //
 //   k_slice_colfft   Fourier slice of the 3-D template (trilinear, Hermitian
 //                    mirror; image.cpp:2450-2607, 2899-3020) x (-1)^(i+j)
@@ -61,7 +62,8 @@ struct BatchArgs {
     unsigned long long* hist;     // hist_bins
     float hist_min, hist_inv_step;
     int hist_bins;
-    int XP;                       // row pitch (complex values) of A, C and Ip
+    int XP;                       // row pitch (complex values) of A, C and Ip: X/2+1 rounded
+                                  // up to a multiple of the pass-B column chunk
     Twiddles tw;
 };
 
@@ -157,12 +159,17 @@ k_slice_colfft(BatchArgs a) {
                     // j > 0 and j = -T/2 interpolate at (0, j); other j < 0 mirror (0, -j)
                     const int jj = (j > 0 || j == -(T / 2)) ? j : -j;
                     const float fy = (float)jj;
-                    val = interp3<T>(a.tmpl, m01 * fy, m11 * fy, m21 * fy);
+                    val = interp3<T>(a.tmpl, __fmul_rn(m01, fy), __fmul_rn(m11, fy), __fmul_rn(m21, fy));
                     if (jj != j) val.y = -val.y;
                 }
             } else {
+                // RotateCoords (matrix.h:32-37) in float without fused multiply-add,
+                // so that samples on the box boundary are kept or dropped exactly
+                // as the reference does
                 const float fx = (float)i, fy = (float)j;
-                val = interp3<T>(a.tmpl, fmaf(m00, fx, m01 * fy), fmaf(m10, fx, m11 * fy), fmaf(m20, fx, m21 * fy));
+                val = interp3<T>(a.tmpl, __fadd_rn(__fmul_rn(m00, fx), __fmul_rn(m01, fy)),
+                                 __fadd_rn(__fmul_rn(m10, fx), __fmul_rn(m11, fy)),
+                                 __fadd_rn(__fmul_rn(m20, fx), __fmul_rn(m21, fy)));
             }
             float f = __ldg(a.filter + (size_t)y * TP + i);
             if ((i + j) & 1) f = -f;
@@ -391,7 +398,7 @@ struct PassC {
     static constexpr int H = X / 2;
     static constexpr int R = 8;
     static constexpr int P = H / R;                 // X/16 threads
-    static constexpr int XP = X / 2 + 4;            // row pitch used for the C buffer
+    static constexpr int XPMAX = X / 2 + 64;        // >= the runtime row pitch of C
     static constexpr int RSF = tmfft::padded_len(H);
 };
 
@@ -399,8 +406,9 @@ template <int X>
 __global__ void __launch_bounds__(X / 16, 2)
 k_pass_c(BatchArgs a, int Y) {
     using PC = PassC<X>;
-    constexpr int H = PC::H, P = PC::P, XP = PC::XP;
-    __shared__ float2 rowbuf[XP];
+    constexpr int H = PC::H, P = PC::P;
+    const int XP = a.XP;
+    __shared__ float2 rowbuf[PC::XPMAX];
     __shared__ float2 fbuf[PC::RSF];
     __shared__ unsigned int shist[1024];
     const int t = threadIdx.x;

@@ -114,6 +114,18 @@ TM_API long long tm_correlations_computed(const tm_ctx *ctx);
  * kernel family (for roofline accounting); any pointer may be NULL. */
 TM_API int tm_last_timing(const tm_ctx *ctx, double *total_ms, double *pass_b_ms, double *pass_c_ms, double *prep_ms);
 
+/* Runs one orientation through every kernel up to the column pass, leaving
+ * the running results untouched, and copies the intermediates (any pointer
+ * may be NULL): slice = filtered Fourier slice after the inverse FFT along y
+ * (T*(T/2+1) complex, [y][x]); projection = real T*T projection before
+ * normalisation; normalisation = (edge mean, 1/sigma) as in
+ * match_template.cpp:1060-1068; rows = forward FFT along x of the T
+ * normalised rows (T*(X/2+1) complex); columns = the correlation spectrum
+ * after the inverse FFT along y (Y*(X/2+1) complex).  For kernel-level
+ * parity tests and diagnostics; it has no counterpart in the reference. */
+TM_API int tm_debug_stage_buffers(tm_ctx *ctx, const float *projection_filter, const float *euler_angle, float *slice,
+                                  float *projection, float *normalisation, float *rows, float *columns);
+
 /* Frees every device buffer of the context. */
 TM_API int tm_destroy(tm_ctx *ctx);
 

@@ -593,19 +593,25 @@ EXPORT void orc_extract_slice(int T, const real *vol, const float *m, real *out)
     const int uby = T % 2 == 0 ? T / 2 - 1 : (T - 1) / 2;
     const int ubx = T % 2 == 0 ? T / 2 : (T - 1) / 2;
     double vr, vi;
+    /* RotateCoords (matrix.h:32-37) evaluates the rotated coordinates in float;
+     * their floor() decides which samples fall outside the box, so they are
+     * computed here with the same float operations (no fused multiply-add). */
     for (int j = lby; j <= uby; j++) {
         int py = j >= 0 ? j : T + j;
         for (int i = 1; i <= ubx; i++) {
-            real x3 = (real)m[0] * i + (real)m[1] * j;
-            real y3 = (real)m[3] * i + (real)m[4] * j;
-            real z3 = (real)m[6] * i + (real)m[7] * j;
+            const float fi = (float)i, fj = (float)j;
+            volatile float px0 = m[0] * fi, px1 = m[1] * fj;
+            volatile float py0 = m[3] * fi, py1 = m[4] * fj;
+            volatile float pz0 = m[6] * fi, pz1 = m[7] * fj;
+            float x3 = px0 + px1, y3 = py0 + py1, z3 = pz0 + pz1;
             interp3(T, vol, x3, y3, z3, &vr, &vi);
             out[2 * ((size_t)py * hc + i)] = (real)vr;
             out[2 * ((size_t)py * hc + i) + 1] = (real)vi;
         }
     }
     for (int j = 1; j <= uby; j++) {
-        real x3 = (real)m[1] * j, y3 = (real)m[4] * j, z3 = (real)m[7] * j;
+        const float fj = (float)j;
+        float x3 = m[1] * fj, y3 = m[4] * fj, z3 = m[7] * fj;
         interp3(T, vol, x3, y3, z3, &vr, &vi);
         out[2 * ((size_t)j * hc)] = (real)vr;
         out[2 * ((size_t)j * hc) + 1] = (real)vi;
@@ -614,7 +620,8 @@ EXPORT void orc_extract_slice(int T, const real *vol, const float *m, real *out)
     }
     if (-lby != uby) {
         int j = lby;
-        real x3 = (real)m[1] * j, y3 = (real)m[4] * j, z3 = (real)m[7] * j;
+        const float fj = (float)j;
+        float x3 = m[1] * fj, y3 = m[4] * fj, z3 = m[7] * fj;
         interp3(T, vol, x3, y3, z3, &vr, &vi);
         int py = T + j;
         out[2 * ((size_t)py * hc)] = (real)vr;
