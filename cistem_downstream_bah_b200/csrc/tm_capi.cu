@@ -49,6 +49,7 @@ struct tm_ctx {
     int* best = nullptr;
     double *sum = nullptr, *sumsq = nullptr;
     unsigned long long* hist = nullptr;
+    int* err_flag = nullptr;
     int lmax = 0;
     long long rot_capacity = 0;
     bool has_template = false, has_image = false;
@@ -98,8 +99,12 @@ struct Impl {
     using PB = tmk::PassB<T, Y>;
     using RC = tmk::RowC2R<T>;
 
+    using PCc = tmk::PassC<X>;
+
     static int configure(tm_ctx* c) {
         TM_CUDA(c, cudaFuncSetAttribute(tmk::k_pass_b<T, Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB::SMEM));
+        TM_CUDA(c, cudaFuncSetAttribute(tmk::k_pass_c<X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)PCc::smem_bytes(c->XP, c->d.histogram_bins)));
         return TM_OK;
     }
 
@@ -128,7 +133,7 @@ struct Impl {
         const int grid = n_items < c->nsm ? n_items : c->nsm;
         tmk::k_pass_b<T, Y><<<grid, PB::NT, PB::SMEM, s>>>(a, n_items);
         if (timing) cudaEventRecord(c->ev_b, s);
-        tmk::k_pass_c<X><<<Y, X / 16, 0, s>>>(a, Y);
+        tmk::k_pass_c<X><<<Y, X / 16, PCc::smem_bytes(c->XP, a.hist_bins), s>>>(a, Y);
         if (timing) cudaEventRecord(c->ev_c, s);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return set_err(c, TM_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
@@ -184,7 +189,7 @@ int wait_stream(tm_ctx* c, double limit_s) {
 
 void free_all(tm_ctx* c) {
     void* ptrs[] = {c->tmpl, c->Ip, c->S, c->A, c->C, c->norm, c->twid, c->P, c->filter, c->rot,
-                    c->rowstat, c->mip, c->best, c->sum, c->sumsq, c->hist};
+                    c->rowstat, c->mip, c->best, c->sum, c->sumsq, c->hist, c->err_flag};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -234,6 +239,7 @@ tmk::BatchArgs make_args(tm_ctx* c) {
     a.hist_inv_step = (float)(1.0 / c->d.histogram_step_scaled);
     a.hist_bins = c->d.histogram_bins;
     a.XP = c->XP;
+    a.err = c->err_flag;
     a.tw.tab = c->twid;
     a.tw.lmax = c->lmax;
     return a;
@@ -260,6 +266,7 @@ int tm_create(const tm_dims* dims, tm_ctx** out) {
         // pitch covers kx = 0 .. X/2 in whole chunks (and stays even for the
         // 16-byte loads of pass C)
         int W = c->Y > 0 ? 16384 / c->Y : 4;
+        if (W > 16) W = 16;
         if (W < 4) W = 4;
         c->XP = (c->X / 2 + 1 + W - 1) / W * W;
     }
@@ -311,6 +318,11 @@ int tm_create(const tm_dims* dims, tm_ctx** out) {
     TRY(dalloc(c, &c->sum, X * Y));
     TRY(dalloc(c, &c->sumsq, X * Y));
     TRY(dalloc(c, &c->hist, (size_t)1024));
+    TRY(dalloc(c, &c->err_flag, (size_t)1));
+    {
+        cudaError_t e = cudaMemset(c->err_flag, 0, sizeof(int));
+        if (e != cudaSuccess) { *out = c; return set_err(c, TM_ERR_CUDA, "memset: %s", cudaGetErrorString(e)); }
+    }
     // A's columns beyond X/2 are never written by the kernels and must read as zero
     {
         cudaError_t e = cudaMemsetAsync(c->A, 0, B * T * XP * sizeof(float2), c->stream);
@@ -467,6 +479,14 @@ int tm_run_plane(tm_ctx* c, const float* projection_filter, const float* euler_a
     TM_CUDA(c, cudaEventRecord(c->ev_c, c->stream));
     int w = wait_stream(c, 3600.0);
     if (w != TM_OK) return w;
+    {
+        int flag = 0;
+        TM_CUDA(c, cudaMemcpy(&flag, c->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+        if (flag) {
+            cudaMemset(c->err_flag, 0, sizeof(int));
+            return set_err(c, TM_ERR_TIMEOUT, "a bulk copy did not complete within its wait limit; results of this plane are invalid");
+        }
+    }
     float tot = 0;
     cudaEventElapsedTime(&tot, c->ev_start, c->ev_c);
     // per-orientation averages of the sampled batches, scaled to the plane

@@ -37,6 +37,21 @@ __device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.
 __device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
 __host__ __device__ constexpr int padded_len(int L) { return L + L / 16; }
 
+// pad16(t + P*r) as a base plus a compile-time offset per r (0 <= t < P, P a
+// multiple or a divisor of 16), so the 16 addresses need one register
+template <int P>
+__device__ __forceinline__ int rd_base(int t) { return (P % 16 == 0) ? t + (t >> 4) : t; }
+template <int P>
+__host__ __device__ constexpr int rd_off(int r) { return (P % 16 == 0) ? r * (P + P / 16) : P * r + ((P * r) >> 4); }
+
+// pad16(idxD + r*Ns) for the Stockham write of a stage with one radix-R
+// butterfly per thread (b = t): idxD = (t/Ns)*Ns*R + t%Ns; Ns == 1 or a multiple of 16
+template <int R>
+__device__ __forceinline__ int wr_base(int t, int Ns) {
+    return Ns == 1 ? pad16(R * t) : pad16((t / Ns) * Ns * R + (t % Ns));
+}
+__host__ __device__ constexpr int wr_off(int r, int Ns) { return Ns == 1 ? r : r * (Ns + Ns / 16); }
+
 template <int DIR>
 __device__ __forceinline__ void dft2(float2& a, float2& b) {
     float2 t = a;
@@ -136,6 +151,43 @@ __device__ __forceinline__ void powers(float2 w, float2* p) {
     }
 }
 
+// e[r] *= w^r for r = 1..RS-1.  The powers come from a shallow product tree
+// (depth <= 4) computed next to their use, so few of them are live at once.
+template <int RS>
+__device__ __forceinline__ void apply_twiddles(float2* e, float2 w) {
+    if constexpr (RS == 2) {
+        e[1] = cmul(e[1], w);
+    } else if constexpr (RS == 4) {
+        const float2 w2 = cmul(w, w);
+        e[1] = cmul(e[1], w);
+        e[2] = cmul(e[2], w2);
+        e[3] = cmul(e[3], cmul(w2, w));
+    } else {
+        const float2 w2 = cmul(w, w);
+        const float2 w3 = cmul(w2, w);
+        const float2 w4 = cmul(w2, w2);
+        e[1] = cmul(e[1], w);
+        e[2] = cmul(e[2], w2);
+        e[3] = cmul(e[3], w3);
+        e[4] = cmul(e[4], w4);
+        e[5] = cmul(e[5], cmul(w4, w));
+        e[6] = cmul(e[6], cmul(w4, w2));
+        e[7] = cmul(e[7], cmul(w4, w3));
+        if constexpr (RS == 16) {
+            const float2 w8 = cmul(w4, w4);
+            e[8] = cmul(e[8], w8);
+            e[9] = cmul(e[9], cmul(w8, w));
+            e[10] = cmul(e[10], cmul(w8, w2));
+            e[11] = cmul(e[11], cmul(w8, w3));
+            const float2 w12 = cmul(w8, w4);
+            e[12] = cmul(e[12], w12);
+            e[13] = cmul(e[13], cmul(w12, w));
+            e[14] = cmul(e[14], cmul(w12, w2));
+            e[15] = cmul(e[15], cmul(w12, w3));
+        }
+    }
+}
+
 // Twiddle source: a table of W_LMAX^m = exp(-2 pi i m / LMAX), m = 0..LMAX-1,
 // for one power-of-two LMAX; W_L^m = table[m * (LMAX / L)].
 struct Twiddles {
@@ -175,8 +227,9 @@ __device__ __forceinline__ void fft(float2 (&v)[R], int t, float2* buf, const Tw
         if (s > 0) {
             // load stage input: x[t + P*r]
             sync();
+            const float2* rb = buf + rd_base<P>(t);
 #pragma unroll
-            for (int r = 0; r < R; r++) v[r] = buf[pad16(t + P * r)];
+            for (int r = 0; r < R; r++) v[r] = rb[rd_off<P>(r)];
         }
         // butterflies: thread does R/RS of them, b = t + P*u, elements v[u + r*(R/RS)]
 #pragma unroll
@@ -187,11 +240,11 @@ __device__ __forceinline__ void fft(float2 (&v)[R], int t, float2* buf, const Tw
             for (int r = 0; r < RS; r++) e[r] = v[u + r * (R / RS)];
             if (s > 0) {
                 const int jm = b % Ns;
-                float2 w = tw.template w<DIR>(jm * (L / (Ns * RS)), L);
-                float2 p[16];
-                powers<16>(w, p);
-#pragma unroll
-                for (int r = 1; r < RS; r++) e[r] = cmul(e[r], p[r]);
+                const float2 w = tw.template w<DIR>(jm * (L / (Ns * RS)), L);
+                if (RS == 16) apply_twiddles<16>(e, w);
+                else if (RS == 8) apply_twiddles<8>(e, w);
+                else if (RS == 4) apply_twiddles<4>(e, w);
+                else if (RS == 2) apply_twiddles<2>(e, w);
             }
             if (RS == 16) dft16<DIR>(e);
             else if (RS == 8) dft8<DIR>(e);
@@ -202,10 +255,72 @@ __device__ __forceinline__ void fft(float2 (&v)[R], int t, float2* buf, const Tw
                 for (int r = 0; r < RS; r++) v[u + r * (R / RS)] = e[r];
             } else {
                 if (u == 0) sync();  // previous readers of buf are done
-                const int idxD = (b / Ns) * Ns * RS + (b % Ns);
+                if (RS == R && (Ns == 1 || Ns % 16 == 0)) {
+                    float2* wb = buf + wr_base<R>(b, Ns);
 #pragma unroll
-                for (int r = 0; r < RS; r++) buf[pad16(idxD + r * Ns)] = e[r];
+                    for (int r = 0; r < RS; r++) wb[wr_off(r, Ns)] = e[r];
+                } else {
+                    const int idxD = (b / Ns) * Ns * RS + (b % Ns);
+#pragma unroll
+                    for (int r = 0; r < RS; r++) buf[pad16(idxD + r * Ns)] = e[r];
+                }
             }
+        }
+        Ns *= RS;
+    }
+}
+
+// Same transform as fft(), with the exchanges done through a float buffer of
+// padded_len(L) entries: real parts first, then imaginary parts.  Uses half
+// the shared memory of fft() at the cost of two extra barriers per exchange.
+template <int L, int R, int DIR, class Sync>
+__device__ __forceinline__ void fft_split(float2 (&v)[R], int t, float* buf, const Twiddles& tw, Sync sync) {
+    using PL = Plan<L, R>;
+    constexpr int P = PL::P;
+    int Ns = 1;
+#pragma unroll
+    for (int s = 0; s < PL::stages; s++) {
+        const int RS = PL::radix(s);
+        const bool last = (s == PL::stages - 1);
+#pragma unroll
+        for (int u = 0; u < R / (RS > 0 ? RS : 1); u++) {
+            const int b = t + P * u;
+            float2 e[16];
+#pragma unroll
+            for (int r = 0; r < RS; r++) e[r] = v[u + r * (R / RS)];
+            if (s > 0) {
+                const int jm = b % Ns;
+                const float2 w = tw.template w<DIR>(jm * (L / (Ns * RS)), L);
+                if (RS == 16) apply_twiddles<16>(e, w);
+                else if (RS == 8) apply_twiddles<8>(e, w);
+                else if (RS == 4) apply_twiddles<4>(e, w);
+                else if (RS == 2) apply_twiddles<2>(e, w);
+            }
+            if (RS == 16) dft16<DIR>(e);
+            else if (RS == 8) dft8<DIR>(e);
+            else if (RS == 4) dft4<DIR>(e[0], e[1], e[2], e[3]);
+            else if (RS == 2) dft2<DIR>(e[0], e[1]);
+#pragma unroll
+            for (int r = 0; r < RS; r++) v[u + r * (R / RS)] = e[r];
+        }
+        if (!last) {
+            // the next stage reads x[t + P*r]; this stage wrote (b/Ns)*Ns*Rs + b%Ns + r*Ns
+            // (non-last stages use RS == R, one butterfly per thread, b = t)
+            float* wb = buf + wr_base<R>(t, Ns);
+            const float* rb = buf + rd_base<P>(t);
+            float nre[R];
+            sync();
+#pragma unroll
+            for (int r = 0; r < R; r++) wb[wr_off(r, Ns)] = v[r].x;
+            sync();
+#pragma unroll
+            for (int r = 0; r < R; r++) nre[r] = rb[rd_off<P>(r)];
+            sync();
+#pragma unroll
+            for (int r = 0; r < R; r++) wb[wr_off(r, Ns)] = v[r].y;
+            sync();
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = make_float2(nre[r], rb[rd_off<P>(r)]);
         }
         Ns *= RS;
     }

@@ -30,6 +30,7 @@
 #pragma once
 #include <float.h>
 #include "tm_fft.cuh"
+#include "tm_ptx.cuh"
 
 namespace tmk {
 
@@ -62,6 +63,7 @@ struct BatchArgs {
     unsigned long long* hist;     // hist_bins
     float hist_min, hist_inv_step;
     int hist_bins;
+    int* err;                     // device error flag (a bounded wait ran out)
     int XP;                       // row pitch (complex values) of A, C and Ip: X/2+1 rounded
                                   // up to a multiple of the pass-B column chunk
     Twiddles tw;
@@ -328,65 +330,104 @@ k_pass_a(BatchArgs a) {
 
 // --------------------------------------------------------------------------------------
 // k_pass_b: persistent; block = W columns x Y/16 threads (thread = c + W*j);
-// work item = (column chunk, orientation), orientation fastest.
+// work item = (column chunk, orientation), orientation fastest, so a block
+// keeps its chunk of the prepared micrograph spectrum I' in shared memory for
+// all orientations of the batch.  Exchanges go through a float buffer (real,
+// then imaginary parts) to leave room for I'; the rows of A for the next item
+// stream in with cp.async while the current item is transformed.
 template <int T, int Y>
 struct PassB {
-    static constexpr int W = 16384 / Y;               // columns per block
-    static constexpr int NT = W * (Y / 16);           // 1024 threads
+    static constexpr int W = (16384 / Y) < 16 ? (16384 / Y) : 16;   // columns per block
+    static constexpr int NT = W * (Y / 16);                         // threads per block
     static constexpr int MY = Y / T, PT = T / 16;
-    static constexpr int RST = skewed(tmfft::padded_len(T), 1);
+    static constexpr int RST = tmfft::padded_len(T) | 1;            // odd: forward regions on distinct banks
     static constexpr int CS0 = (MY * RST > tmfft::padded_len(Y)) ? MY * RST : tmfft::padded_len(Y);
-    static constexpr int CS = round_up16(CS0) + 16 / W;  // column stride, = 16/W mod 16
-    static constexpr size_t SMEM = sizeof(float2) * ((size_t)W * CS + (size_t)T * W);
+    static constexpr int CSKEW = W <= 32 ? 32 / W : 1;              // column regions on distinct banks
+    static constexpr int CS = (CS0 + 31) / 32 * 32 + CSKEW;          // floats per column region
+    static constexpr size_t EXCH = (sizeof(float) * W * CS + 15) / 16 * 16;
+    static constexpr size_t IPB = sizeof(float2) * 16 * NT;         // I' values, 16 per thread
+    static constexpr size_t ASZ = sizeof(float2) * T * W;           // one A staging buffer
+    // double-buffer the rows of A when shared memory allows
+    static constexpr int ABUFS = (EXCH + IPB + 2 * ASZ <= 232448) ? 2 : 1;
+    static constexpr size_t SMEM = EXCH + IPB + ABUFS * ASZ;
+    static_assert(SMEM <= 232448, "pass B shared memory exceeds the per-block limit");
 };
 
 template <int T, int Y>
-__global__ void __launch_bounds__(1024, 1)
+__global__ void __launch_bounds__(PassB<T, Y>::NT, 1)
 k_pass_b(BatchArgs a, int n_items) {
     using PB = PassB<T, Y>;
-    constexpr int W = PB::W, MY = PB::MY, PT = PB::PT;
+    constexpr int W = PB::W, MY = PB::MY, PT = PB::PT, NT = PB::NT;
     const int XP = a.XP;
-    extern __shared__ float2 smem_b[];
-    float2* cols = smem_b;
-    float2* Asm = smem_b + (size_t)W * PB::CS;
-    const int c = threadIdx.x % W, j = threadIdx.x / W;
+    extern __shared__ __align__(16) unsigned char smem_b[];
+    float* exch = reinterpret_cast<float*>(smem_b);
+    float2* ipv = reinterpret_cast<float2*>(smem_b + PB::EXCH);
+    float2* abuf = ipv + 16 * NT;
+    const int tid = threadIdx.x;
+    const int c = tid % W, j = tid / W;
     const int s = j % MY, tp = j / MY;
-    float2* colbuf = cols + (size_t)c * PB::CS;
-    float2* fwdbuf = colbuf + s * PB::RST;
-    // twiddles of the pruned forward: W_Y^(s * (tp + PT*r))
-    const float2 w0 = a.tw.template w<-1>(s * tp, Y);
-    const float2 w1 = a.tw.template w<-1>(s * PT, Y);
+    float* colbuf = exch + c * PB::CS;
+    float* fwdbuf = colbuf + s * PB::RST;
     auto sync = [] __device__() { __syncthreads(); };
     const int per = (n_items + gridDim.x - 1) / gridDim.x;
     const int it0 = blockIdx.x * per;
     const int it1 = min(n_items, it0 + per);
+    if (it0 >= it1) return;
+    auto issue_rows = [&](int it, float2* dst) {
+        const int ch = it / a.nb, oo = it % a.nb;
+        const float2* src = a.A + (size_t)oo * T * XP + ch * W;
+        for (int e = tid; e < T * W; e += NT) tmptx::cp_async8(dst + e, src + (size_t)(e / W) * XP + (e % W));
+    };
+    if (PB::ABUFS == 2) {
+        issue_rows(it0, abuf);
+        tmptx::cp_async_commit();
+    }
+    int cur_chunk = -1;
     for (int it = it0; it < it1; it++) {
+        const int kk = it - it0;
+        const float2* acur = abuf + (PB::ABUFS == 2 ? (kk & 1) : 0) * (T * W);
+        float2* anext = abuf + (PB::ABUFS == 2 ? ((kk + 1) & 1) : 0) * (T * W);
         const int chunk = it / a.nb, o = it % a.nb;
         const int kx0 = chunk * W;
-        __syncthreads();  // previous item finished with Asm / cols
-        const float2* Ao = a.A + (size_t)o * T * XP + kx0;
-        for (int e = threadIdx.x; e < T * W; e += PB::NT) Asm[e] = Ao[(size_t)(e / W) * XP + (e % W)];
-        __syncthreads();
+        __syncthreads();  // the previous item is done with the staging and exchange buffers
+        if (PB::ABUFS == 2) {
+            if (it + 1 < it1) issue_rows(it + 1, anext);
+            tmptx::cp_async_commit();
+            tmptx::cp_async_wait<1>();
+        } else {
+            issue_rows(it, anext);
+            tmptx::cp_async_commit();
+            tmptx::cp_async_wait<0>();
+        }
+        __syncthreads();  // this item's rows of A are visible to every thread
+        if (chunk != cur_chunk) {
+            // thread-private copy of the 16 I' values this thread multiplies with
+            const float2* Ic = a.Ip + kx0 + c;
+#pragma unroll
+            for (int r = 0; r < 16; r++) ipv[r * NT + tid] = __ldg(Ic + (size_t)(j + (Y / 16) * r) * XP);
+            cur_chunk = chunk;
+        }
         float2 v[16];
-        float2 w = w0;
+        {
+            // twiddles of the pruned forward: W_Y^(s * (tp + PT*r))
+            float2 w = a.tw.template w<-1>(s * tp, Y);
+            const float2 w1 = a.tw.template w<-1>(s * PT, Y);
 #pragma unroll
-        for (int r = 0; r < 16; r++) {
-            v[r] = cmul(Asm[(tp + PT * r) * W + c], w);
-            w = cmul(w, w1);
+            for (int r = 0; r < 16; r++) {
+                v[r] = cmul(acur[(tp + PT * r) * W + c], w);
+                w = cmul(w, w1);
+            }
         }
-        tmfft::fft<T, 16, -1>(v, tp, fwdbuf, a.tw, sync);
+        tmfft::fft_split<T, 16, -1>(v, tp, fwdbuf, a.tw, sync);
         // thread (s, tp) holds F[k], k = s + MY*(tp + PT*r) = j + (Y/16)*r
-        const float2* Ic = a.Ip + kx0 + c;
 #pragma unroll
-        for (int r = 0; r < 16; r++) {
-            const int k = j + (Y / 16) * r;
-            v[r] = cmul_conj(__ldg(Ic + (size_t)k * XP), v[r]);
-        }
-        tmfft::fft<Y, 16, +1>(v, j, colbuf, a.tw, sync);
+        for (int r = 0; r < 16; r++) v[r] = cmul_conj(ipv[r * NT + tid], v[r]);
+        tmfft::fft_split<Y, 16, +1>(v, j, colbuf, a.tw, sync);
         float2* Co = a.C + (size_t)o * Y * XP + kx0 + c;
 #pragma unroll
         for (int r = 0; r < 16; r++) Co[(size_t)(j + (Y / 16) * r) * XP] = v[r];
     }
+    tmptx::cp_async_wait<0>();
 }
 
 // --------------------------------------------------------------------------------------
@@ -398,8 +439,9 @@ struct PassC {
     static constexpr int H = X / 2;
     static constexpr int R = 8;
     static constexpr int P = H / R;                 // X/16 threads
-    static constexpr int XPMAX = X / 2 + 64;        // >= the runtime row pitch of C
     static constexpr int RSF = tmfft::padded_len(H);
+    // dynamic shared memory for a row pitch XP and `bins` histogram bins
+    static size_t smem_bytes(int XP, int bins) { return 128 + sizeof(float2) * (2 * (size_t)XP + RSF) + 4 * (size_t)bins; }
 };
 
 template <int X>
@@ -407,13 +449,29 @@ __global__ void __launch_bounds__(X / 16, 2)
 k_pass_c(BatchArgs a, int Y) {
     using PC = PassC<X>;
     constexpr int H = PC::H, P = PC::P;
+    constexpr uint32_t kWaitLimit = 1u << 24;
     const int XP = a.XP;
-    __shared__ float2 rowbuf[PC::XPMAX];
-    __shared__ float2 fbuf[PC::RSF];
-    __shared__ unsigned int shist[1024];
+    // rows of C stream in through 1-D bulk copies, double buffered: the copy
+    // of orientation o+1 runs while orientation o is transformed.
+    // dynamic shared memory: mbarriers | row buffer 0 | row buffer 1 | FFT buffer | histogram
+    extern __shared__ __align__(128) unsigned char smem_c[];
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_c);
+    float2* const rows = reinterpret_cast<float2*>(smem_c + 128);   // two buffers of XP
+    float2* fbuf = rows + 2 * XP;
+    unsigned int* shist = reinterpret_cast<unsigned int*>(fbuf + PC::RSF);
     const int t = threadIdx.x;
     const int y = blockIdx.x;
+    const uint32_t row_bytes = (uint32_t)XP * (uint32_t)sizeof(float2);
+    if (t == 0) {
+        tmptx::mbar_init(&mbar[0], 1);
+        tmptx::mbar_init(&mbar[1], 1);
+    }
     for (int b = t; b < a.hist_bins; b += P) shist[b] = 0u;
+    __syncthreads();
+    if (t == 0 && a.nb > 0) {
+        tmptx::mbar_arrive_expect_tx(&mbar[0], row_bytes);
+        tmptx::bulk_g2s(rows, a.C + (size_t)y * XP, row_bytes, &mbar[0]);
+    }
     float mip[16];
     int best[16];
     float fs[16], fq[16];
@@ -429,17 +487,25 @@ k_pass_c(BatchArgs a, int Y) {
         fq[2 * r] = 0.f; fq[2 * r + 1] = 0.f;
     }
     auto sync = [] __device__() { __syncthreads(); };
+    bool timed_out = false;
     for (int o = 0; o < a.nb; o++) {
-        const float4* src = reinterpret_cast<const float4*>(a.C + ((size_t)o * Y + y) * XP);
-        float4* dst = reinterpret_cast<float4*>(rowbuf);
-        for (int e = t; e < XP / 2; e += P) dst[e] = __ldg(src + e);
-        __syncthreads();
+        const int buf = o & 1;
+        __syncthreads();  // iteration o-1 is done with row buffer buf ^ 1
+        if (t == 0 && o + 1 < a.nb) {
+            tmptx::mbar_arrive_expect_tx(&mbar[buf ^ 1], row_bytes);
+            tmptx::bulk_g2s(rows + (buf ^ 1) * XP, a.C + ((size_t)(o + 1) * Y + y) * XP, row_bytes, &mbar[buf ^ 1]);
+        }
+        if (!tmptx::mbar_wait_bounded(&mbar[buf], (o >> 1) & 1, kWaitLimit)) {
+            timed_out = true;
+            atomicExch(a.err, 1);
+        }
+        const float2* rb = rows + buf * XP;
         float2 v[8];
 #pragma unroll
         for (int r = 0; r < 8; r++) {
             const int k = t + P * r;
-            float2 hk = rowbuf[k];
-            float2 hm = rowbuf[H - k];
+            float2 hk = rb[k];
+            float2 hm = rb[H - k];
             if (k == 0) { hk.y = 0.f; hm.y = 0.f; }
             const float2 e = make_float2(hk.x + hm.x, hk.y - hm.y);
             const float2 d = make_float2(hk.x - hm.x, hk.y + hm.y);
@@ -461,6 +527,12 @@ k_pass_c(BatchArgs a, int Y) {
                 if (bin >= 0 && bin < a.hist_bins) atomicAdd(&shist[bin], 1u);
             }
         }
+    }
+    if (timed_out) {
+        // leave no bulk copy in flight into this block's shared memory
+        tmptx::mbar_wait_bounded(&mbar[0], 0, kWaitLimit);
+        tmptx::mbar_wait_bounded(&mbar[1], 0, kWaitLimit);
+        return;
     }
 #pragma unroll
     for (int r = 0; r < 8; r++) {
