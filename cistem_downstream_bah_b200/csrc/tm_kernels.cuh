@@ -330,27 +330,29 @@ k_pass_a(BatchArgs a) {
 
 // --------------------------------------------------------------------------------------
 // k_pass_b: persistent; block = W columns x Y/16 threads (thread = c + W*j);
-// work item = (column chunk, orientation), orientation fastest, so a block
-// keeps its chunk of the prepared micrograph spectrum I' in shared memory for
-// all orientations of the batch.  Exchanges go through a float buffer (real,
-// then imaginary parts) to leave room for I'; the rows of A for the next item
-// stream in with cp.async while the current item is transformed.
+// work item = (column chunk, orientation), orientation fastest.  Each thread
+// parks the 16 values of the prepared micrograph spectrum I' it multiplies
+// with in tensor memory (TMEM, 32 columns of its lane) for all orientations of
+// the chunk, which leaves shared memory to full complex exchange buffers.  The
+// rows of A for the next item stream in with cp.async while the current item
+// is transformed.
 template <int T, int Y>
 struct PassB {
     static constexpr int W = (16384 / Y) < 16 ? (16384 / Y) : 16;   // columns per block
     static constexpr int NT = W * (Y / 16);                         // threads per block
     static constexpr int MY = Y / T, PT = T / 16;
-    static constexpr int RST = tmfft::padded_len(T) | 1;            // odd: forward regions on distinct banks
+    // bank skews (float2 units, half-warp = 16 lanes = (16/W) values of j x W columns)
+    static constexpr int RST = (tmfft::padded_len(T) + 15) / 16 * 16 + 1;       // == 1 (mod 16)
     static constexpr int CS0 = (MY * RST > tmfft::padded_len(Y)) ? MY * RST : tmfft::padded_len(Y);
-    static constexpr int CSKEW = W <= 32 ? 32 / W : 1;              // column regions on distinct banks
-    static constexpr int CS = (CS0 + 31) / 32 * 32 + CSKEW;          // floats per column region
-    static constexpr size_t EXCH = (sizeof(float) * W * CS + 15) / 16 * 16;
-    static constexpr size_t IPB = sizeof(float2) * 16 * NT;         // I' values, 16 per thread
+    static constexpr int CS = (CS0 + 15) / 16 * 16 + 16 / W;                  // == 16/W (mod 16)
+    static constexpr size_t EXCH = (sizeof(float2) * W * CS + 15) / 16 * 16;
     static constexpr size_t ASZ = sizeof(float2) * T * W;           // one A staging buffer
-    // double-buffer the rows of A when shared memory allows
-    static constexpr int ABUFS = (EXCH + IPB + 2 * ASZ <= 232448) ? 2 : 1;
-    static constexpr size_t SMEM = EXCH + IPB + ABUFS * ASZ;
+    static constexpr int ABUFS = (EXCH + 2 * ASZ + 64 <= 232448) ? 2 : 1;
+    static constexpr size_t SMEM = EXCH + ABUFS * ASZ + 64;         // + TMEM address slot
+    // TMEM: 32 columns per thread, NT/128 threads share a lane
+    static constexpr uint32_t TMEM_COLS = (NT / 128) * 32 < 32 ? 32 : (NT / 128) * 32;
     static_assert(SMEM <= 232448, "pass B shared memory exceeds the per-block limit");
+    static_assert(NT % 128 == 0 && TMEM_COLS <= 512, "TMEM layout needs whole warp quads");
 };
 
 template <int T, int Y>
@@ -360,19 +362,28 @@ k_pass_b(BatchArgs a, int n_items) {
     constexpr int W = PB::W, MY = PB::MY, PT = PB::PT, NT = PB::NT;
     const int XP = a.XP;
     extern __shared__ __align__(16) unsigned char smem_b[];
-    float* exch = reinterpret_cast<float*>(smem_b);
-    float2* ipv = reinterpret_cast<float2*>(smem_b + PB::EXCH);
-    float2* abuf = ipv + 16 * NT;
+    float2* exch = reinterpret_cast<float2*>(smem_b);
+    float2* abuf = reinterpret_cast<float2*>(smem_b + PB::EXCH);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem_b + PB::EXCH + PB::ABUFS * PB::ASZ);
     const int tid = threadIdx.x;
+    const int warp = tid >> 5;
     const int c = tid % W, j = tid / W;
     const int s = j % MY, tp = j / MY;
-    float* colbuf = exch + c * PB::CS;
-    float* fwdbuf = colbuf + s * PB::RST;
+    float2* colbuf = exch + c * PB::CS;
+    float2* fwdbuf = colbuf + s * PB::RST;
     auto sync = [] __device__() { __syncthreads(); };
     const int per = (n_items + gridDim.x - 1) / gridDim.x;
     const int it0 = blockIdx.x * per;
     const int it1 = min(n_items, it0 + per);
     if (it0 >= it1) return;
+    if (warp == 0) {
+        tmptx::tmem_alloc(tmem_slot, PB::TMEM_COLS);
+        tmptx::tmem_relinquish();
+    }
+    tmptx::tmem_fence_before_sync();
+    __syncthreads();
+    tmptx::tmem_fence_after_sync();
+    const uint32_t tmem = *tmem_slot + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(32 * (warp >> 2));
     auto issue_rows = [&](int it, float2* dst) {
         const int ch = it / a.nb, oo = it % a.nb;
         const float2* src = a.A + (size_t)oo * T * XP + ch * W;
@@ -401,10 +412,20 @@ k_pass_b(BatchArgs a, int n_items) {
         }
         __syncthreads();  // this item's rows of A are visible to every thread
         if (chunk != cur_chunk) {
-            // thread-private copy of the 16 I' values this thread multiplies with
+            // the 16 I' values this thread multiplies with, into its TMEM columns
             const float2* Ic = a.Ip + kx0 + c;
+            float buf[16];
 #pragma unroll
-            for (int r = 0; r < 16; r++) ipv[r * NT + tid] = __ldg(Ic + (size_t)(j + (Y / 16) * r) * XP);
+            for (int h = 0; h < 2; h++) {
+#pragma unroll
+                for (int r = 0; r < 8; r++) {
+                    const float2 iv = __ldg(Ic + (size_t)(j + (Y / 16) * (8 * h + r)) * XP);
+                    buf[2 * r] = iv.x;
+                    buf[2 * r + 1] = iv.y;
+                }
+                tmptx::tmem_st16(tmem + 16 * h, buf);
+            }
+            tmptx::tmem_wait_st();
             cur_chunk = chunk;
         }
         float2 v[16];
@@ -418,16 +439,26 @@ k_pass_b(BatchArgs a, int n_items) {
                 w = cmul(w, w1);
             }
         }
-        tmfft::fft_split<T, 16, -1>(v, tp, fwdbuf, a.tw, sync);
+        tmfft::fft<T, 16, -1>(v, tp, fwdbuf, a.tw, sync);
         // thread (s, tp) holds F[k], k = s + MY*(tp + PT*r) = j + (Y/16)*r
 #pragma unroll
-        for (int r = 0; r < 16; r++) v[r] = cmul_conj(ipv[r * NT + tid], v[r]);
-        tmfft::fft_split<Y, 16, +1>(v, j, colbuf, a.tw, sync);
+        for (int h = 0; h < 2; h++) {
+            float iv[16];
+            tmptx::tmem_ld16(tmem + 16 * h, iv);
+            tmptx::tmem_wait_ld();
+#pragma unroll
+            for (int r = 0; r < 8; r++) v[8 * h + r] = cmul_conj(make_float2(iv[2 * r], iv[2 * r + 1]), v[8 * h + r]);
+        }
+        tmfft::fft<Y, 16, +1>(v, j, colbuf, a.tw, sync);
         float2* Co = a.C + (size_t)o * Y * XP + kx0 + c;
 #pragma unroll
         for (int r = 0; r < 16; r++) Co[(size_t)(j + (Y / 16) * r) * XP] = v[r];
     }
     tmptx::cp_async_wait<0>();
+    tmptx::tmem_fence_before_sync();
+    __syncthreads();
+    tmptx::tmem_fence_after_sync();
+    if (warp == 0) tmptx::tmem_dealloc(*tmem_slot, PB::TMEM_COLS);
 }
 
 // --------------------------------------------------------------------------------------
