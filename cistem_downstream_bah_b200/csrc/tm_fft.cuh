@@ -224,6 +224,10 @@ __device__ __forceinline__ void fft(float2 (&v)[R], int t, float2* buf, const Tw
     for (int s = 0; s < PL::stages; s++) {
         const int RS = PL::radix(s);
         const bool last = (s == PL::stages - 1);
+        // twiddle base of this stage for the first butterfly, loaded before the
+        // exchange so its latency hides behind the barrier and shared loads
+        float2 w_first = make_float2(1.f, 0.f);
+        if (s > 0) w_first = tw.template w<DIR>((t % Ns) * (L / (Ns * RS)), L);
         if (s > 0) {
             // load stage input: x[t + P*r]
             sync();
@@ -240,7 +244,7 @@ __device__ __forceinline__ void fft(float2 (&v)[R], int t, float2* buf, const Tw
             for (int r = 0; r < RS; r++) e[r] = v[u + r * (R / RS)];
             if (s > 0) {
                 const int jm = b % Ns;
-                const float2 w = tw.template w<DIR>(jm * (L / (Ns * RS)), L);
+                const float2 w = (u == 0) ? w_first : tw.template w<DIR>(jm * (L / (Ns * RS)), L);
                 if (RS == 16) apply_twiddles<16>(e, w);
                 else if (RS == 8) apply_twiddles<8>(e, w);
                 else if (RS == 4) apply_twiddles<4>(e, w);

@@ -400,7 +400,14 @@ k_pass_b(BatchArgs a, int n_items) {
         float2* anext = abuf + (PB::ABUFS == 2 ? ((kk + 1) & 1) : 0) * (T * W);
         const int chunk = it / a.nb, o = it % a.nb;
         const int kx0 = chunk * W;
-        __syncthreads();  // the previous item is done with the staging and exchange buffers
+        // twiddles of the pruned forward, W_Y^(s * (tp + PT*r)) = w0 * w1^r, loaded early
+        const float2 w0 = a.tw.template w<-1>(s * tp, Y);
+        const float2 w1 = a.tw.template w<-1>(s * PT, Y);
+        // The buffer the next rows go into was last read at the start of the
+        // previous item's forward transform, whose barriers every thread has
+        // passed; the exchange buffers are guarded by the transforms' own barriers.
+        // With a single staging buffer the rows are reloaded in place, after a barrier.
+        if (PB::ABUFS == 1) __syncthreads();
         if (PB::ABUFS == 2) {
             if (it + 1 < it1) issue_rows(it + 1, anext);
             tmptx::cp_async_commit();
@@ -430,9 +437,7 @@ k_pass_b(BatchArgs a, int n_items) {
         }
         float2 v[16];
         {
-            // twiddles of the pruned forward: W_Y^(s * (tp + PT*r))
-            float2 w = a.tw.template w<-1>(s * tp, Y);
-            const float2 w1 = a.tw.template w<-1>(s * PT, Y);
+            float2 w = w0;
 #pragma unroll
             for (int r = 0; r < 16; r++) {
                 v[r] = cmul(acur[(tp + PT * r) * W + c], w);
@@ -441,13 +446,17 @@ k_pass_b(BatchArgs a, int n_items) {
         }
         tmfft::fft<T, 16, -1>(v, tp, fwdbuf, a.tw, sync);
         // thread (s, tp) holds F[k], k = s + MY*(tp + PT*r) = j + (Y/16)*r
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
+        {
             float iv[16];
-            tmptx::tmem_ld16(tmem + 16 * h, iv);
+            tmptx::tmem_ld16(tmem, iv);
+            tmptx::tmem_wait_ld();
+            float iw[16];
+            tmptx::tmem_ld16(tmem + 16, iw);   // in flight while the first half is multiplied
+#pragma unroll
+            for (int r = 0; r < 8; r++) v[r] = cmul_conj(make_float2(iv[2 * r], iv[2 * r + 1]), v[r]);
             tmptx::tmem_wait_ld();
 #pragma unroll
-            for (int r = 0; r < 8; r++) v[8 * h + r] = cmul_conj(make_float2(iv[2 * r], iv[2 * r + 1]), v[8 * h + r]);
+            for (int r = 0; r < 8; r++) v[8 + r] = cmul_conj(make_float2(iw[2 * r], iw[2 * r + 1]), v[8 + r]);
         }
         tmfft::fft<Y, 16, +1>(v, j, colbuf, a.tw, sync);
         float2* Co = a.C + (size_t)o * Y * XP + kx0 + c;
