@@ -30,7 +30,7 @@ TM_ERR_CANCELLED = -6
 EXPORTED = [
     "tm_create", "tm_set_template", "tm_set_image", "tm_reset_results", "tm_run_plane",
     "tm_get_results", "tm_correlations_computed", "tm_last_timing", "tm_debug_stage_buffers", "tm_destroy",
-    "tm_last_error", "tm_version",
+    "tm_last_error", "tm_version", "tm_run_plane_noalloc",
 ]
 
 
@@ -80,6 +80,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.tm_correlations_computed.restype = ctypes.c_longlong
     L.tm_last_timing.argtypes = [vp] + [ctypes.POINTER(ctypes.c_double)] * 4
     L.tm_debug_stage_buffers.argtypes = [vp] * 8
+    L.tm_run_plane_noalloc.argtypes = [ip, ctypes.POINTER(TmDims), vp, vp, vp, vp, ip, ip, vp, vp, vp, vp, vp, vp]
     L.tm_destroy.argtypes = [vp]
     L.tm_last_error.argtypes = [vp]
     L.tm_last_error.restype = ctypes.c_char_p

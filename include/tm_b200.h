@@ -126,6 +126,37 @@ TM_API int tm_last_timing(const tm_ctx *ctx, double *total_ms, double *pass_b_ms
 TM_API int tm_debug_stage_buffers(tm_ctx *ctx, const float *projection_filter, const float *euler_angle, float *slice,
                                   float *projection, float *normalisation, float *rows, float *columns);
 
+/* Plane search that allocates no device memory, for callers that cannot call
+ * cudaMalloc: code inside a host framework that owns every device allocation
+ * through its own pool, plugins that are only handed pre-allocated buffers,
+ * and code that must not allocate while a stream is being captured.  It has no
+ * counterpart in the reference.
+ *
+ * Same search as tm_run_plane, on the caller's device buffers: the template
+ * spectrum (as tm_set_template), the whitened micrograph spectrum (as
+ * tm_set_image), the projection filter, and the running results -- MIP
+ * (start at -FLT_MAX), best orientation index (start at -1; receives
+ * first_orientation_index + the orientation's position in euler_angles),
+ * sum, sum of squares (start at 0) and histogram (start at 0), each
+ * image_y*image_x ([y][x]) or histogram_bins long.  euler_angles is host
+ * memory, n_orientations (phi, theta, psi) triples.  The work is ordered on
+ * `stream` (a cudaStream_t; NULL = the default stream) and the call returns
+ * when it is done.
+ *
+ * All intermediates live in one fixed device array of 16 MiB, which every GPU
+ * that loads this library holds until the process exits; geometries whose
+ * intermediates exceed it, and geometries without a compiled variant (template
+ * 32 on 256x256 or 512x512, template 64 on 512x512), return TM_ERR_UNSUPPORTED.
+ * The first call on a device looks up that array's device address and sets
+ * kernel attributes, so make it before any stream capture.  Every call reuses
+ * the same array: calls that overlap on the GPU (other streams, other host
+ * threads) race and corrupt each other's results. */
+TM_API int tm_run_plane_noalloc(int device, const tm_dims *dims, const float *d_template_spectrum,
+                                const float *d_image_spectrum, const float *d_projection_filter,
+                                const float *euler_angles, int n_orientations, int first_orientation_index,
+                                float *d_mip, int *d_best, double *d_sum, double *d_sum_of_squares,
+                                unsigned long long *d_histogram, void *stream);
+
 /* Frees every device buffer of the context. */
 TM_API int tm_destroy(tm_ctx *ctx);
 
