@@ -1,0 +1,101 @@
+// host_capi.cpp -- C entry points of the host preparation library
+// (libtm_host.so), so that tests can hold the C++ preparation against the
+// oracle and against numpy.  Complex arrays are interleaved float pairs.
+#include <cstring>
+#include <string>
+
+#include "mrc.hpp"
+#include "prep.hpp"
+
+#define TMH_API extern "C" __attribute__((visibility("default")))
+
+using namespace tmhost;
+
+namespace {
+Image2 wrap(int nx, int ny, const float* v) {
+    Image2 im;
+    im.nx = nx;
+    im.ny = ny;
+    im.v.assign(v, v + (size_t)nx * ny);
+    return im;
+}
+}  // namespace
+
+// whitened half spectrum (ny*(nx/2+1) complex) and the curve; returns the
+// number of curve points written (at most curve_cap)
+TMH_API int tmh_whiten(int nx, int ny, const float* image, float* spec_out, double* curve_out, int curve_cap) {
+    Whitened w = whiten(wrap(nx, ny, image));
+    std::memcpy(spec_out, w.spectrum.data(), w.spectrum.size() * sizeof(float) * 2);
+    const int n = (int)w.curve.size() < curve_cap ? (int)w.curve.size() : curve_cap;
+    std::memcpy(curve_out, w.curve.data(), n * sizeof(double));
+    return (int)w.curve.size();
+}
+
+TMH_API void tmh_template_spectrum(int T, const float* volume, float factor, float* spec_out) {
+    std::vector<float> vol(volume, volume + (size_t)T * T * T);
+    auto s = template_spectrum(vol, T, factor);
+    std::memcpy(spec_out, s.data(), s.size() * sizeof(float) * 2);
+}
+
+TMH_API void tmh_projection_filter(int T, const double* curve, int curve_n, float kv, float cs_mm, float amp, float df1,
+                                   float df2, float ang_deg, float pixel, float phase_deg, float defocus_offset,
+                                   float* out) {
+    std::vector<double> c(curve, curve + curve_n);
+    CtfParams p{kv, cs_mm, amp, df1, df2, ang_deg, pixel, phase_deg};
+    auto f = projection_filter(T, c, p, defocus_offset);
+    std::memcpy(out, f.data(), f.size() * sizeof(float));
+}
+
+TMH_API int tmh_search_grid(const char* symmetry, float angular_step, float* out, int max_out) {
+    auto g = search_grid(angular_step, symmetry);
+    for (int i = 0; i < (int)g.size() && i < max_out; i++) {
+        out[2 * i] = g[i].first;
+        out[2 * i + 1] = g[i].second;
+    }
+    return g.empty() ? -1 : (int)g.size();
+}
+
+TMH_API int tmh_psi_list(float start, float step, float max, float* out, int max_out) {
+    auto p = psi_list(start, step, max);
+    for (int i = 0; i < (int)p.size() && i < max_out; i++) out[i] = p[i];
+    return (int)p.size();
+}
+
+TMH_API int tmh_factorize_dimension(int original, int template_size) { return factorize_dimension(original, template_size); }
+TMH_API int tmh_is_power_of_two(int n) { return is_power_of_two(n) ? 1 : 0; }
+TMH_API float tmh_angular_step(float resolution, float radius) { return angular_step_for(resolution, radius); }
+TMH_API double tmh_erfcinv(double x) { return erfcinv_approx(x); }
+TMH_API float tmh_edge_mean(int nx, int ny, const float* image) { return edge_mean(wrap(nx, ny, image)); }
+
+TMH_API void tmh_clip_into(int nx, int ny, const float* in, int ox, int oy, float pad, float* out) {
+    Image2 o = clip_into(wrap(nx, ny, in), ox, oy, pad);
+    std::memcpy(out, o.v.data(), o.v.size() * sizeof(float));
+}
+
+TMH_API void tmh_rotate90(int nx, int ny, const float* in, int positive, float* out) {
+    Image2 o = rotate90(wrap(nx, ny, in), positive != 0);
+    std::memcpy(out, o.v.data(), o.v.size() * sizeof(float));
+}
+
+// MRC: dims (nx, ny, nz) and pixel size of a file, then its data
+TMH_API int tmh_mrc_info(const char* path, int* dims, float* pixel_size) {
+    MrcData d;
+    std::string err;
+    if (!read_mrc(path, d, err)) return -1;
+    dims[0] = d.nx; dims[1] = d.ny; dims[2] = d.nz;
+    *pixel_size = d.pixel_size;
+    return 0;
+}
+
+TMH_API int tmh_mrc_read(const char* path, float* out) {
+    MrcData d;
+    std::string err;
+    if (!read_mrc(path, d, err)) return -1;
+    std::memcpy(out, d.data.data(), d.data.size() * sizeof(float));
+    return 0;
+}
+
+TMH_API int tmh_mrc_write(const char* path, int nx, int ny, int nz, const float* data, float pixel_size) {
+    std::string err;
+    return write_mrc(path, nx, ny, nz, data, pixel_size, err) ? 0 : -1;
+}

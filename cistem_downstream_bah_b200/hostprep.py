@@ -1,0 +1,157 @@
+"""ctypes bindings of the C++ host preparation library (lib/libtm_host.so).
+
+The library holds the host side of match_template that runs once per
+micrograph or plane -- whitening, template spectrum (with the pixel-size
+change), projection filter, search grid, factorisation and MRC I/O -- in C++
+(host/*.cpp).  These bindings let Python callers and the tests use it; the
+match_template program (lib/match_template) links the same sources.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libtm_host.so")
+CLI_PATH = os.path.join(_HERE, "lib", "match_template")
+_lib = None
+
+EXPORTED = [
+    "tmh_whiten", "tmh_template_spectrum", "tmh_projection_filter", "tmh_search_grid", "tmh_psi_list",
+    "tmh_factorize_dimension", "tmh_is_power_of_two", "tmh_angular_step", "tmh_erfcinv", "tmh_edge_mean",
+    "tmh_clip_into", "tmh_rotate90", "tmh_mrc_info", "tmh_mrc_read", "tmh_mrc_write",
+]
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run cistem_downstream_bah_b200/build.py first")
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        f, i, d = ctypes.c_float, ctypes.c_int, ctypes.c_double
+        L.tmh_whiten.argtypes = [i, i, P, P, P, i]
+        L.tmh_whiten.restype = i
+        L.tmh_template_spectrum.argtypes = [i, P, f, P]
+        L.tmh_projection_filter.argtypes = [i, P, i, f, f, f, f, f, f, f, f, f, P]
+        L.tmh_search_grid.argtypes = [ctypes.c_char_p, f, P, i]
+        L.tmh_search_grid.restype = i
+        L.tmh_psi_list.argtypes = [f, f, f, P, i]
+        L.tmh_psi_list.restype = i
+        L.tmh_factorize_dimension.argtypes = [i, i]
+        L.tmh_factorize_dimension.restype = i
+        L.tmh_is_power_of_two.argtypes = [i]
+        L.tmh_is_power_of_two.restype = i
+        L.tmh_angular_step.argtypes = [f, f]
+        L.tmh_angular_step.restype = f
+        L.tmh_erfcinv.argtypes = [d]
+        L.tmh_erfcinv.restype = d
+        L.tmh_edge_mean.argtypes = [i, i, P]
+        L.tmh_edge_mean.restype = f
+        L.tmh_clip_into.argtypes = [i, i, P, i, i, f, P]
+        L.tmh_rotate90.argtypes = [i, i, P, i, P]
+        L.tmh_mrc_info.argtypes = [ctypes.c_char_p, P, P]
+        L.tmh_mrc_info.restype = i
+        L.tmh_mrc_read.argtypes = [ctypes.c_char_p, P]
+        L.tmh_mrc_read.restype = i
+        L.tmh_mrc_write.argtypes = [ctypes.c_char_p, i, i, i, P, f]
+        L.tmh_mrc_write.restype = i
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def whiten(image):
+    img = _f32(image)
+    ny, nx = img.shape
+    spec = np.zeros((ny, nx // 2 + 1), np.complex64)
+    curve = np.zeros(4 * nx + 16, np.float64)
+    n = lib().tmh_whiten(nx, ny, _p(img), _p(spec), _p(curve), len(curve))
+    return spec, curve[:n].copy()
+
+
+def template_spectrum(volume, factor=1.0):
+    vol = _f32(volume)
+    T = vol.shape[0]
+    out = np.zeros((T, T, T // 2 + 1), np.complex64)
+    lib().tmh_template_spectrum(T, _p(vol), float(factor), _p(out))
+    return out
+
+
+def projection_filter(T, curve, *, kv, cs_mm, amplitude_contrast, defocus1, defocus2, astigmatism_angle=0.0,
+                      pixel_size, phase_shift_deg=0.0, defocus_offset=0.0):
+    c = np.ascontiguousarray(curve, np.float64)
+    out = np.zeros((T, T // 2 + 1), np.float32)
+    lib().tmh_projection_filter(T, _p(c), len(c), kv, cs_mm, amplitude_contrast, defocus1, defocus2,
+                                astigmatism_angle, pixel_size, phase_shift_deg, defocus_offset, _p(out))
+    return out
+
+
+def search_grid(angular_step, symmetry="C1"):
+    n = lib().tmh_search_grid(symmetry.encode(), angular_step, None, 0)
+    if n < 0:
+        raise ValueError(f"bad symmetry {symmetry}")
+    out = np.zeros((n, 2), np.float32)
+    lib().tmh_search_grid(symmetry.encode(), angular_step, _p(out), n)
+    return out
+
+
+def psi_list(start, step, max_):
+    n = lib().tmh_psi_list(start, step, max_, None, 0)
+    out = np.zeros(n, np.float32)
+    lib().tmh_psi_list(start, step, max_, _p(out), n)
+    return out
+
+
+def factorize_dimension(original, template_size):
+    return lib().tmh_factorize_dimension(int(original), int(template_size))
+
+
+def edge_mean(img):
+    a = _f32(img)
+    return lib().tmh_edge_mean(a.shape[1], a.shape[0], _p(a))
+
+
+def clip_into(img, ox, oy, pad=0.0):
+    a = _f32(img)
+    out = np.zeros((oy, ox), np.float32)
+    lib().tmh_clip_into(a.shape[1], a.shape[0], _p(a), ox, oy, pad, _p(out))
+    return out
+
+
+def rotate90(img, positive=True):
+    a = _f32(img)
+    out = np.zeros((a.shape[1], a.shape[0]), np.float32)
+    lib().tmh_rotate90(a.shape[1], a.shape[0], _p(a), int(positive), _p(out))
+    return out
+
+
+def read_mrc(path):
+    """(data [z][y][x] float32, pixel size) of an MRC file (modes 0, 1, 2, 6, 12)."""
+    dims = np.zeros(3, np.int32)
+    px = np.zeros(1, np.float32)
+    if lib().tmh_mrc_info(str(path).encode(), _p(dims), _p(px)) != 0:
+        raise OSError(f"cannot read MRC file {path}")
+    out = np.zeros((dims[2], dims[1], dims[0]), np.float32)
+    if lib().tmh_mrc_read(str(path).encode(), _p(out)) != 0:
+        raise OSError(f"cannot read MRC file {path}")
+    return out, float(px[0])
+
+
+def write_mrc(path, data, pixel_size=1.0):
+    a = _f32(data)
+    if a.ndim == 2:
+        a = a[None]
+    nz, ny, nx = a.shape
+    if lib().tmh_mrc_write(str(path).encode(), nx, ny, nz, _p(a), pixel_size) != 0:
+        raise OSError(f"cannot write MRC file {path}")

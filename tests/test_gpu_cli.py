@@ -1,0 +1,110 @@
+"""The match_template program (C++ host over the C ABI) end to end on the GPU,
+against the oracle pipeline: the reference CPU path restated (whitening,
+template spectrum, projection filters, the search over three defocus planes,
+statistics, resize to the original micrograph, the histogram file)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from cistem_downstream_bah_b200 import hostprep as H
+from cistem_downstream_bah_b200 import synthetic
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+T, PIXEL, DEFOCUS = 32, 2.0, 8000.0
+STEP, PSI_STEP, DF_RANGE, DF_STEP = 20.0, 20.0, 200.0, 200.0
+
+
+def _files(tmp):
+    names = ["mip", "psi", "theta", "phi", "defocus", "pixel", "scaled", "avg", "std"]
+    return {n: str(tmp / f"{n}.mrc") for n in names}
+
+
+def _run_cli(tmp, img_path, tpl_path):
+    f = _files(tmp)
+    args = [img_path, tpl_path, PIXEL, 300.0, 2.7, 0.07, DEFOCUS, DEFOCUS, 0.0, 300.0, 8.0, STEP, 20,
+            DF_RANGE, DF_STEP, 0.0, 0.0, 1.0, "no", 0.0, 0.0,
+            f["mip"], f["psi"], f["theta"], f["phi"], f["defocus"], f["pixel"], f["scaled"], f["avg"], "C1",
+            PSI_STEP, str(tmp / "hist.txt"), -1, -1, 0, 0, f["std"], "/dev/null", "/dev/null", 10.0, "yes", 1]
+    assert len(args) == 42
+    r = subprocess.run([H.CLI_PATH, *map(str, args)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    return f, r.stdout
+
+
+def _oracle_pipeline(img, vol):
+    Y0, X0 = img.shape
+    X, Y = O.factorize_dimension(X0, T), O.factorize_dimension(Y0, T)
+    padded = O.clip_into_real(img.astype(np.float64), X, Y, float(H.edge_mean(img)))
+    ispec, curve = O.whiten_image(padded)
+    tspec = O.prepare_template(vol.astype(np.float64))
+    ang = O.orientation_list(O.search_grid(STEP), O.psi_list(0.0, PSI_STEP, 360.0))
+    sq = np.sqrt(float(X * Y))
+    hstep = np.float32((22.5 - (-12.5)) / np.float32(512))
+    st = O.SearchState(X, Y)
+    n_planes = 0
+    for i in (-1, 0, 1):
+        filt = O.projection_filter(T, curve, kv=300.0, cs_mm=2.7, amplitude_contrast=0.07, defocus1=DEFOCUS,
+                                   defocus2=DEFOCUS, pixel_size=PIXEL, defocus_offset=i * DF_STEP)
+        O.search(st, tspec, ispec, filt, ang, hist_min_scaled=-12.5 / sq, hist_step_scaled=float(hstep) / sq,
+                 defocus_value=float(np.float32(i) * np.float32(DF_STEP)), pixel_value=0.0)
+        n_planes += 1
+    n_total = len(ang) * n_planes
+    mip, z, avg, sd = O.finalize(st, n_total, sq)
+    shape = (Y, X)
+
+    def back(a, edge):
+        a = np.asarray(a, np.float32).reshape(shape)
+        return O.clip_into_real(a.astype(np.float64), X0, Y0, float(H.edge_mean(a)) if edge else 0.0).astype(np.float32)
+
+    decided = ((st.mip - st.second) > 1e-4 * np.abs(st.mip)).reshape(shape)
+    return dict(mip=back(mip, True), scaled=back(z, True), avg=back(avg, True), std=back(sd, True),
+                psi=back(st.psi, False), theta=back(st.theta, False), phi=back(st.phi, False),
+                defocus=back(st.defocus, False), decided=O.clip_into_real(decided.astype(np.float64), X0, Y0, 0.0) > 0.5,
+                hist=st.hist[:512], n_total=n_total, X0=X0, Y0=Y0)
+
+
+def test_match_template_program_matches_oracle(tmp_path):
+    vol = synthetic.template_volume(T, PIXEL, n_atoms=600, radius_A=T * PIXEL * 0.3, seed=21)
+    img, truth = synthetic.micrograph(250, 256, PIXEL, n_atoms=600, radius_A=T * PIXEL * 0.3, n_particles=3,
+                                      snr=2.0, defocus_A=DEFOCUS, seed=22, atom_seed=21)
+    H.write_mrc(tmp_path / "img.mrc", img, PIXEL)
+    H.write_mrc(tmp_path / "tpl.mrc", vol, PIXEL)
+    files, stdout = _run_cli(tmp_path, str(tmp_path / "img.mrc"), str(tmp_path / "tpl.mrc"))
+    assert "old x, y; new x, y = 256 250 256 256" in stdout
+    ref = _oracle_pipeline(img.astype(np.float32), vol.astype(np.float32))
+    got = {k: H.read_mrc(v)[0][0] for k, v in files.items()}
+    for k in got:
+        assert got[k].shape == (250, 256), k
+        assert abs(H.read_mrc(files[k])[1] - PIXEL) < 1e-6
+    scale = np.abs(ref["mip"]).max()
+    assert np.abs(got["mip"] - ref["mip"]).max() <= 1e-4 * scale
+    assert np.abs(got["avg"] - ref["avg"]).max() <= 1e-4 * np.abs(ref["std"]).max()
+    assert np.abs(got["std"] - ref["std"]).max() <= 1e-4 * np.abs(ref["std"]).max()
+    assert np.abs(got["scaled"] - ref["scaled"]).max() <= 2e-3
+    d = ref["decided"]
+    assert d.mean() > 0.9
+    for k in ("psi", "theta", "phi", "defocus"):
+        assert np.array_equal(got[k][d], ref[k][d]), k
+    assert np.array_equal(got["pixel"], np.zeros_like(got["pixel"]))
+    # histogram text file: two comment lines, then 512 rows of 4 columns
+    lines = open(tmp_path / "hist.txt").read().splitlines()
+    assert lines[0].startswith("# Expected threshold = ")
+    assert lines[1] == "# SNR, histogram, survival histogram, random survival histogram"
+    rows = np.array([[float(v) for v in ln.split()] for ln in lines[2:]])
+    assert rows.shape == (512, 4)
+    assert np.allclose(rows[:, 0], -12.5 + 35.0 / 512 * (np.arange(512) + 0.5), atol=1e-4)
+    h = rows[:, 1]
+    assert abs(h.sum() - ref["hist"].sum()) <= 2 + 1e-4 * ref["hist"].sum()
+    assert np.all(np.abs(h - ref["hist"]) <= 2 + 1e-3 * ref["hist"])
+    assert np.allclose(rows[:, 2], np.cumsum(h[::-1])[::-1])
+    expected_threshold = np.sqrt(2.0) * O.erfcinv(2.0 / (256.0 * 250.0 * ref["n_total"]))
+    assert lines[0] == "# Expected threshold = %.2f" % np.float32(expected_threshold)
+    # the planted particles are found at their positions
+    for (px, py) in truth["positions"]:
+        y, x = int(round(py)), int(round(px))
+        win = got["scaled"][max(0, y - 3):y + 4, max(0, x - 3):x + 4]
+        assert win.max() > 5.0, (px, py, win.max())
