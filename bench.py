@@ -42,9 +42,24 @@ sys.path.insert(0, ROOT)
 METRIC = "search points/s (original micrograph pixels x orientations)"
 UNIT = "points/s"
 
-WORKLOAD = dict(name="4096x4096 micrograph, 256^3 template @1.0 A/px, C1 2.5/1.5 deg grid",
-                nx=4096, ny=4096, T=256, pixel_size=1.0, n_atoms=120000, radius_A=110.0, particles=80,
-                snr=0.03, defocus=12000.0, angular_step=2.5, psi_step=1.5)
+WORKLOADS = {
+    # the metric's configuration (default)
+    "full": dict(name="4096x4096 micrograph, 256^3 template @1.0 A/px, C1 2.5/1.5 deg grid",
+                 nx=4096, ny=4096, T=256, pixel_size=1.0, n_atoms=120000, radius_A=110.0, particles=80,
+                 snr=0.03, defocus=12000.0, angular_step=2.5, psi_step=1.5),
+    # the uneven micrograph sizes of the batched configuration, one at a time
+    "uneven3710": dict(name="3838x3710 micrograph (padded 4096x3888), 256^3 template @1.0 A/px, C1 3.0/2.0 deg grid",
+                       nx=3838, ny=3710, T=256, pixel_size=1.0, n_atoms=120000, radius_A=110.0, particles=70,
+                       snr=0.03, defocus=14000.0, angular_step=3.0, psi_step=2.0),
+    "uneven5760": dict(name="5760x4092 micrograph (padded 5832x4096, rotated), 256^3 template @1.0 A/px, C1 3.0/2.0 deg grid",
+                       nx=5760, ny=4092, T=256, pixel_size=1.0, n_atoms=120000, radius_A=110.0, particles=110,
+                       snr=0.03, defocus=10000.0, angular_step=3.0, psi_step=2.0),
+    # the stress configuration's geometry (one micrograph, one plane)
+    "stress384": dict(name="5760x4092 micrograph (padded 5832x4096, rotated), 384^3 template @0.8 A/px, C1 2.5/1.5 deg grid",
+                      nx=5760, ny=4092, T=384, pixel_size=0.8, n_atoms=250000, radius_A=150.0, particles=40,
+                      snr=0.03, defocus=12000.0, angular_step=2.5, psi_step=1.5),
+}
+WORKLOAD = WORKLOADS["full"]
 
 
 def peaks():
@@ -113,15 +128,21 @@ class ClockSampler:
 
 def make_inputs(seed=20261204):
     """Synthetic micrograph and template, prepared as the reference's
-    DoCalculation prepares them (whitening, template spectrum, CTF filter)."""
-    from cistem_downstream_bah_b200 import prep, synthetic
+    DoCalculation prepares them: size factorisation with edge-mean padding and
+    the 90-degree rotation (match_template.cpp:520-596, C++ host library),
+    whitening, template spectrum, CTF filter."""
+    from cistem_downstream_bah_b200 import hostprep, prep, synthetic
     w = WORKLOAD
     vol = synthetic.template_volume(w["T"], w["pixel_size"], w["n_atoms"], w["radius_A"], seed=seed)
     mic, _ = synthetic.micrograph(w["ny"], w["nx"], w["pixel_size"], w["n_atoms"], w["radius_A"], w["particles"],
                                   w["snr"], w["defocus"], seed=seed + 1, atom_seed=seed)
-    X = prep.factorize_dimension(w["nx"], w["T"])
-    Y = prep.factorize_dimension(w["ny"], w["T"])
-    assert (X, Y) == (w["nx"], w["ny"])
+    X = hostprep.factorize_dimension(w["nx"], w["T"])
+    Y = hostprep.factorize_dimension(w["ny"], w["T"])
+    if (X, Y) != (w["nx"], w["ny"]):
+        mic = hostprep.clip_into(mic, X, Y, hostprep.edge_mean(mic))
+    if not hostprep.lib().tmh_is_power_of_two(X) and hostprep.lib().tmh_is_power_of_two(Y):
+        mic = hostprep.rotate90(mic, True)
+        X, Y = Y, X
     ispec, curve = prep.whiten(mic)
     tspec = prep.template_spectrum(vol)
     filt = prep.projection_filter(w["T"], curve, kv=300.0, cs_mm=2.7, amplitude_contrast=0.07,
@@ -253,12 +274,16 @@ def run_ours(args):
     dominant = "k_pass_b" if b_ms >= c_ms else "k_pass_c"
     alg_b = 8.0 * N * nb
     alg_c = 4.0 * N * nb
+    # DRAM bytes per launch from the committed ncu captures of this workload
+    # (profiles/k_pass_b_4096x4096_t256.md, profiles/k_pass_c_4096x4096_t256.md);
+    # they apply to the default workload and batch only
+    default_shape = (X, Y, T, nb) == (4096, 4096, 256, 32)
     if dominant == "k_pass_b":
         ach = alg_b / (b_launch_ms * 1e-3) / 1e9
-        traffic = args.traffic_b
+        traffic = args.traffic_b if args.traffic_b is not None else (PROFILED_TRAFFIC["k_pass_b"] if default_shape else None)
     else:
         ach = alg_c / (c_launch_ms * 1e-3) / 1e9
-        traffic = args.traffic_c
+        traffic = args.traffic_c if args.traffic_c is not None else (PROFILED_TRAFFIC["k_pass_c"] if default_shape else None)
 
     cpu = cpu_baseline(inp, sample=args.cpu_sample) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     sc.close()
@@ -287,6 +312,10 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+# ncu dram__bytes_read.sum + dram__bytes_write.sum per launch (32 orientations, 4096^2, 256^3)
+PROFILED_TRAFFIC = {"k_pass_b": 0.869e9 + 2.142e9, "k_pass_c": 2.555e9 + 0.382e9}
 
 
 def _oracle_sample(inp, n_orient, bits=32):
@@ -351,9 +380,13 @@ def main():
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--cpu-sample", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="full", choices=sorted(WORKLOADS),
+                    help="full = the metric's 4096^2 configuration; the others are the uneven and stress geometries")
     ap.add_argument("--traffic-b", type=float, default=None, help="ncu DRAM bytes per pass-B launch")
     ap.add_argument("--traffic-c", type=float, default=None, help="ncu DRAM bytes per pass-C launch")
     args = ap.parse_args()
+    global WORKLOAD
+    WORKLOAD = WORKLOADS[args.workload]
     if args.warmup < 3 and args.impl == "ours":
         print("note: fewer than 3 warm-up steps", file=sys.stderr)
     if args.impl == "reference":
