@@ -42,7 +42,8 @@ struct tm_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_prep = nullptr, ev_b = nullptr, ev_c = nullptr, ev_end = nullptr;
     // device buffers
-    float2 *tmpl = nullptr, *Ip = nullptr, *S = nullptr, *A = nullptr, *C = nullptr, *norm = nullptr, *twid = nullptr;
+    float2 *tmpl = nullptr, *Ip = nullptr, *S = nullptr, *A = nullptr, *C = nullptr, *norm = nullptr;
+    float2 *twx = nullptr, *twy = nullptr, *twt = nullptr;   // twiddle tables of the x, y and template lengths
     float *P = nullptr, *filter = nullptr, *rot = nullptr;
     double* rowstat = nullptr;
     float* mip = nullptr;
@@ -50,7 +51,6 @@ struct tm_ctx {
     double *sum = nullptr, *sumsq = nullptr;
     unsigned long long* hist = nullptr;
     int* err_flag = nullptr;
-    int lmax = 0;
     long long rot_capacity = 0;
     bool has_template = false, has_image = false;
     // bookkeeping for decoding the argmax
@@ -89,6 +89,7 @@ int set_err(tm_ctx* c, int code, const char* fmt, ...) {
 
 struct Variant {
     int T, X, Y;
+    int W;   // pass-B column chunk
     int (*run_batch)(tm_ctx*, tmk::BatchArgs&, bool timing);
     int (*configure)(tm_ctx*);
     int (*run_stages)(tm_ctx*, tmk::BatchArgs&);   // every kernel before the MIP epilogue
@@ -96,26 +97,16 @@ struct Variant {
 
 template <int T, int X, int Y>
 struct Impl {
-    using PB = tmk::PassB<T, Y>;
-    using RC = tmk::RowC2R<T>;
-
-    using PCc = tmk::PassC<X>;
+    using LN = tmk::Launch<T, X, Y>;
 
     static int configure(tm_ctx* c) {
-        TM_CUDA(c, cudaFuncSetAttribute(tmk::k_pass_b<T, Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB::SMEM));
-        TM_CUDA(c, cudaFuncSetAttribute(tmk::k_pass_c<X>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)PCc::smem_bytes(c->XP, c->d.histogram_bins)));
+        TM_CUDA(c, LN::configure(c->XP, c->d.histogram_bins));
         return TM_OK;
     }
 
     static int run_stages(tm_ctx* c, tmk::BatchArgs& a) {
-        cudaStream_t s = c->stream;
-        tmk::k_slice_colfft<T><<<dim3((T / 2 + 1 + 15) / 16, a.nb), T, 0, s>>>(a);
-        tmk::k_row_c2r<T><<<dim3(T / RC::ROWS, a.nb), RC::NT, 0, s>>>(a);
-        tmk::k_norm<T><<<(a.nb + 7) / 8, 256, 0, s>>>(a, (long long)X * Y);
-        tmk::k_pass_a<T, X><<<dim3(T, a.nb), X / 16, 0, s>>>(a);
-        const int n_items = (c->XP / PB::W) * a.nb;
-        tmk::k_pass_b<T, Y><<<n_items < c->nsm ? n_items : c->nsm, PB::NT, PB::SMEM, s>>>(a, n_items);
+        LN::prep(a, c->stream);
+        LN::pass_b(a, c->stream, c->nsm);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return set_err(c, TM_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
         return TM_OK;
@@ -123,17 +114,11 @@ struct Impl {
 
     static int run_batch(tm_ctx* c, tmk::BatchArgs& a, bool timing) {
         cudaStream_t s = c->stream;
-        tmk::k_slice_colfft<T><<<dim3((T / 2 + 1 + 15) / 16, a.nb), T, 0, s>>>(a);
-        tmk::k_row_c2r<T><<<dim3(T / RC::ROWS, a.nb), RC::NT, 0, s>>>(a);
-        tmk::k_norm<T><<<(a.nb + 7) / 8, 256, 0, s>>>(a, (long long)X * Y);
-        tmk::k_pass_a<T, X><<<dim3(T, a.nb), X / 16, 0, s>>>(a);
+        LN::prep(a, s);
         if (timing) cudaEventRecord(c->ev_prep, s);
-        const int nchunk = c->XP / PB::W;
-        const int n_items = nchunk * a.nb;
-        const int grid = n_items < c->nsm ? n_items : c->nsm;
-        tmk::k_pass_b<T, Y><<<grid, PB::NT, PB::SMEM, s>>>(a, n_items);
+        LN::pass_b(a, s, c->nsm);
         if (timing) cudaEventRecord(c->ev_b, s);
-        tmk::k_pass_c<X><<<Y, X / 16, PCc::smem_bytes(c->XP, a.hist_bins), s>>>(a, Y);
+        LN::pass_c(a, s);
         if (timing) cudaEventRecord(c->ev_c, s);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return set_err(c, TM_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
@@ -141,8 +126,16 @@ struct Impl {
     }
 };
 
-#define TM_VARIANT(T, X, Y) {T, X, Y, &Impl<T, X, Y>::run_batch, &Impl<T, X, Y>::configure, &Impl<T, X, Y>::run_stages}
+#define TM_VARIANT(T, X, Y) \
+    {T, X, Y, tmk::Launch<T, X, Y>::pass_b_width, &Impl<T, X, Y>::run_batch, &Impl<T, X, Y>::configure, &Impl<T, X, Y>::run_stages}
 
+// Geometries with compiled kernels: template box T on a padded X x Y
+// micrograph.  X is a power of two (the reference turns a micrograph whose
+// padded width is not a power of two but whose height is by 90 degrees,
+// match_template.cpp:587-596); Y may carry factors of 3 (3888 = 2^4 3^5 and
+// 5832 = 2^3 3^6 are what its factorisation gives for 3710- and 5760-pixel
+// sides).  The small 288- and 48-sized geometries exercise the same code paths
+// for tests.
 const Variant kVariants[] = {
     TM_VARIANT(32, 256, 256),
     TM_VARIANT(32, 512, 256),
@@ -155,6 +148,13 @@ const Variant kVariants[] = {
     TM_VARIANT(256, 2048, 2048),
     TM_VARIANT(256, 4096, 4096),
     TM_VARIANT(64, 4096, 4096),
+    TM_VARIANT(32, 256, 288),
+    TM_VARIANT(48, 256, 256),
+    TM_VARIANT(48, 256, 288),
+    TM_VARIANT(256, 4096, 3888),
+    TM_VARIANT(256, 4096, 5832),
+    TM_VARIANT(384, 4096, 4096),
+    TM_VARIANT(384, 4096, 5832),
 };
 
 const Variant* find_variant(int T, int X, int Y) {
@@ -188,7 +188,7 @@ int wait_stream(tm_ctx* c, double limit_s) {
 }
 
 void free_all(tm_ctx* c) {
-    void* ptrs[] = {c->tmpl, c->Ip, c->S, c->A, c->C, c->norm, c->twid, c->P, c->filter, c->rot,
+    void* ptrs[] = {c->tmpl, c->Ip, c->S, c->A, c->C, c->norm, c->twx, c->twy, c->twt, c->P, c->filter, c->rot,
                     c->rowstat, c->mip, c->best, c->sum, c->sumsq, c->hist, c->err_flag};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -240,8 +240,12 @@ tmk::BatchArgs make_args(tm_ctx* c) {
     a.hist_bins = c->d.histogram_bins;
     a.XP = c->XP;
     a.err = c->err_flag;
-    a.tw.tab = c->twid;
-    a.tw.lmax = c->lmax;
+    a.tw.tab = c->twx;
+    a.tw.lmax = c->X;
+    a.twy.tab = c->twy;
+    a.twy.lmax = c->Y;
+    a.twt.tab = c->twt;
+    a.twt.lmax = c->T;
     return a;
 }
 
@@ -261,30 +265,21 @@ int tm_create(const tm_dims* dims, tm_ctx** out) {
     c->X = dims->image_x;
     c->Y = dims->image_y;
     c->T = dims->template_size;
-    {
-        // pass B processes W = 16384 / Y adjacent columns per block; the row
-        // pitch covers kx = 0 .. X/2 in whole chunks (and stays even for the
-        // 16-byte loads of pass C)
-        int W = c->Y > 0 ? 16384 / c->Y : 4;
-        if (W > 16) W = 16;
-        if (W < 4) W = 4;
-        c->XP = (c->X / 2 + 1 + W - 1) / W * W;
-    }
     c->TP = c->T / 2 + 1;
     c->B = dims->orientation_batch > 0 ? dims->orientation_batch : 32;
     if (dims->histogram_bins <= 0 || dims->histogram_bins > 1024 || !(dims->histogram_step_scaled > 0)) {
         *out = c;
         return set_err(c, TM_ERR_INVALID, "histogram_bins must be 1..1024 and the step positive");
     }
-    if (c->XP > c->X / 2 + 64) {
-        *out = c;
-        return set_err(c, TM_ERR_UNSUPPORTED, "image height %d too small for the column pass", c->Y);
-    }
     c->var = find_variant(c->T, c->X, c->Y);
     if (!c->var) {
         *out = c;
         return set_err(c, TM_ERR_UNSUPPORTED, "no kernel variant for template %d and image %d x %d", c->T, c->X, c->Y);
     }
+    // the row pitch covers kx = 0 .. X/2 in whole pass-B chunks (and stays
+    // even for the 16-byte loads of pass C)
+    c->XP = (c->X / 2 + 1 + c->var->W - 1) / c->var->W * c->var->W;
+    if (c->XP % 2) c->XP += c->var->W;
     c->device = dims->device;
     int rc;
 #define TRY(x) if ((rc = (x)) != TM_OK) { *out = c; return rc; }
@@ -328,17 +323,21 @@ int tm_create(const tm_dims* dims, tm_ctx** out) {
         cudaError_t e = cudaMemsetAsync(c->A, 0, B * T * XP * sizeof(float2), c->stream);
         if (e != cudaSuccess) { *out = c; return set_err(c, TM_ERR_CUDA, "memset: %s", cudaGetErrorString(e)); }
     }
-    // twiddle table W_LMAX^m for the largest transform length
-    c->lmax = (int)(X > Y ? X : Y);
-    TRY(dalloc(c, &c->twid, (size_t)c->lmax));
+    // twiddle tables W_L^m = exp(-2 pi i m / L) for L = X, Y and T: every
+    // transform length of a kernel divides the length of the table it uses
     {
-        std::vector<float2> tw(c->lmax);
-        for (int m = 0; m < c->lmax; m++) {
-            double ang = -2.0 * M_PI * (double)m / (double)c->lmax;
-            tw[m] = make_float2((float)cos(ang), (float)sin(ang));
+        float2** tabs[3] = {&c->twx, &c->twy, &c->twt};
+        const int lens[3] = {c->X, c->Y, c->T};
+        for (int k = 0; k < 3; k++) {
+            TRY(dalloc(c, tabs[k], (size_t)lens[k]));
+            std::vector<float2> tw(lens[k]);
+            for (int m = 0; m < lens[k]; m++) {
+                double ang = -2.0 * M_PI * (double)m / (double)lens[k];
+                tw[m] = make_float2((float)cos(ang), (float)sin(ang));
+            }
+            cudaError_t e = cudaMemcpy(*tabs[k], tw.data(), sizeof(float2) * lens[k], cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) { *out = c; return set_err(c, TM_ERR_CUDA, "twiddle upload: %s", cudaGetErrorString(e)); }
         }
-        cudaError_t e = cudaMemcpy(c->twid, tw.data(), sizeof(float2) * c->lmax, cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) { *out = c; return set_err(c, TM_ERR_CUDA, "twiddle upload: %s", cudaGetErrorString(e)); }
     }
     TRY(c->var->configure(c));
 #undef TRY

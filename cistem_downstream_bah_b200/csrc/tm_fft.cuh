@@ -3,10 +3,13 @@
 // An L-point complex transform is spread over P = L / R threads that each hold
 // R values in registers.  On entry thread t holds x[t + P*r] (r = 0..R-1); on
 // exit it holds X[t + P*r] (natural order, same stride).  Stages use radix R
-// except the last, which may use a smaller radix RL (RL divides R); between
-// stages the values go through a padded shared-memory buffer (Stockham
-// autosort: stage s reads element b + r*L/Rs and writes (b/Ns)*Ns*Rs + b%Ns +
-// r*Ns, with Ns the product of the earlier radices).
+// while R divides what is left of L, then the largest divisors of R that do
+// (a thread then does R/Rs butterflies of radix Rs); between stages the values
+// go through a padded shared-memory buffer (Stockham autosort: stage s reads
+// element b + r*L/Rs and writes (b/Ns)*Ns*Rs + b%Ns + r*Ns, with Ns the
+// product of the earlier radices).  Radices 2, 3, 4, 6, 8, 9, 12, 16, 18 and
+// 24 are available, which covers the 2^a 3^b sizes the micrograph
+// factorisation produces (match_template.cpp:527-583).
 //
 // Direction: DIR = -1 forward (exp(-2 pi i k n / L)), +1 inverse
 // (unnormalised), matching the reference's FFTW conventions
@@ -15,7 +18,43 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 namespace tmfft {
+
+// compile-time loop: f(std::integral_constant<int, i>) for i = 0..N-1
+template <class F, int... Is>
+__device__ __forceinline__ void sfor_impl(F&& f, std::integer_sequence<int, Is...>) {
+    (f(std::integral_constant<int, Is>{}), ...);
+}
+template <int N, class F>
+__device__ __forceinline__ void sfor(F&& f) {
+    sfor_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+// exp(2 pi i k / n) evaluated at compile time (Taylor series after reducing
+// the angle to [-pi, pi]); used for the constants inside the small DFTs
+__host__ __device__ constexpr double ct_angle(int k, int n) {
+    int m = ((k % n) + n) % n;
+    if (2 * m > n) m -= n;
+    return 2.0 * 3.14159265358979323846 * (double)m / (double)n;
+}
+__host__ __device__ constexpr double ct_sin(double x) {
+    double term = x, sum = x;
+    for (int i = 1; i < 30; i++) {
+        term *= -x * x / ((2.0 * i) * (2.0 * i + 1.0));
+        sum += term;
+    }
+    return sum;
+}
+__host__ __device__ constexpr double ct_cos(double x) {
+    double term = 1.0, sum = 1.0;
+    for (int i = 1; i < 30; i++) {
+        term *= -x * x / ((2.0 * i - 1.0) * (2.0 * i));
+        sum += term;
+    }
+    return sum;
+}
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
@@ -45,7 +84,8 @@ template <int P>
 __host__ __device__ constexpr int rd_off(int r) { return (P % 16 == 0) ? r * (P + P / 16) : P * r + ((P * r) >> 4); }
 
 // pad16(idxD + r*Ns) for the Stockham write of a stage with one radix-R
-// butterfly per thread (b = t): idxD = (t/Ns)*Ns*R + t%Ns; Ns == 1 or a multiple of 16
+// butterfly per thread (b = t): idxD = (t/Ns)*Ns*R + t%Ns; valid for Ns == 1
+// with R dividing 16, and for Ns a multiple of 16
 template <int R>
 __device__ __forceinline__ int wr_base(int t, int Ns) {
     return Ns == 1 ? pad16(R * t) : pad16((t / Ns) * Ns * R + (t % Ns));
@@ -124,12 +164,77 @@ __device__ __forceinline__ void dft16(float2* v) {
     for (int i = 0; i < 16; i++) v[i] = o[i];
 }
 
+template <int DIR>
+__device__ __forceinline__ void dft3(float2& a, float2& b, float2& c) {
+    // X1,2 = a - (b+c)/2 +- DIR i (sqrt(3)/2) (b-c)
+    constexpr float h = 0.86602540378443864676f;
+    const float2 sm = cadd(b, c), df = csub(b, c);
+    const float2 m = make_float2(fmaf(-0.5f, sm.x, a.x), fmaf(-0.5f, sm.y, a.y));
+    const float2 r = mul_i<DIR>(make_float2(h * df.x, h * df.y));
+    a = cadd(a, sm);
+    b = cadd(m, r);
+    c = csub(m, r);
+}
+
+// x * W_R^K with W_R = exp(DIR 2 pi i / R), K a compile-time constant
+template <int R, int K, int DIR>
+__device__ __forceinline__ float2 twc(float2 x) {
+    constexpr int k = ((K % R) + R) % R;
+    if constexpr (k == 0) return x;
+    else if constexpr (4 * k == R) return mul_i<DIR>(x);
+    else if constexpr (2 * k == R) return make_float2(-x.x, -x.y);
+    else if constexpr (4 * k == 3 * R) return mul_i<-DIR>(x);
+    else {
+        constexpr float c = (float)ct_cos(ct_angle(k, R));
+        constexpr float sn = (float)(DIR * ct_sin(ct_angle(k, R)));
+        return cmul(x, make_float2(c, sn));
+    }
+}
+
+template <int RS, int DIR>
+__device__ __forceinline__ void dft(float2* v);
+
+// R1*R2-point DFT in natural order: r = R2*r1 + r2, q = q1 + R1*q2
+// (R2 inner transforms of length R1, twiddles W_R^(r2 q1), R1 of length R2)
+template <int R1, int R2, int DIR>
+__device__ __forceinline__ void dft_pq(float2* v) {
+    constexpr int R = R1 * R2;
+    float2 u[R];
+    sfor<R2>([&](auto r2c) {
+        constexpr int r2 = decltype(r2c)::value;
+        float2 t[R1];
+#pragma unroll
+        for (int r1 = 0; r1 < R1; r1++) t[r1] = v[R2 * r1 + r2];
+        dft<R1, DIR>(t);
+        sfor<R1>([&](auto q1c) {
+            constexpr int q1 = decltype(q1c)::value;
+            u[r2 * R1 + q1] = twc<R, r2 * q1, DIR>(t[q1]);
+        });
+    });
+#pragma unroll
+    for (int q1 = 0; q1 < R1; q1++) {
+        float2 t[R2];
+#pragma unroll
+        for (int r2 = 0; r2 < R2; r2++) t[r2] = u[r2 * R1 + q1];
+        dft<R2, DIR>(t);
+#pragma unroll
+        for (int q2 = 0; q2 < R2; q2++) v[q1 + R1 * q2] = t[q2];
+    }
+}
+
 template <int RS, int DIR>
 __device__ __forceinline__ void dft(float2* v) {
     if constexpr (RS == 16) dft16<DIR>(v);
     else if constexpr (RS == 8) dft8<DIR>(v);
     else if constexpr (RS == 4) dft4<DIR>(v[0], v[1], v[2], v[3]);
     else if constexpr (RS == 2) dft2<DIR>(v[0], v[1]);
+    else if constexpr (RS == 3) dft3<DIR>(v[0], v[1], v[2]);
+    else if constexpr (RS == 6) dft_pq<3, 2, DIR>(v);
+    else if constexpr (RS == 9) dft_pq<3, 3, DIR>(v);
+    else if constexpr (RS == 12) dft_pq<4, 3, DIR>(v);
+    else if constexpr (RS == 18) dft_pq<9, 2, DIR>(v);
+    else if constexpr (RS == 24) dft_pq<8, 3, DIR>(v);
+    else static_assert(RS == 1, "unsupported radix");
 }
 
 // powers w^0 .. w^(n-1) by a shallow multiplication tree (depth <= 4)
@@ -155,7 +260,15 @@ __device__ __forceinline__ void powers(float2 w, float2* p) {
 // (depth <= 4) computed next to their use, so few of them are live at once.
 template <int RS>
 __device__ __forceinline__ void apply_twiddles(float2* e, float2 w) {
-    if constexpr (RS == 2) {
+    if constexpr (RS != 2 && RS != 4 && RS != 8 && RS != 16) {
+        // w^k by a product tree of depth log2(RS)
+        float2 p[RS];
+        p[1] = w;
+#pragma unroll
+        for (int k = 2; k < RS; k++) p[k] = cmul(p[k >> 1], p[k - (k >> 1)]);
+#pragma unroll
+        for (int k = 1; k < RS; k++) e[k] = cmul(e[k], p[k]);
+    } else if constexpr (RS == 2) {
         e[1] = cmul(e[1], w);
     } else if constexpr (RS == 4) {
         const float2 w2 = cmul(w, w);
@@ -188,27 +301,56 @@ __device__ __forceinline__ void apply_twiddles(float2* e, float2 w) {
     }
 }
 
-// Twiddle source: a table of W_LMAX^m = exp(-2 pi i m / LMAX), m = 0..LMAX-1,
-// for one power-of-two LMAX; W_L^m = table[m * (LMAX / L)].
+// Twiddle source: a table of W_LMAX^m = exp(-2 pi i m / LMAX), m = 0..LMAX-1;
+// W_L^m = table[(m mod L) * (LMAX / L)] for every L that divides LMAX.
 struct Twiddles {
     const float2* __restrict__ tab;
     int lmax;
     template <int DIR>
     __device__ __forceinline__ float2 w(int m, int L) const {
-        float2 t = __ldg(tab + (size_t)(m & (L - 1)) * (lmax / L));
+        const int mm = (L & (L - 1)) == 0 ? (m & (L - 1)) : (m % L);
+        float2 t = __ldg(tab + (size_t)mm * (lmax / L));
         return DIR < 0 ? t : conjf2(t);
     }
 };
 
-// Number of stages and radix of stage s for L = R^k * RL.
+// Radix plan of an L-point transform with R values per thread: R while R
+// divides what is left, then the largest divisors of R that divide the rest.
+struct RadixSeq {
+    int n;        // stages, -1 if L cannot be split this way
+    int r[24];
+};
+__host__ __device__ constexpr RadixSeq radix_seq(int L, int R) {
+    RadixSeq q{0, {}};
+    int m = L;
+    while (m > 1 && m % R == 0 && q.n < 24) {
+        q.r[q.n++] = R;
+        m /= R;
+    }
+    while (m > 1) {
+        int d = R;
+        while (d > 1 && !(R % d == 0 && m % d == 0)) d--;
+        if (d <= 1 || q.n >= 24) return RadixSeq{-1, {}};
+        q.r[q.n++] = d;
+        m /= d;
+    }
+    return q;
+}
+__host__ __device__ constexpr bool plannable(int L, int R) { return L % R == 0 && radix_seq(L, R).n > 0; }
+
 template <int L, int R>
 struct Plan {
-    static constexpr int full = [] { int n = 0, m = L; while (m % R == 0 && m > 1) { m /= R; n++; } return n; }();
-    static constexpr int RL = [] { int m = L; while (m % R == 0 && m > 1) m /= R; return m; }();
-    static constexpr int stages = full + (RL > 1 ? 1 : 0);
+    static constexpr RadixSeq seq = radix_seq(L, R);
+    static_assert(L % R == 0 && seq.n > 0, "transform length cannot be planned with this radix");
+    static constexpr int stages = seq.n;
     static constexpr int P = L / R;
-    static_assert(RL == 1 || R % RL == 0, "last radix must divide R");
-    __host__ __device__ static constexpr int radix(int s) { return s < full ? R : RL; }
+    __host__ __device__ static constexpr int radix(int s) { return seq.r[s]; }
+    // product of the radices of the stages before s
+    __host__ __device__ static constexpr int ns(int s) {
+        int n = 1;
+        for (int i = 0; i < s; i++) n *= seq.r[i];
+        return n;
+    }
 };
 
 // One cooperative FFT.  `sync` is a callable barrier over all threads that
@@ -219,47 +361,49 @@ template <int L, int R, int DIR, class Sync>
 __device__ __forceinline__ void fft(float2 (&v)[R], int t, float2* buf, const Twiddles& tw, Sync sync) {
     using PL = Plan<L, R>;
     constexpr int P = PL::P;
-    int Ns = 1;
-#pragma unroll
-    for (int s = 0; s < PL::stages; s++) {
-        const int RS = PL::radix(s);
-        const bool last = (s == PL::stages - 1);
+    sfor<PL::stages>([&](auto sc) {
+        constexpr int s = decltype(sc)::value;
+        constexpr int RS = PL::radix(s);
+        constexpr int Ns = PL::ns(s);
+        constexpr bool last = (s == PL::stages - 1);
         // twiddle base of this stage for the first butterfly, loaded before the
         // exchange so its latency hides behind the barrier and shared loads
         float2 w_first = make_float2(1.f, 0.f);
-        if (s > 0) w_first = tw.template w<DIR>((t % Ns) * (L / (Ns * RS)), L);
-        if (s > 0) {
+        if constexpr (s > 0) w_first = tw.template w<DIR>((t % Ns) * (L / (Ns * RS)), L);
+        if constexpr (s > 0) {
             // load stage input: x[t + P*r]
             sync();
-            const float2* rb = buf + rd_base<P>(t);
+            if constexpr (P % 16 == 0 || 16 % P == 0) {
+                const float2* rb = buf + rd_base<P>(t);
 #pragma unroll
-            for (int r = 0; r < R; r++) v[r] = rb[rd_off<P>(r)];
+                for (int r = 0; r < R; r++) v[r] = rb[rd_off<P>(r)];
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; r++) v[r] = buf[pad16(t + P * r)];
+            }
         }
         // butterflies: thread does R/RS of them, b = t + P*u, elements v[u + r*(R/RS)]
 #pragma unroll
-        for (int u = 0; u < R / (RS > 0 ? RS : 1); u++) {
+        for (int u = 0; u < R / RS; u++) {
             const int b = t + P * u;
-            float2 e[16];
+            float2 e[RS];
 #pragma unroll
             for (int r = 0; r < RS; r++) e[r] = v[u + r * (R / RS)];
-            if (s > 0) {
+            if constexpr (s > 0) {
                 const int jm = b % Ns;
                 const float2 w = (u == 0) ? w_first : tw.template w<DIR>(jm * (L / (Ns * RS)), L);
-                if (RS == 16) apply_twiddles<16>(e, w);
-                else if (RS == 8) apply_twiddles<8>(e, w);
-                else if (RS == 4) apply_twiddles<4>(e, w);
-                else if (RS == 2) apply_twiddles<2>(e, w);
+                apply_twiddles<RS>(e, w);
             }
-            if (RS == 16) dft16<DIR>(e);
-            else if (RS == 8) dft8<DIR>(e);
-            else if (RS == 4) dft4<DIR>(e[0], e[1], e[2], e[3]);
-            else if (RS == 2) dft2<DIR>(e[0], e[1]);
-            if (last) {
+            dft<RS, DIR>(e);
+            if constexpr (last) {
 #pragma unroll
                 for (int r = 0; r < RS; r++) v[u + r * (R / RS)] = e[r];
             } else {
                 if (u == 0) sync();  // previous readers of buf are done
-                if (RS == R && (Ns == 1 || Ns % 16 == 0)) {
+                // base + compile-time offsets equal pad16(idxD + r*Ns) when no
+                // 16-element boundary falls inside a butterfly (Ns == 1, R | 16)
+                // or every stride is a whole number of 16-blocks (16 | Ns)
+                if constexpr (RS == R && ((Ns == 1 && 16 % R == 0) || Ns % 16 == 0)) {
                     float2* wb = buf + wr_base<R>(b, Ns);
 #pragma unroll
                     for (int r = 0; r < RS; r++) wb[wr_off(r, Ns)] = e[r];
@@ -270,64 +414,7 @@ __device__ __forceinline__ void fft(float2 (&v)[R], int t, float2* buf, const Tw
                 }
             }
         }
-        Ns *= RS;
-    }
-}
-
-// Same transform as fft(), with the exchanges done through a float buffer of
-// padded_len(L) entries: real parts first, then imaginary parts.  Uses half
-// the shared memory of fft() at the cost of two extra barriers per exchange.
-template <int L, int R, int DIR, class Sync>
-__device__ __forceinline__ void fft_split(float2 (&v)[R], int t, float* buf, const Twiddles& tw, Sync sync) {
-    using PL = Plan<L, R>;
-    constexpr int P = PL::P;
-    int Ns = 1;
-#pragma unroll
-    for (int s = 0; s < PL::stages; s++) {
-        const int RS = PL::radix(s);
-        const bool last = (s == PL::stages - 1);
-#pragma unroll
-        for (int u = 0; u < R / (RS > 0 ? RS : 1); u++) {
-            const int b = t + P * u;
-            float2 e[16];
-#pragma unroll
-            for (int r = 0; r < RS; r++) e[r] = v[u + r * (R / RS)];
-            if (s > 0) {
-                const int jm = b % Ns;
-                const float2 w = tw.template w<DIR>(jm * (L / (Ns * RS)), L);
-                if (RS == 16) apply_twiddles<16>(e, w);
-                else if (RS == 8) apply_twiddles<8>(e, w);
-                else if (RS == 4) apply_twiddles<4>(e, w);
-                else if (RS == 2) apply_twiddles<2>(e, w);
-            }
-            if (RS == 16) dft16<DIR>(e);
-            else if (RS == 8) dft8<DIR>(e);
-            else if (RS == 4) dft4<DIR>(e[0], e[1], e[2], e[3]);
-            else if (RS == 2) dft2<DIR>(e[0], e[1]);
-#pragma unroll
-            for (int r = 0; r < RS; r++) v[u + r * (R / RS)] = e[r];
-        }
-        if (!last) {
-            // the next stage reads x[t + P*r]; this stage wrote (b/Ns)*Ns*Rs + b%Ns + r*Ns
-            // (non-last stages use RS == R, one butterfly per thread, b = t)
-            float* wb = buf + wr_base<R>(t, Ns);
-            const float* rb = buf + rd_base<P>(t);
-            float nre[R];
-            sync();
-#pragma unroll
-            for (int r = 0; r < R; r++) wb[wr_off(r, Ns)] = v[r].x;
-            sync();
-#pragma unroll
-            for (int r = 0; r < R; r++) nre[r] = rb[rd_off<P>(r)];
-            sync();
-#pragma unroll
-            for (int r = 0; r < R; r++) wb[wr_off(r, Ns)] = v[r].y;
-            sync();
-#pragma unroll
-            for (int r = 0; r < R; r++) v[r] = make_float2(nre[r], rb[rd_off<P>(r)]);
-        }
-        Ns *= RS;
-    }
+    });
 }
 
 }  // namespace tmfft

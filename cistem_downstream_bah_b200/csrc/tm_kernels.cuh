@@ -42,6 +42,19 @@ __host__ __device__ constexpr int round_up16(int v) { return (v + 15) / 16 * 16;
 // region stride >= len whose value mod 16 equals `rem` (bank skew between regions)
 __host__ __device__ constexpr int skewed(int len, int rem) { return round_up16(len) + rem; }
 
+// Length of the pruned forward transform of T non-zero samples inside an
+// N-point transform: the smallest L >= T that divides N and that the radix-V
+// plan can split.  The N-point spectrum is then N/L twiddled L-point
+// transforms of the zero-padded samples.
+__host__ __device__ constexpr int prune_len(int T, int N, int V) {
+    for (int L = T; L <= N; L++)
+        if (N % L == 0 && tmfft::plannable(L, V)) return L;
+    return -1;
+}
+// values per thread of the column transforms: 16 for powers of two, 18 for
+// heights with a factor 3
+__host__ __device__ constexpr int col_radix(int Y) { return Y % 3 == 0 ? 18 : 16; }
+
 struct BatchArgs {
     int nb;                       // orientations in this batch
     int orient0;                  // index of the batch's first orientation within the plane
@@ -66,7 +79,9 @@ struct BatchArgs {
     int* err;                     // device error flag (a bounded wait ran out)
     int XP;                       // row pitch (complex values) of A, C and Ip: X/2+1 rounded
                                   // up to a multiple of the pass-B column chunk
-    Twiddles tw;
+    Twiddles tw;                  // x axis (passes A and C): every length divides X
+    Twiddles twy;                 // y axis (pass B): every length divides Y
+    Twiddles twt;                 // template box (slice and projection kernels): lengths divide T
 };
 
 // --------------------------------------------------------------------------------------
@@ -135,23 +150,33 @@ __device__ __forceinline__ float2 interp3(const float2* __restrict__ vol, float 
 }
 
 // --------------------------------------------------------------------------------------
-// k_slice_colfft: block = 16 columns x (T/16) threads; grid = (ceil((T/2+1)/16), nb)
+// k_slice_colfft: block = CB columns x (T/V) threads (column fastest);
+// grid = (ceil((T/2+1)/CB), nb)
 template <int T>
-__global__ void __launch_bounds__(T)
+struct SliceCol {
+    static constexpr int V = T % 3 == 0 ? 24 : 16;   // values per thread
+    static constexpr int PT = T / V;                 // threads per column
+    static constexpr int RS = skewed(tmfft::padded_len(T), 1);
+    static constexpr int CB = (16 * RS * 8 <= 48 * 1024) ? 16 : 8;   // columns per block
+    static constexpr int NT = CB * PT;
+};
+
+template <int T>
+__global__ void __launch_bounds__(SliceCol<T>::NT)
 k_slice_colfft(BatchArgs a) {
+    using SC = SliceCol<T>;
     constexpr int TP = T / 2 + 1;
-    constexpr int PT = T / 16;
-    constexpr int RS = skewed(tmfft::padded_len(T), 1);
-    __shared__ float2 sm[16 * RS];
-    const int il = threadIdx.x & 15, tp = threadIdx.x >> 4;
-    const int i = blockIdx.x * 16 + il;
+    constexpr int PT = SC::PT, V = SC::V, CB = SC::CB, RS = SC::RS;
+    __shared__ float2 sm[CB * RS];
+    const int il = threadIdx.x % CB, tp = threadIdx.x / CB;
+    const int i = blockIdx.x * CB + il;
     const int o = blockIdx.y;
     const bool valid = i <= T / 2;
     const float* m = a.rot + 6 * (size_t)(a.orient0 + o);
     const float m00 = __ldg(m), m01 = __ldg(m + 1), m10 = __ldg(m + 2), m11 = __ldg(m + 3), m20 = __ldg(m + 4), m21 = __ldg(m + 5);
-    float2 v[16];
+    float2 v[V];
 #pragma unroll
-    for (int r = 0; r < 16; r++) {
+    for (int r = 0; r < V; r++) {
         const int y = tp + PT * r;
         const int j = y < T / 2 ? y : y - T;
         float2 val = make_float2(0.f, 0.f);
@@ -180,11 +205,11 @@ k_slice_colfft(BatchArgs a) {
         }
         v[r] = val;
     }
-    tmfft::fft<T, 16, +1>(v, tp, sm + il * RS, a.tw, [] __device__() { __syncthreads(); });
+    tmfft::fft<T, V, +1>(v, tp, sm + il * RS, a.twt, [] __device__() { __syncthreads(); });
     if (valid) {
         float2* out = a.S + (size_t)o * T * TP;
 #pragma unroll
-        for (int r = 0; r < 16; r++) out[(size_t)(tp + PT * r) * TP + i] = v[r];
+        for (int r = 0; r < V; r++) out[(size_t)(tp + PT * r) * TP + i] = v[r];
     }
 }
 
@@ -195,40 +220,43 @@ k_slice_colfft(BatchArgs a) {
 template <int T>
 struct RowC2R {
     static constexpr int H = T / 2;
-    static constexpr int PH = H / 16;                           // threads per row
-    static constexpr int ROWS = (256 / PH) < T ? (256 / PH) : T;  // rows per block
-    static constexpr int NT = ROWS * PH;
+    static constexpr int V = H % 3 == 0 ? 24 : 16;              // values per thread
+    static constexpr int PH = H / V;                            // threads per row
     static constexpr int RS = skewed(tmfft::padded_len(H), PH % 16);
+    static constexpr int ROWS0 = (256 / PH) < T ? (256 / PH) : T;
+    static constexpr int ROWS = (ROWS0 * RS * 8 <= 48 * 1024) ? ROWS0 : ROWS0 / 2;   // rows per block
+    static constexpr int NT = ROWS * PH;
+    static_assert(32 % PH == 0 || PH % 32 == 0, "row reductions use warp shuffles");
 };
 
 template <int T>
 __global__ void __launch_bounds__(RowC2R<T>::NT)
 k_row_c2r(BatchArgs a) {
     using RC = RowC2R<T>;
-    constexpr int TP = T / 2 + 1, H = RC::H, PH = RC::PH, ROWS = RC::ROWS;
+    constexpr int TP = T / 2 + 1, H = RC::H, PH = RC::PH, ROWS = RC::ROWS, V = RC::V;
     constexpr int RS = RC::RS;
     __shared__ float2 sm[ROWS * RS];
     const int t = threadIdx.x % PH, rl = threadIdx.x / PH;
     const int y = blockIdx.x * ROWS + rl;
     const int o = blockIdx.y;
     const float2* Hrow = a.S + ((size_t)o * T + y) * TP;
-    float2 v[16];
+    float2 v[V];
 #pragma unroll
-    for (int r = 0; r < 16; r++) {
+    for (int r = 0; r < V; r++) {
         const int k = t + PH * r;
         float2 hk = Hrow[k];
         float2 hm = Hrow[H - k];
         if (k == 0) { hk.y = 0.f; hm.y = 0.f; }
         const float2 e = make_float2(hk.x + hm.x, hk.y - hm.y);
         const float2 d = make_float2(hk.x - hm.x, hk.y + hm.y);
-        const float2 od = cmul(d, a.tw.template w<+1>(k, T));
+        const float2 od = cmul(d, a.twt.template w<+1>(k, T));
         v[r] = make_float2(e.x - od.y, e.y + od.x);
     }
-    tmfft::fft<H, 16, +1>(v, t, sm + rl * RS, a.tw, [] __device__() { __syncthreads(); });
+    tmfft::fft<H, V, +1>(v, t, sm + rl * RS, a.twt, [] __device__() { __syncthreads(); });
     float* prow = a.P + ((size_t)o * T + y) * T;
     float s = 0.f, q = 0.f;
 #pragma unroll
-    for (int r = 0; r < 16; r++) {
+    for (int r = 0; r < V; r++) {
         const int mm = t + PH * r;
         reinterpret_cast<float2*>(prow)[mm] = v[r];
         s += v[r].x + v[r].y;
@@ -293,13 +321,17 @@ k_norm(BatchArgs a, long long n_image) {
 }
 
 // --------------------------------------------------------------------------------------
-// k_pass_a: one block per (row, orientation); X/16 threads, thread j = s + MX*t'
+// k_pass_a: one block per (row, orientation); X/16 threads, thread j = s + MX*t'.
+// The T samples are the first T of an LA-point zero-padded input (LA = T when T
+// divides X).
 template <int T, int X>
 __global__ void __launch_bounds__(X / 16)
 k_pass_a(BatchArgs a) {
     const int XP = a.XP;
-    constexpr int MX = X / T, PT = T / 16;
-    constexpr int RS = skewed(tmfft::padded_len(T), 1);
+    constexpr int LA = prune_len(T, X, 16);
+    constexpr int MX = X / LA, PT = LA / 16;
+    constexpr int RS = skewed(tmfft::padded_len(LA), 1);
+    static_assert(LA > 0, "no pruned row transform for this template and width");
     __shared__ float2 sm[MX * RS];
     __shared__ float q[T];
     const int j = threadIdx.x;
@@ -315,11 +347,12 @@ k_pass_a(BatchArgs a) {
     float2 w = w0;
 #pragma unroll
     for (int r = 0; r < 16; r++) {
-        const float qv = q[tp + PT * r];
+        const int n = tp + PT * r;
+        const float qv = (LA == T || n < T) ? q[n] : 0.f;
         v[r] = make_float2(qv * w.x, qv * w.y);
         w = cmul(w, w1);
     }
-    tmfft::fft<T, 16, -1>(v, tp, sm + s * RS, a.tw, [] __device__() { __syncthreads(); });
+    tmfft::fft<LA, 16, -1>(v, tp, sm + s * RS, a.tw, [] __device__() { __syncthreads(); });
     float2* out = a.A + ((size_t)o * T + row) * XP;
 #pragma unroll
     for (int r = 0; r < 16; r++) {
@@ -329,37 +362,61 @@ k_pass_a(BatchArgs a) {
 }
 
 // --------------------------------------------------------------------------------------
-// k_pass_b: persistent; block = W columns x Y/16 threads (thread = c + W*j);
-// work item = (column chunk, orientation), orientation fastest.  Each thread
-// parks the 16 values of the prepared micrograph spectrum I' it multiplies
-// with in tensor memory (TMEM, 32 columns of its lane) for all orientations of
-// the chunk, which leaves shared memory to full complex exchange buffers.  The
-// rows of A for the next item stream in with cp.async while the current item
-// is transformed.
+// k_pass_b: persistent; block = W columns x P threads (thread = c + W*j,
+// P = Y/V); work item = (column chunk, orientation), orientation fastest.
+// Each thread parks the V values of the prepared micrograph spectrum I' it
+// multiplies with in tensor memory (TMEM, 2V columns of its lane) for all
+// orientations of the chunk, which leaves shared memory to full complex
+// exchange buffers; a trailing partial warp (when W*P is not a multiple of 32)
+// reads its I' values from global memory instead, since tcgen05 loads are
+// whole-warp operations.  The rows of A for the next item stream in with
+// cp.async while the current item is transformed.  The forward transform
+// along y is pruned: MY = Y/L twiddled L-point transforms of the T rows of A
+// zero-padded to L (L = T for power-of-two heights).
 template <int T, int Y>
 struct PassB {
-    static constexpr int W = (16384 / Y) < 16 ? (16384 / Y) : 16;   // columns per block
-    static constexpr int NT = W * (Y / 16);                         // threads per block
-    static constexpr int MY = Y / T, PT = T / 16;
+    static constexpr int V = col_radix(Y);                          // values per thread
+    static constexpr int P = Y / V;                                 // threads per column
+    static constexpr int W = (16 * P <= 1024) ? 16 : (8 * P <= 1024) ? 8 : (4 * P <= 1024) ? 4 : 2;   // columns per block
+    static constexpr int NT = W * P;                                // threads per block
+    static constexpr int L = prune_len(T, Y, V);                    // pruned forward length
+    static constexpr int MY = Y / L, PT = L / V;
+    static constexpr int FULL_WARPS = NT / 32;
     // bank skews (float2 units, half-warp = 16 lanes = (16/W) values of j x W columns)
-    static constexpr int RST = (tmfft::padded_len(T) + 15) / 16 * 16 + 1;       // == 1 (mod 16)
+    static constexpr int RST = (tmfft::padded_len(L) + 15) / 16 * 16 + 1;       // == 1 (mod 16)
     static constexpr int CS0 = (MY * RST > tmfft::padded_len(Y)) ? MY * RST : tmfft::padded_len(Y);
     static constexpr int CS = (CS0 + 15) / 16 * 16 + 16 / W;                  // == 16/W (mod 16)
     static constexpr size_t EXCH = (sizeof(float2) * W * CS + 15) / 16 * 16;
     static constexpr size_t ASZ = sizeof(float2) * T * W;           // one A staging buffer
     static constexpr int ABUFS = (EXCH + 2 * ASZ + 64 <= 232448) ? 2 : 1;
     static constexpr size_t SMEM = EXCH + ABUFS * ASZ + 64;         // + TMEM address slot
-    // TMEM: 32 columns per thread, NT/128 threads share a lane
-    static constexpr uint32_t TMEM_COLS = (NT / 128) * 32 < 32 ? 32 : (NT / 128) * 32;
-    static_assert(SMEM <= 232448, "pass B shared memory exceeds the per-block limit");
-    static_assert(NT % 128 == 0 && TMEM_COLS <= 512, "TMEM layout needs whole warp quads");
+    // TMEM: 2V columns per thread; the warps of one lane quadrant sit side by side
+    static constexpr int TCOLS = 2 * V;
+    static constexpr uint32_t TMEM_COLS = [] {
+        const int need = ((FULL_WARPS + 3) / 4) * TCOLS;
+        uint32_t n = 32;
+        while ((int)n < need) n *= 2;
+        return n;
+    }();
+    static_assert(L > 0 && Y % V == 0 && P % PT == 0, "no pruned plan for this template and height");
+    static_assert(NT <= 1024 && SMEM <= 232448, "pass B block exceeds the per-block limits");
+    static_assert(TMEM_COLS <= 512, "pass B TMEM layout exceeds 512 columns");
+    static_assert(V == 16 || V == 18, "TMEM load sequence covers 16 or 18 values");
 };
+
+// I' values of one thread (V complex, 2V floats) into its TMEM columns
+template <int V>
+__device__ __forceinline__ void tmem_put_values(uint32_t taddr, const float* f) {
+    tmptx::tmem_st16(taddr, f);
+    tmptx::tmem_st16(taddr + 16, f + 16);
+    if constexpr (V == 18) tmptx::tmem_st4(taddr + 32, f + 32);
+}
 
 template <int T, int Y>
 __global__ void __launch_bounds__(PassB<T, Y>::NT, 1)
 k_pass_b(BatchArgs a, int n_items) {
     using PB = PassB<T, Y>;
-    constexpr int W = PB::W, MY = PB::MY, PT = PB::PT, NT = PB::NT;
+    constexpr int W = PB::W, MY = PB::MY, PT = PB::PT, NT = PB::NT, V = PB::V, P = PB::P, L = PB::L;
     const int XP = a.XP;
     extern __shared__ __align__(16) unsigned char smem_b[];
     float2* exch = reinterpret_cast<float2*>(smem_b);
@@ -367,6 +424,7 @@ k_pass_b(BatchArgs a, int n_items) {
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem_b + PB::EXCH + PB::ABUFS * PB::ASZ);
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
+    const bool tmem_warp = warp < PB::FULL_WARPS;   // uniform per warp
     const int c = tid % W, j = tid / W;
     const int s = j % MY, tp = j / MY;
     float2* colbuf = exch + c * PB::CS;
@@ -383,7 +441,7 @@ k_pass_b(BatchArgs a, int n_items) {
     tmptx::tmem_fence_before_sync();
     __syncthreads();
     tmptx::tmem_fence_after_sync();
-    const uint32_t tmem = *tmem_slot + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(32 * (warp >> 2));
+    const uint32_t tmem = *tmem_slot + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(PB::TCOLS * (warp >> 2));
     auto issue_rows = [&](int it, float2* dst) {
         const int ch = it / a.nb, oo = it % a.nb;
         const float2* src = a.A + (size_t)oo * T * XP + ch * W;
@@ -400,9 +458,10 @@ k_pass_b(BatchArgs a, int n_items) {
         float2* anext = abuf + (PB::ABUFS == 2 ? ((kk + 1) & 1) : 0) * (T * W);
         const int chunk = it / a.nb, o = it % a.nb;
         const int kx0 = chunk * W;
+        const float2* Ic = a.Ip + kx0 + c;
         // twiddles of the pruned forward, W_Y^(s * (tp + PT*r)) = w0 * w1^r, loaded early
-        const float2 w0 = a.tw.template w<-1>(s * tp, Y);
-        const float2 w1 = a.tw.template w<-1>(s * PT, Y);
+        const float2 w0 = a.twy.template w<-1>(s * tp, Y);
+        const float2 w1 = a.twy.template w<-1>(s * PT, Y);
         // The buffer the next rows go into was last read at the start of the
         // previous item's forward transform, whose barriers every thread has
         // passed; the exchange buffers are guarded by the transforms' own barriers.
@@ -418,50 +477,55 @@ k_pass_b(BatchArgs a, int n_items) {
             tmptx::cp_async_wait<0>();
         }
         __syncthreads();  // this item's rows of A are visible to every thread
-        if (chunk != cur_chunk) {
-            // the 16 I' values this thread multiplies with, into its TMEM columns
-            const float2* Ic = a.Ip + kx0 + c;
-            float buf[16];
+        if (chunk != cur_chunk && tmem_warp) {
+            // the V I' values this thread multiplies with, into its TMEM columns
+            float buf[2 * V];
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-#pragma unroll
-                for (int r = 0; r < 8; r++) {
-                    const float2 iv = __ldg(Ic + (size_t)(j + (Y / 16) * (8 * h + r)) * XP);
-                    buf[2 * r] = iv.x;
-                    buf[2 * r + 1] = iv.y;
-                }
-                tmptx::tmem_st16(tmem + 16 * h, buf);
+            for (int r = 0; r < V; r++) {
+                const float2 iv = __ldg(Ic + (size_t)(j + P * r) * XP);
+                buf[2 * r] = iv.x;
+                buf[2 * r + 1] = iv.y;
             }
+            tmem_put_values<V>(tmem, buf);
             tmptx::tmem_wait_st();
-            cur_chunk = chunk;
         }
-        float2 v[16];
+        cur_chunk = chunk;
+        float2 v[V];
         {
             float2 w = w0;
 #pragma unroll
-            for (int r = 0; r < 16; r++) {
-                v[r] = cmul(acur[(tp + PT * r) * W + c], w);
+            for (int r = 0; r < V; r++) {
+                const int n = tp + PT * r;   // rows n >= T of the L-point input are zero
+                v[r] = (L == T || n < T) ? cmul(acur[n * W + c], w) : make_float2(0.f, 0.f);
                 w = cmul(w, w1);
             }
         }
-        tmfft::fft<T, 16, -1>(v, tp, fwdbuf, a.tw, sync);
-        // thread (s, tp) holds F[k], k = s + MY*(tp + PT*r) = j + (Y/16)*r
-        {
+        tmfft::fft<L, V, -1>(v, tp, fwdbuf, a.twy, sync);
+        // thread (s, tp) holds F[k], k = s + MY*(tp + PT*r) = j + P*r
+        if (tmem_warp) {
             float iv[16];
             tmptx::tmem_ld16(tmem, iv);
             tmptx::tmem_wait_ld();
-            float iw[16];
-            tmptx::tmem_ld16(tmem + 16, iw);   // in flight while the first half is multiplied
+            float iw[16], ix[4];
+            tmptx::tmem_ld16(tmem + 16, iw);   // in flight while the first values are multiplied
+            if constexpr (V == 18) tmptx::tmem_ld4(tmem + 32, ix);
 #pragma unroll
             for (int r = 0; r < 8; r++) v[r] = cmul_conj(make_float2(iv[2 * r], iv[2 * r + 1]), v[r]);
             tmptx::tmem_wait_ld();
 #pragma unroll
             for (int r = 0; r < 8; r++) v[8 + r] = cmul_conj(make_float2(iw[2 * r], iw[2 * r + 1]), v[8 + r]);
+            if constexpr (V == 18) {
+                v[16] = cmul_conj(make_float2(ix[0], ix[1]), v[16]);
+                v[17] = cmul_conj(make_float2(ix[2], ix[3]), v[17]);
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < V; r++) v[r] = cmul_conj(__ldg(Ic + (size_t)(j + P * r) * XP), v[r]);
         }
-        tmfft::fft<Y, 16, +1>(v, j, colbuf, a.tw, sync);
+        tmfft::fft<Y, V, +1>(v, j, colbuf, a.twy, sync);
         float2* Co = a.C + (size_t)o * Y * XP + kx0 + c;
 #pragma unroll
-        for (int r = 0; r < 16; r++) Co[(size_t)(j + (Y / 16) * r) * XP] = v[r];
+        for (int r = 0; r < V; r++) Co[(size_t)(j + P * r) * XP] = v[r];
     }
     tmptx::cp_async_wait<0>();
     tmptx::tmem_fence_before_sync();
@@ -602,5 +666,35 @@ __global__ void k_reset_state(float* mip, int* best, double* sum, double* sumsq,
         sumsq[i] = 0.0;
     }
 }
+
+// --------------------------------------------------------------------------------------
+// Launch shapes of one geometry, shared by every entry point.
+template <int T, int X, int Y>
+struct Launch {
+    using PB = PassB<T, Y>;
+    using PC = PassC<X>;
+    using SC = SliceCol<T>;
+    using RC = RowC2R<T>;
+    static constexpr int pass_b_width = PB::W;
+    static cudaError_t configure(int XP, int bins) {
+        cudaError_t e = cudaFuncSetAttribute(k_pass_b<T, Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB::SMEM);
+        if (e != cudaSuccess) return e;
+        return cudaFuncSetAttribute(k_pass_c<X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PC::smem_bytes(XP, bins));
+    }
+    // slice, projection, normalisation and row transforms
+    static void prep(BatchArgs& a, cudaStream_t s) {
+        k_slice_colfft<T><<<dim3((T / 2 + 1 + SC::CB - 1) / SC::CB, a.nb), SC::NT, 0, s>>>(a);
+        k_row_c2r<T><<<dim3(T / RC::ROWS, a.nb), RC::NT, 0, s>>>(a);
+        k_norm<T><<<(a.nb + 7) / 8, 256, 0, s>>>(a, (long long)X * Y);
+        k_pass_a<T, X><<<dim3(T, a.nb), X / 16, 0, s>>>(a);
+    }
+    static void pass_b(BatchArgs& a, cudaStream_t s, int nsm) {
+        const int n_items = (a.XP / PB::W) * a.nb;
+        k_pass_b<T, Y><<<n_items < nsm ? n_items : nsm, PB::NT, PB::SMEM, s>>>(a, n_items);
+    }
+    static void pass_c(BatchArgs& a, cudaStream_t s) {
+        k_pass_c<X><<<Y, X / 16, PC::smem_bytes(a.XP, a.hist_bins), s>>>(a, Y);
+    }
+};
 
 }  // namespace tmk

@@ -48,24 +48,14 @@ std::mutex g_setup_mutex;
 
 template <int T, int X, int Y>
 struct NoAllocImpl {
-    using PB = tmna::tmk::PassB<T, Y>;
-    using PC = tmna::tmk::PassC<X>;
-    using RC = tmna::tmk::RowC2R<T>;
-    static cudaError_t configure(int XP, int bins) {
-        cudaError_t e = cudaFuncSetAttribute(tmna::tmk::k_pass_b<T, Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB::SMEM);
-        if (e != cudaSuccess) return e;
-        return cudaFuncSetAttribute(tmna::tmk::k_pass_c<X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PC::smem_bytes(XP, bins));
-    }
+    using LN = tmna::tmk::Launch<T, X, Y>;
+    static cudaError_t configure(int XP, int bins) { return LN::configure(XP, bins); }
     static void run_batch(tmna::tmk::BatchArgs& a, cudaStream_t s, int nsm) {
-        tmna::tmk::k_slice_colfft<T><<<dim3((T / 2 + 1 + 15) / 16, a.nb), T, 0, s>>>(a);
-        tmna::tmk::k_row_c2r<T><<<dim3(T / RC::ROWS, a.nb), RC::NT, 0, s>>>(a);
-        tmna::tmk::k_norm<T><<<(a.nb + 7) / 8, 256, 0, s>>>(a, (long long)X * Y);
-        tmna::tmk::k_pass_a<T, X><<<dim3(T, a.nb), X / 16, 0, s>>>(a);
-        const int n_items = (a.XP / PB::W) * a.nb;
-        tmna::tmk::k_pass_b<T, Y><<<n_items < nsm ? n_items : nsm, PB::NT, PB::SMEM, s>>>(a, n_items);
-        tmna::tmk::k_pass_c<X><<<Y, X / 16, PC::smem_bytes(a.XP, a.hist_bins), s>>>(a, Y);
+        LN::prep(a, s);
+        LN::pass_b(a, s, nsm);
+        LN::pass_c(a, s);
     }
-    static int pass_b_width() { return PB::W; }
+    static int pass_b_width() { return LN::pass_b_width; }
 };
 
 struct NoAllocVariant {
@@ -224,6 +214,8 @@ extern "C" int tm_run_plane_noalloc(int device, const tm_dims* dims, const float
     a.err = reinterpret_cast<int*>(base + o_err);
     a.tw.tab = reinterpret_cast<const float2*>(base + o_tw);
     a.tw.lmax = lmax;
+    a.twy = a.tw;   // the geometries here are powers of two: X, Y and T divide lmax
+    a.twt = a.tw;
 
     // The array keeps the previous call's contents: rebuild the tables, clear
     // the error flag and the row spectra (their columns beyond X/2 are read as zero).
