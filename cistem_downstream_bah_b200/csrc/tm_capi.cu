@@ -89,7 +89,7 @@ int set_err(tm_ctx* c, int code, const char* fmt, ...) {
 
 struct Variant {
     int T, X, Y;
-    int W;   // pass-B column chunk
+    int W;   // row pitch alignment of the pass-B column chunks (columns)
     int (*run_batch)(tm_ctx*, tmk::BatchArgs&, bool timing);
     int (*configure)(tm_ctx*);
     int (*run_stages)(tm_ctx*, tmk::BatchArgs&);   // every kernel before the MIP epilogue

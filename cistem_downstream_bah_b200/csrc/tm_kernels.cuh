@@ -363,7 +363,10 @@ k_pass_a(BatchArgs a) {
 
 // --------------------------------------------------------------------------------------
 // k_pass_b: persistent; block = W columns x P threads (thread = c + W*j,
-// P = Y/V); work item = (column chunk, orientation), orientation fastest.
+// P = Y/V); work item = (column chunk, orientation), orientation fastest
+// (for 2-column chunks, the two chunks of a 4-column group alternate for each
+// orientation, so both halves of every 32-byte row sector are written one
+// item apart and merge in L2).
 // Each thread parks the V values of the prepared micrograph spectrum I' it
 // multiplies with in tensor memory (TMEM, 2V columns of its lane) for all
 // orientations of the chunk, which leaves shared memory to full complex
@@ -382,6 +385,9 @@ struct PassB {
     static constexpr int L = prune_len(T, Y, V);                    // pruned forward length
     static constexpr int MY = Y / L, PT = L / V;
     static constexpr int FULL_WARPS = NT / 32;
+    // chunks written back to back for one orientation, so that together they
+    // cover whole 32-byte sectors of a row (G > 1 only for 2-column chunks)
+    static constexpr int G = W >= 4 ? 1 : 4 / W;
     // bank skews (float2 units, half-warp = 16 lanes = (16/W) values of j x W columns)
     static constexpr int RST = (tmfft::padded_len(L) + 15) / 16 * 16 + 1;       // == 1 (mod 16)
     static constexpr int CS0 = (MY * RST > tmfft::padded_len(Y)) ? MY * RST : tmfft::padded_len(Y);
@@ -393,7 +399,7 @@ struct PassB {
     // TMEM: 2V columns per thread; the warps of one lane quadrant sit side by side
     static constexpr int TCOLS = 2 * V;
     static constexpr uint32_t TMEM_COLS = [] {
-        const int need = ((FULL_WARPS + 3) / 4) * TCOLS;
+        const int need = ((FULL_WARPS + 3) / 4) * TCOLS * G;
         uint32_t n = 32;
         while ((int)n < need) n *= 2;
         return n;
@@ -441,9 +447,13 @@ k_pass_b(BatchArgs a, int n_items) {
     tmptx::tmem_fence_before_sync();
     __syncthreads();
     tmptx::tmem_fence_after_sync();
-    const uint32_t tmem = *tmem_slot + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(PB::TCOLS * (warp >> 2));
+    constexpr int G = PB::G;
+    const uint32_t tmem = *tmem_slot + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(PB::TCOLS * G * (warp >> 2));
+    // item -> (chunk, orientation): group of G chunks outer, orientation, chunk in group inner
+    auto chunk_of = [&](int it) { return (it / (G * a.nb)) * G + it % G; };
+    auto orient_of = [&](int it) { return (it % (G * a.nb)) / G; };
     auto issue_rows = [&](int it, float2* dst) {
-        const int ch = it / a.nb, oo = it % a.nb;
+        const int ch = chunk_of(it), oo = orient_of(it);
         const float2* src = a.A + (size_t)oo * T * XP + ch * W;
         for (int e = tid; e < T * W; e += NT) tmptx::cp_async8(dst + e, src + (size_t)(e / W) * XP + (e % W));
     };
@@ -451,12 +461,13 @@ k_pass_b(BatchArgs a, int n_items) {
         issue_rows(it0, abuf);
         tmptx::cp_async_commit();
     }
-    int cur_chunk = -1;
+    int cur_group = -1;
     for (int it = it0; it < it1; it++) {
         const int kk = it - it0;
         const float2* acur = abuf + (PB::ABUFS == 2 ? (kk & 1) : 0) * (T * W);
         float2* anext = abuf + (PB::ABUFS == 2 ? ((kk + 1) & 1) : 0) * (T * W);
-        const int chunk = it / a.nb, o = it % a.nb;
+        const int chunk = chunk_of(it), o = orient_of(it);
+        const int group = chunk / G, slot = chunk % G;
         const int kx0 = chunk * W;
         const float2* Ic = a.Ip + kx0 + c;
         // twiddles of the pruned forward, W_Y^(s * (tp + PT*r)) = w0 * w1^r, loaded early
@@ -477,19 +488,25 @@ k_pass_b(BatchArgs a, int n_items) {
             tmptx::cp_async_wait<0>();
         }
         __syncthreads();  // this item's rows of A are visible to every thread
-        if (chunk != cur_chunk && tmem_warp) {
-            // the V I' values this thread multiplies with, into its TMEM columns
-            float buf[2 * V];
+        if (group != cur_group && tmem_warp) {
+            // the V I' values this thread multiplies with in each chunk of the
+            // group, into its TMEM columns
+#pragma unroll 1
+            for (int g = 0; g < G; g++) {
+                const float2* Ig = a.Ip + (group * G + g) * W + c;
+                float buf[2 * V];
 #pragma unroll
-            for (int r = 0; r < V; r++) {
-                const float2 iv = __ldg(Ic + (size_t)(j + P * r) * XP);
-                buf[2 * r] = iv.x;
-                buf[2 * r + 1] = iv.y;
+                for (int r = 0; r < V; r++) {
+                    const float2 iv = __ldg(Ig + (size_t)(j + P * r) * XP);
+                    buf[2 * r] = iv.x;
+                    buf[2 * r + 1] = iv.y;
+                }
+                tmem_put_values<V>(tmem + g * PB::TCOLS, buf);
             }
-            tmem_put_values<V>(tmem, buf);
             tmptx::tmem_wait_st();
         }
-        cur_chunk = chunk;
+        cur_group = group;
+        const uint32_t tslot = tmem + slot * PB::TCOLS;
         float2 v[V];
         {
             float2 w = w0;
@@ -504,11 +521,11 @@ k_pass_b(BatchArgs a, int n_items) {
         // thread (s, tp) holds F[k], k = s + MY*(tp + PT*r) = j + P*r
         if (tmem_warp) {
             float iv[16];
-            tmptx::tmem_ld16(tmem, iv);
+            tmptx::tmem_ld16(tslot, iv);
             tmptx::tmem_wait_ld();
             float iw[16], ix[4];
-            tmptx::tmem_ld16(tmem + 16, iw);   // in flight while the first values are multiplied
-            if constexpr (V == 18) tmptx::tmem_ld4(tmem + 32, ix);
+            tmptx::tmem_ld16(tslot + 16, iw);   // in flight while the first values are multiplied
+            if constexpr (V == 18) tmptx::tmem_ld4(tslot + 32, ix);
 #pragma unroll
             for (int r = 0; r < 8; r++) v[r] = cmul_conj(make_float2(iv[2 * r], iv[2 * r + 1]), v[r]);
             tmptx::tmem_wait_ld();
@@ -675,7 +692,7 @@ struct Launch {
     using PC = PassC<X>;
     using SC = SliceCol<T>;
     using RC = RowC2R<T>;
-    static constexpr int pass_b_width = PB::W;
+    static constexpr int pass_b_width = PB::W * PB::G;   // row pitch alignment (columns)
     static cudaError_t configure(int XP, int bins) {
         cudaError_t e = cudaFuncSetAttribute(k_pass_b<T, Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB::SMEM);
         if (e != cudaSuccess) return e;
