@@ -363,10 +363,11 @@ k_pass_a(BatchArgs a) {
 
 // --------------------------------------------------------------------------------------
 // k_pass_b: persistent; block = W columns x P threads (thread = c + W*j,
-// P = Y/V); work item = (column chunk, orientation), orientation fastest
-// (for 2-column chunks, the two chunks of a 4-column group alternate for each
-// orientation, so both halves of every 32-byte row sector are written one
-// item apart and merge in L2).
+// P = Y/V); work item = (group of G column chunks, orientation), orientation
+// fastest.  With 2-column chunks (tall micrographs, where 4 columns would need
+// more than 1024 threads) an item covers two chunks one after the other and
+// writes its 4 columns from shared memory, so every store fills whole 32-byte
+// row sectors (16-byte partial-sector stores cost DRAM read-modify-writes).
 // Each thread parks the V values of the prepared micrograph spectrum I' it
 // multiplies with in tensor memory (TMEM, 2V columns of its lane) for all
 // orientations of the chunk, which leaves shared memory to full complex
@@ -388,12 +389,13 @@ struct PassB {
     // chunks written back to back for one orientation, so that together they
     // cover whole 32-byte sectors of a row (G > 1 only for 2-column chunks)
     static constexpr int G = W >= 4 ? 1 : 4 / W;
+    static constexpr int WG = W * G;                                // columns per work item
     // bank skews (float2 units, half-warp = 16 lanes = (16/W) values of j x W columns)
     static constexpr int RST = (tmfft::padded_len(L) + 15) / 16 * 16 + 1;       // == 1 (mod 16)
     static constexpr int CS0 = (MY * RST > tmfft::padded_len(Y)) ? MY * RST : tmfft::padded_len(Y);
     static constexpr int CS = (CS0 + 15) / 16 * 16 + 16 / W;                  // == 16/W (mod 16)
-    static constexpr size_t EXCH = (sizeof(float2) * W * CS + 15) / 16 * 16;
-    static constexpr size_t ASZ = sizeof(float2) * T * W;           // one A staging buffer
+    static constexpr size_t EXCH = (sizeof(float2) * WG * CS + 15) / 16 * 16;
+    static constexpr size_t ASZ = sizeof(float2) * T * WG;          // one A staging buffer
     static constexpr int ABUFS = (EXCH + 2 * ASZ + 64 <= 232448) ? 2 : 1;
     static constexpr size_t SMEM = EXCH + ABUFS * ASZ + 64;         // + TMEM address slot
     // TMEM: 2V columns per thread; the warps of one lane quadrant sit side by side
@@ -433,8 +435,7 @@ k_pass_b(BatchArgs a, int n_items) {
     const bool tmem_warp = warp < PB::FULL_WARPS;   // uniform per warp
     const int c = tid % W, j = tid / W;
     const int s = j % MY, tp = j / MY;
-    float2* colbuf = exch + c * PB::CS;
-    float2* fwdbuf = colbuf + s * PB::RST;
+    constexpr int G = PB::G, WG = PB::WG;
     auto sync = [] __device__() { __syncthreads(); };
     const int per = (n_items + gridDim.x - 1) / gridDim.x;
     const int it0 = blockIdx.x * per;
@@ -447,15 +448,11 @@ k_pass_b(BatchArgs a, int n_items) {
     tmptx::tmem_fence_before_sync();
     __syncthreads();
     tmptx::tmem_fence_after_sync();
-    constexpr int G = PB::G;
     const uint32_t tmem = *tmem_slot + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(PB::TCOLS * G * (warp >> 2));
-    // item -> (chunk, orientation): group of G chunks outer, orientation, chunk in group inner
-    auto chunk_of = [&](int it) { return (it / (G * a.nb)) * G + it % G; };
-    auto orient_of = [&](int it) { return (it % (G * a.nb)) / G; };
     auto issue_rows = [&](int it, float2* dst) {
-        const int ch = chunk_of(it), oo = orient_of(it);
-        const float2* src = a.A + (size_t)oo * T * XP + ch * W;
-        for (int e = tid; e < T * W; e += NT) tmptx::cp_async8(dst + e, src + (size_t)(e / W) * XP + (e % W));
+        const int grp = it / a.nb, oo = it % a.nb;
+        const float2* src = a.A + (size_t)oo * T * XP + grp * WG;
+        for (int e = tid; e < T * WG; e += NT) tmptx::cp_async8(dst + e, src + (size_t)(e / WG) * XP + (e % WG));
     };
     if (PB::ABUFS == 2) {
         issue_rows(it0, abuf);
@@ -464,12 +461,10 @@ k_pass_b(BatchArgs a, int n_items) {
     int cur_group = -1;
     for (int it = it0; it < it1; it++) {
         const int kk = it - it0;
-        const float2* acur = abuf + (PB::ABUFS == 2 ? (kk & 1) : 0) * (T * W);
-        float2* anext = abuf + (PB::ABUFS == 2 ? ((kk + 1) & 1) : 0) * (T * W);
-        const int chunk = chunk_of(it), o = orient_of(it);
-        const int group = chunk / G, slot = chunk % G;
-        const int kx0 = chunk * W;
-        const float2* Ic = a.Ip + kx0 + c;
+        const float2* acur = abuf + (PB::ABUFS == 2 ? (kk & 1) : 0) * (T * WG);
+        float2* anext = abuf + (PB::ABUFS == 2 ? ((kk + 1) & 1) : 0) * (T * WG);
+        const int group = it / a.nb, o = it % a.nb;
+        const int kx0 = group * WG;
         // twiddles of the pruned forward, W_Y^(s * (tp + PT*r)) = w0 * w1^r, loaded early
         const float2 w0 = a.twy.template w<-1>(s * tp, Y);
         const float2 w1 = a.twy.template w<-1>(s * PT, Y);
@@ -493,7 +488,7 @@ k_pass_b(BatchArgs a, int n_items) {
             // group, into its TMEM columns
 #pragma unroll 1
             for (int g = 0; g < G; g++) {
-                const float2* Ig = a.Ip + (group * G + g) * W + c;
+                const float2* Ig = a.Ip + kx0 + g * W + c;
                 float buf[2 * V];
 #pragma unroll
                 for (int r = 0; r < V; r++) {
@@ -506,43 +501,65 @@ k_pass_b(BatchArgs a, int n_items) {
             tmptx::tmem_wait_st();
         }
         cur_group = group;
-        const uint32_t tslot = tmem + slot * PB::TCOLS;
-        float2 v[V];
-        {
-            float2 w = w0;
+#pragma unroll 1
+        for (int g = 0; g < G; g++) {
+            const int col = g * W + c;   // column within the item
+            float2* colbuf = exch + col * PB::CS;
+            float2* fwdbuf = colbuf + s * PB::RST;
+            const uint32_t tslot = tmem + g * PB::TCOLS;
+            float2 v[V];
+            {
+                float2 w = w0;
 #pragma unroll
-            for (int r = 0; r < V; r++) {
-                const int n = tp + PT * r;   // rows n >= T of the L-point input are zero
-                v[r] = (L == T || n < T) ? cmul(acur[n * W + c], w) : make_float2(0.f, 0.f);
-                w = cmul(w, w1);
+                for (int r = 0; r < V; r++) {
+                    const int n = tp + PT * r;   // rows n >= T of the L-point input are zero
+                    v[r] = (L == T || n < T) ? cmul(acur[n * WG + col], w) : make_float2(0.f, 0.f);
+                    w = cmul(w, w1);
+                }
+            }
+            tmfft::fft<L, V, -1>(v, tp, fwdbuf, a.twy, sync);
+            // thread (s, tp) holds F[k], k = s + MY*(tp + PT*r) = j + P*r
+            if (tmem_warp) {
+                float iv[16];
+                tmptx::tmem_ld16(tslot, iv);
+                tmptx::tmem_wait_ld();
+                float iw[16], ix[4];
+                tmptx::tmem_ld16(tslot + 16, iw);   // in flight while the first values are multiplied
+                if constexpr (V == 18) tmptx::tmem_ld4(tslot + 32, ix);
+#pragma unroll
+                for (int r = 0; r < 8; r++) v[r] = cmul_conj(make_float2(iv[2 * r], iv[2 * r + 1]), v[r]);
+                tmptx::tmem_wait_ld();
+#pragma unroll
+                for (int r = 0; r < 8; r++) v[8 + r] = cmul_conj(make_float2(iw[2 * r], iw[2 * r + 1]), v[8 + r]);
+                if constexpr (V == 18) {
+                    v[16] = cmul_conj(make_float2(ix[0], ix[1]), v[16]);
+                    v[17] = cmul_conj(make_float2(ix[2], ix[3]), v[17]);
+                }
+            } else {
+                const float2* Ic = a.Ip + kx0 + col;
+#pragma unroll
+                for (int r = 0; r < V; r++) v[r] = cmul_conj(__ldg(Ic + (size_t)(j + P * r) * XP), v[r]);
+            }
+            tmfft::fft<Y, V, +1>(v, j, colbuf, a.twy, sync);
+            if constexpr (G == 1) {
+                float2* Co = a.C + (size_t)o * Y * XP + kx0 + col;
+#pragma unroll
+                for (int r = 0; r < V; r++) Co[(size_t)(j + P * r) * XP] = v[r];
+            } else {
+                sync();   // every thread has read its last-stage inputs from colbuf
+#pragma unroll
+                for (int r = 0; r < V; r++) colbuf[tmfft::pad16(j + P * r)] = v[r];
             }
         }
-        tmfft::fft<L, V, -1>(v, tp, fwdbuf, a.twy, sync);
-        // thread (s, tp) holds F[k], k = s + MY*(tp + PT*r) = j + P*r
-        if (tmem_warp) {
-            float iv[16];
-            tmptx::tmem_ld16(tslot, iv);
-            tmptx::tmem_wait_ld();
-            float iw[16], ix[4];
-            tmptx::tmem_ld16(tslot + 16, iw);   // in flight while the first values are multiplied
-            if constexpr (V == 18) tmptx::tmem_ld4(tslot + 32, ix);
-#pragma unroll
-            for (int r = 0; r < 8; r++) v[r] = cmul_conj(make_float2(iv[2 * r], iv[2 * r + 1]), v[r]);
-            tmptx::tmem_wait_ld();
-#pragma unroll
-            for (int r = 0; r < 8; r++) v[8 + r] = cmul_conj(make_float2(iw[2 * r], iw[2 * r + 1]), v[8 + r]);
-            if constexpr (V == 18) {
-                v[16] = cmul_conj(make_float2(ix[0], ix[1]), v[16]);
-                v[17] = cmul_conj(make_float2(ix[2], ix[3]), v[17]);
+        if constexpr (G > 1) {
+            // the item's WG columns, row by row: whole 32-byte sectors per row
+            sync();
+            float2* Co = a.C + (size_t)o * Y * XP + kx0;
+            for (int e = tid; e < Y * WG; e += NT) {
+                const int row = e / WG, cc = e % WG;
+                Co[(size_t)row * XP + cc] = exch[cc * PB::CS + tmfft::pad16(row)];
             }
-        } else {
-#pragma unroll
-            for (int r = 0; r < V; r++) v[r] = cmul_conj(__ldg(Ic + (size_t)(j + P * r) * XP), v[r]);
         }
-        tmfft::fft<Y, V, +1>(v, j, colbuf, a.twy, sync);
-        float2* Co = a.C + (size_t)o * Y * XP + kx0 + c;
-#pragma unroll
-        for (int r = 0; r < V; r++) Co[(size_t)(j + P * r) * XP] = v[r];
     }
     tmptx::cp_async_wait<0>();
     tmptx::tmem_fence_before_sync();
@@ -692,7 +709,7 @@ struct Launch {
     using PC = PassC<X>;
     using SC = SliceCol<T>;
     using RC = RowC2R<T>;
-    static constexpr int pass_b_width = PB::W * PB::G;   // row pitch alignment (columns)
+    static constexpr int pass_b_width = PB::WG;   // row pitch alignment (columns)
     static cudaError_t configure(int XP, int bins) {
         cudaError_t e = cudaFuncSetAttribute(k_pass_b<T, Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB::SMEM);
         if (e != cudaSuccess) return e;
@@ -706,7 +723,7 @@ struct Launch {
         k_pass_a<T, X><<<dim3(T, a.nb), X / 16, 0, s>>>(a);
     }
     static void pass_b(BatchArgs& a, cudaStream_t s, int nsm) {
-        const int n_items = (a.XP / PB::W) * a.nb;
+        const int n_items = (a.XP / PB::WG) * a.nb;
         k_pass_b<T, Y><<<n_items < nsm ? n_items : nsm, PB::NT, PB::SMEM, s>>>(a, n_items);
     }
     static void pass_c(BatchArgs& a, cudaStream_t s) {
