@@ -47,6 +47,14 @@ WORKLOADS = {
     "full": dict(name="4096x4096 micrograph, 256^3 template @1.0 A/px, C1 2.5/1.5 deg grid",
                  nx=4096, ny=4096, T=256, pixel_size=1.0, n_atoms=120000, radius_A=110.0, particles=80,
                  snr=0.03, defocus=12000.0, angular_step=2.5, psi_step=1.5),
+    # the CPU-runnable configuration
+    "cpu1024": dict(name="1024x1024 micrograph, 64^3 template @1.5 A/px, C1 15/15 deg grid",
+                    nx=1024, ny=1024, T=64, pixel_size=1.5, n_atoms=3000, radius_A=40.0, particles=10,
+                    snr=0.05, defocus=12000.0, angular_step=15.0, psi_step=15.0),
+    # the coarse search of the learned-proposal configuration
+    "coarse": dict(name="4096x4096 micrograph, 256^3 template @1.0 A/px, C1 7.5/5.0 deg grid (coarse)",
+                   nx=4096, ny=4096, T=256, pixel_size=1.0, n_atoms=120000, radius_A=110.0, particles=80,
+                   snr=0.03, defocus=12000.0, angular_step=7.5, psi_step=5.0),
     # the uneven micrograph sizes of the batched configuration, one at a time
     "uneven3710": dict(name="3838x3710 micrograph (padded 4096x3888), 256^3 template @1.0 A/px, C1 3.0/2.0 deg grid",
                        nx=3838, ny=3710, T=256, pixel_size=1.0, n_atoms=120000, radius_A=110.0, particles=70,

@@ -5,6 +5,7 @@
 #include <string>
 
 #include "mrc.hpp"
+#include "peaks.hpp"
 #include "prep.hpp"
 
 #define TMH_API extern "C" __attribute__((visibility("default")))
@@ -98,4 +99,20 @@ TMH_API int tmh_mrc_read(const char* path, float* out) {
 TMH_API int tmh_mrc_write(const char* path, int nx, int ny, int nz, const float* data, float pixel_size) {
     std::string err;
     return write_mrc(path, nx, ny, nz, data, pixel_size, err) ? 0 : -1;
+}
+
+// peak list of a scaled MIP (modified copy); out receives 10 floats per peak:
+// x_pos, y_pos, psi, theta, phi, defocus, pixel_size, peak_height, x, y
+TMH_API int tmh_find_peaks(int nx, int ny, const float* scaled_mip, const float* psi, const float* theta,
+                           const float* phi, const float* defocus, const float* pixel, float threshold,
+                           int min_peak_radius, int template_size, float pixel_size, float* out, int max_peaks) {
+    std::vector<float> m(scaled_mip, scaled_mip + (size_t)nx * ny);
+    auto pk = find_peaks(nx, ny, m, psi, theta, phi, defocus, pixel, threshold, min_peak_radius, template_size,
+                         pixel_size, max_peaks);
+    for (size_t k = 0; k < pk.size(); k++) {
+        float* o = out + 10 * k;
+        o[0] = pk[k].x_pos; o[1] = pk[k].y_pos; o[2] = pk[k].psi; o[3] = pk[k].theta; o[4] = pk[k].phi;
+        o[5] = pk[k].defocus; o[6] = pk[k].pixel_size; o[7] = pk[k].peak_height; o[8] = (float)pk[k].x; o[9] = (float)pk[k].y;
+    }
+    return (int)pk.size();
 }

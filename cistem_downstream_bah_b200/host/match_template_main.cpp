@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "mrc.hpp"
+#include "peaks.hpp"
 #include "prep.hpp"
 #include "template_matching_core.hpp"
 
@@ -463,6 +464,27 @@ int run(const JobArgs& a) {
                      survival[i], expected[i]);
     if (std::fclose(hf) != 0) throw CoreError(TM_ERR_INVALID, "write failed for " + a.output_histogram_file);
     std::printf("Expected threshold = %.2f\n", expected_threshold);
+
+    // Peak list (the reference's result aggregation, match_template.cpp:1838-1975):
+    // written when the result file argument (38) names a file.  The reference
+    // stores these records in its project database and draws a projection
+    // montage into that file; this program writes the records as text.
+    if (!a.result_output_filename.empty() && a.result_output_filename != "/dev/null") {
+        Image2 z = out(scaled, true), ps = out(best_psi, false), th = out(best_theta, false), ph = out(best_phi, false);
+        Image2 df = out(best_defocus, false), px = out(best_pixel, false);
+        const auto peaks = find_peaks(z.nx, z.ny, z.v, ps.v.data(), th.v.data(), ph.v.data(), df.v.data(), px.v.data(),
+                                      expected_threshold, (int)a.min_peak_radius, T, a.pixel_size);
+        FILE* pf = std::fopen(a.result_output_filename.c_str(), "w");
+        if (!pf) throw CoreError(TM_ERR_INVALID, "cannot write " + a.result_output_filename);
+        std::fprintf(pf, "# %zu peaks above the expected threshold %.2f (min peak radius %d px)\n", peaks.size(),
+                     expected_threshold, (int)a.min_peak_radius);
+        std::fprintf(pf, "# x (A), y (A), psi, theta, phi, defocus, pixel size, peak height\n");
+        for (const PeakInfo& p : peaks)
+            std::fprintf(pf, "%f %f %f %f %f %f %f %f\n", p.x_pos, p.y_pos, p.psi, p.theta, p.phi, p.defocus,
+                         p.pixel_size, p.peak_height);
+        if (std::fclose(pf) != 0) throw CoreError(TM_ERR_INVALID, "write failed for " + a.result_output_filename);
+        std::printf("%zu peaks written to %s\n", peaks.size(), a.result_output_filename.c_str());
+    }
     return 0;
 }
 

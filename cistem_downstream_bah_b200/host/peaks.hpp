@@ -1,0 +1,27 @@
+// peaks.hpp -- peak list of a finished search: the loop of the reference's
+// result aggregation (src/programs/match_template/match_template.cpp:1838-1975)
+// over the scaled MIP, with Image::FindPeakWithIntegerCoordinates
+// (src/core/image.cpp:9961-10110) as the peak search.
+#pragma once
+#include <vector>
+
+namespace tmhost {
+
+struct PeakInfo {
+    float x_pos, y_pos;          // Angstrom (pixel coordinate x pixel size)
+    float psi, theta, phi;       // degrees
+    float defocus, pixel_size;   // offsets recorded by the search
+    float peak_height;           // scaled MIP (z-score) at the peak
+    int x, y;                    // pixel coordinates
+};
+
+// Repeatedly takes the first maximum of `scaled_mip` in scan order among
+// pixels at least template_size/4+1 from every edge, stops when it is below
+// `threshold`, records the best orientation there and blanks a disc of
+// radius `min_peak_radius` pixels (the reference's half-open square bounds).
+// `scaled_mip` is modified.  At most max_peaks peaks (the reference stops at 1000).
+std::vector<PeakInfo> find_peaks(int nx, int ny, std::vector<float>& scaled_mip, const float* psi, const float* theta,
+                                 const float* phi, const float* defocus, const float* pixel, float threshold,
+                                 int min_peak_radius, int template_size, float pixel_size, int max_peaks = 1000);
+
+}  // namespace tmhost

@@ -21,7 +21,7 @@ _lib = None
 EXPORTED = [
     "tmh_whiten", "tmh_template_spectrum", "tmh_projection_filter", "tmh_search_grid", "tmh_psi_list",
     "tmh_factorize_dimension", "tmh_is_power_of_two", "tmh_angular_step", "tmh_erfcinv", "tmh_edge_mean",
-    "tmh_clip_into", "tmh_rotate90", "tmh_mrc_info", "tmh_mrc_read", "tmh_mrc_write",
+    "tmh_clip_into", "tmh_rotate90", "tmh_mrc_info", "tmh_mrc_read", "tmh_mrc_write", "tmh_find_peaks",
 ]
 
 
@@ -59,6 +59,8 @@ def lib() -> ctypes.CDLL:
         L.tmh_mrc_read.restype = i
         L.tmh_mrc_write.argtypes = [ctypes.c_char_p, i, i, i, P, f]
         L.tmh_mrc_write.restype = i
+        L.tmh_find_peaks.argtypes = [i, i, P, P, P, P, P, P, f, i, i, f, P, i]
+        L.tmh_find_peaks.restype = i
         _lib = L
     return _lib
 
@@ -155,3 +157,16 @@ def write_mrc(path, data, pixel_size=1.0):
     nz, ny, nx = a.shape
     if lib().tmh_mrc_write(str(path).encode(), nx, ny, nz, _p(a), pixel_size) != 0:
         raise OSError(f"cannot write MRC file {path}")
+
+
+def find_peaks(scaled_mip, psi, theta, phi, defocus, pixel, threshold, min_peak_radius, template_size, pixel_size,
+               max_peaks=1000):
+    """Peak records (one row each: x_pos, y_pos, psi, theta, phi, defocus,
+    pixel_size, peak_height, x, y) of a scaled MIP, as the reference's result
+    aggregation finds them."""
+    arrs = [_f32(a) for a in (scaled_mip, psi, theta, phi, defocus, pixel)]
+    ny, nx = arrs[0].shape
+    out = np.zeros((max_peaks, 10), np.float32)
+    n = lib().tmh_find_peaks(nx, ny, *[_p(a) for a in arrs], float(threshold), int(min_peak_radius),
+                             int(template_size), float(pixel_size), _p(out), max_peaks)
+    return out[:n].copy()

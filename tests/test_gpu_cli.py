@@ -28,7 +28,7 @@ def _run_cli(tmp, img_path, tpl_path):
     args = [img_path, tpl_path, PIXEL, 300.0, 2.7, 0.07, DEFOCUS, DEFOCUS, 0.0, 300.0, 8.0, STEP, 20,
             DF_RANGE, DF_STEP, 0.0, 0.0, 1.0, "no", 0.0, 0.0,
             f["mip"], f["psi"], f["theta"], f["phi"], f["defocus"], f["pixel"], f["scaled"], f["avg"], "C1",
-            PSI_STEP, str(tmp / "hist.txt"), -1, -1, 0, 0, f["std"], "/dev/null", "/dev/null", 10.0, "yes", 1]
+            PSI_STEP, str(tmp / "hist.txt"), -1, -1, 0, 0, f["std"], "/dev/null", str(tmp / "peaks.txt"), 10.0, "yes", 1]
     assert len(args) == 42
     r = subprocess.run([H.CLI_PATH, *map(str, args)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
@@ -109,3 +109,18 @@ def test_match_template_program_matches_oracle(tmp_path):
         y, x = int(round(py)), int(round(px))
         win = got["scaled"][max(0, y - 3):y + 4, max(0, x - 3):x + 4]
         assert win.max() > 4.0, (px, py, win.max())
+    # the peak list (argument 38): the reference's peak loop on the written maps,
+    # and every planted particle away from the edges is among the peaks
+    rows = [ln.split() for ln in open(tmp_path / "peaks.txt").read().splitlines() if not ln.startswith("#")]
+    peaks = np.array(rows, np.float32).reshape(-1, 8)
+    ref_peaks = H.find_peaks(got["scaled"], got["psi"], got["theta"], got["phi"], got["defocus"], got["pixel"],
+                             threshold=float(np.float32(np.sqrt(np.float32(2.0))) *
+                                             np.float32(O.erfcinv(2.0 / (256.0 * 250.0 * ref["n_total"])))),
+                             min_peak_radius=10, template_size=T,
+                             pixel_size=PIXEL)
+    assert np.allclose(peaks, ref_peaks[:, :8], rtol=1e-5, atol=1e-3)
+    for (px, py) in truth["positions"]:
+        if min(px, py, 256 - px, 250 - py) < T // 4 + 2:
+            continue
+        d = np.hypot(peaks[:, 0] / PIXEL - px, peaks[:, 1] / PIXEL - py)
+        assert d.min() < 3.0, (px, py, d.min())

@@ -179,3 +179,40 @@ def test_cli_rejects_blank_scripted_answer(tmp_path):
     r = subprocess.run([H.CLI_PATH], input="\n", capture_output=True, text=True, timeout=60)
     assert r.returncode != 0
     assert "Blank answer in scripted mode" in r.stdout
+
+
+def _reference_peaks(z, maps, threshold, radius, T, pixel_size):
+    """The reference's peak loop (match_template.cpp:1865-1928) in numpy."""
+    z = z.copy()
+    ny, nx = z.shape
+    e = T // 4 + 1
+    out = []
+    while len(out) < 1000:
+        sub = z[e:ny - e + 1, e:nx - e + 1]
+        k = int(np.argmax(sub))            # first maximum in scan order
+        j, i = divmod(k, sub.shape[1])
+        j, i = j + e, i + e
+        if z[j, i] < threshold:
+            break
+        rec = [i * pixel_size, j * pixel_size] + [m[j, i] for m in maps] + [z[j, i]]
+        for jj in range(max(j - radius, 0), min(j + radius, ny)):
+            for ii in range(max(i - radius, 0), min(i + radius, nx)):
+                if (ii - i) ** 2 + (jj - j) ** 2 <= radius * radius:
+                    z[jj, ii] = -np.finfo(np.float32).max
+        out.append(rec)
+    return np.array(out, np.float32).reshape(-1, 8)
+
+
+def test_peak_list_matches_the_reference_loop():
+    rng = np.random.default_rng(7)
+    ny, nx, T = 120, 150, 32
+    z = rng.normal(size=(ny, nx)).astype(np.float32)
+    for (y, x, h) in ((30, 40, 12.0), (31, 44, 11.0), (90, 100, 9.0), (60, 10, 15.0), (5, 75, 20.0)):
+        z[y, x] = h
+    maps = [rng.uniform(0, 360, size=(ny, nx)).astype(np.float32) for _ in range(3)] + \
+        [rng.choice([-200.0, 0.0, 200.0], size=(ny, nx)).astype(np.float32), np.zeros((ny, nx), np.float32)]
+    ref = _reference_peaks(z, maps, 8.0, 10, T, 1.5)
+    got = H.find_peaks(z, *maps, threshold=8.0, min_peak_radius=10, template_size=T, pixel_size=1.5)
+    # (5, 75) lies within T/4+1 of an edge; (31, 44) is blanked by (30, 40)
+    assert [tuple(int(v) for v in p) for p in got[:, 8:]] == [(10, 60), (40, 30), (100, 90)]
+    assert np.array_equal(got[:, :8], ref)
