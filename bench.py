@@ -349,8 +349,8 @@ def cpu_baseline(inp, sample=None):
     secs = _oracle_sample(inp, n)
     pts = WORKLOAD["nx"] * WORKLOAD["ny"] * n / secs
     return {"value": pts, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"first {n} orientations of the grid on the full 4096^2 micrograph, FP32 oracle build, "
-                      f"{threads} OpenMP threads, {secs:.1f} s"}
+            "sample": f"first {n} orientations of the grid on the full {inp['X']}x{inp['Y']} (padded) micrograph, "
+                      f"FP32 oracle build, {threads} OpenMP threads, {secs:.1f} s"}
 
 
 def run_reference(args):

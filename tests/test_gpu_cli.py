@@ -119,8 +119,11 @@ def test_match_template_program_matches_oracle(tmp_path):
                              min_peak_radius=10, template_size=T,
                              pixel_size=PIXEL)
     assert np.allclose(peaks, ref_peaks[:, :8], rtol=1e-5, atol=1e-3)
+    thr = float(lines[0].split("=")[1])
+    assert len(peaks) >= 1 and np.all(peaks[:, 7] >= thr - 0.01)
     for (px, py) in truth["positions"]:
-        if min(px, py, 256 - px, 250 - py) < T // 4 + 2:
-            continue
+        y, x = int(round(py)), int(round(px))
+        if min(px, py, 256 - px, 250 - py) < T // 4 + 2 or got["scaled"][y - 3:y + 4, x - 3:x + 4].max() < thr + 0.5:
+            continue   # near an edge, or not above the threshold
         d = np.hypot(peaks[:, 0] / PIXEL - px, peaks[:, 1] / PIXEL - py)
         assert d.min() < 3.0, (px, py, d.min())
