@@ -218,6 +218,10 @@ def run_ours(args):
                          orientation_batch=args.batch, device=local)
     sc.set_template(inp["tspec"])
     sc.set_image(inp["ispec"])
+    if args.batch == 0:
+        # the library's autotuner picks the orientations per device pass
+        sc.autotune(inp["filt"], inp["angles"][:256])
+    batch = sc.orientation_batch()
 
     def chunk(i):
         a = (i * per_step) % n_orient_total
@@ -273,7 +277,7 @@ def run_ours(args):
     # ---- roofline for the dominant kernel (per launch = one orientation batch)
     hbm_peak, peak_kind = peaks()
     N = X * Y
-    nb = sc_batch = (args.batch or 32)
+    nb = batch
     n_launch = n_done / nb
     b_launch_ms = b_ms / max(n_launch, 1)
     c_launch_ms = c_ms / max(n_launch, 1)
@@ -285,13 +289,13 @@ def run_ours(args):
     # DRAM bytes per launch from the committed ncu captures of this workload
     # (profiles/k_pass_b_4096x4096_t256.md, profiles/k_pass_c_4096x4096_t256.md);
     # they apply to the default workload and batch only
-    default_shape = (X, Y, T, nb) == (4096, 4096, 256, 32)
+    prof = PROFILED_TRAFFIC.get(nb) if (X, Y, T) == (4096, 4096, 256) else None
     if dominant == "k_pass_b":
         ach = alg_b / (b_launch_ms * 1e-3) / 1e9
-        traffic = args.traffic_b if args.traffic_b is not None else (PROFILED_TRAFFIC["k_pass_b"] if default_shape else None)
+        traffic = args.traffic_b if args.traffic_b is not None else (prof["k_pass_b"] if prof else None)
     else:
         ach = alg_c / (c_launch_ms * 1e-3) / 1e9
-        traffic = args.traffic_c if args.traffic_c is not None else (PROFILED_TRAFFIC["k_pass_c"] if default_shape else None)
+        traffic = args.traffic_c if args.traffic_c is not None else (prof["k_pass_c"] if prof else None)
 
     cpu = cpu_baseline(inp, sample=args.cpu_sample) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     sc.close()
@@ -303,6 +307,7 @@ def run_ours(args):
             "config": {"workload": WORKLOAD["name"], "micrograph": [WORKLOAD["nx"], WORKLOAD["ny"]],
                        "padded": [X, Y], "template": T, "orientations_per_step": per_step,
                        "grid_orientations": n_orient_total, "orientation_batch": nb,
+                       "orientation_batch_autotuned": args.batch == 0,
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2: each batch writes a %.1f GB intermediate" % (nb * Y * (X // 2 + 4) * 8 / 1e9)},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
@@ -322,8 +327,11 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-# ncu dram__bytes_read.sum + dram__bytes_write.sum per launch (32 orientations, 4096^2, 256^3)
-PROFILED_TRAFFIC = {"k_pass_b": 0.869e9 + 2.142e9, "k_pass_c": 2.555e9 + 0.382e9}
+# ncu dram__bytes_read.sum + dram__bytes_write.sum per launch at 4096^2 / 256^3, by orientation batch
+PROFILED_TRAFFIC = {
+    32: {"k_pass_b": 0.869e9 + 2.142e9, "k_pass_c": 2.555e9 + 0.382e9},
+    64: {"k_pass_b": 1.408e9 + 4.292e9, "k_pass_c": 4.707e9 + 0.388e9},
+}
 
 
 def _oracle_sample(inp, n_orient, bits=32):
@@ -385,7 +393,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--orientations-per-step", type=int, default=1024)
-    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--batch", type=int, default=0, help="orientations per device pass; 0 = autotuned")
     ap.add_argument("--cpu-sample", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="full", choices=sorted(WORKLOADS),

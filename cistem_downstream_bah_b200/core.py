@@ -30,7 +30,7 @@ TM_ERR_CANCELLED = -6
 EXPORTED = [
     "tm_create", "tm_set_template", "tm_set_image", "tm_reset_results", "tm_run_plane",
     "tm_get_results", "tm_correlations_computed", "tm_last_timing", "tm_debug_stage_buffers", "tm_destroy",
-    "tm_last_error", "tm_version", "tm_run_plane_noalloc",
+    "tm_last_error", "tm_version", "tm_run_plane_noalloc", "tm_autotune_batch", "tm_orientation_batch",
 ]
 
 
@@ -81,6 +81,9 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.tm_last_timing.argtypes = [vp] + [ctypes.POINTER(ctypes.c_double)] * 4
     L.tm_debug_stage_buffers.argtypes = [vp] * 8
     L.tm_run_plane_noalloc.argtypes = [ip, ctypes.POINTER(TmDims), vp, vp, vp, vp, ip, ip, vp, vp, vp, vp, vp, vp]
+    L.tm_autotune_batch.argtypes = [vp, vp, vp, ip, ctypes.POINTER(ctypes.c_int)]
+    L.tm_orientation_batch.argtypes = [vp]
+    L.tm_orientation_batch.restype = ctypes.c_int
     L.tm_destroy.argtypes = [vp]
     L.tm_last_error.argtypes = [vp]
     L.tm_last_error.restype = ctypes.c_char_p
@@ -136,6 +139,19 @@ class SearchCore:
         a = np.ascontiguousarray(euler_angles, dtype=np.float32).reshape(-1, 3)
         cb = PROGRESS_FN(progress) if progress else PROGRESS_FN()
         self._check(self.L.tm_run_plane(self.h, _ptr(f), _ptr(a), len(a), defocus_offset, pixel_size_offset, cb, None))
+
+    def autotune(self, projection_filter, euler_angles):
+        """Picks the orientations per device pass (16, 32 or 64) by timing the
+        given orientations (contexts created with orientation_batch=0); clears
+        the running results.  Returns the batch."""
+        f = np.ascontiguousarray(projection_filter, dtype=np.float32)
+        a = np.ascontiguousarray(euler_angles, dtype=np.float32).reshape(-1, 3)
+        b = ctypes.c_int(0)
+        self._check(self.L.tm_autotune_batch(self.h, _ptr(f), _ptr(a), len(a), ctypes.byref(b)))
+        return b.value
+
+    def orientation_batch(self):
+        return int(self.L.tm_orientation_batch(self.h))
 
     def results(self):
         n = self.X * self.Y

@@ -37,6 +37,7 @@ struct Variant;
 struct tm_ctx {
     tm_dims d{};
     int X = 0, Y = 0, T = 0, XP = 0, TP = 0, B = 0;
+    int Bcap = 0;   // orientation capacity of the batch buffers (B <= Bcap)
     int device = 0, nsm = 0;
     const Variant* var = nullptr;
     cudaStream_t stream = nullptr;
@@ -267,6 +268,7 @@ int tm_create(const tm_dims* dims, tm_ctx** out) {
     c->T = dims->template_size;
     c->TP = c->T / 2 + 1;
     c->B = dims->orientation_batch > 0 ? dims->orientation_batch : 32;
+    c->Bcap = dims->orientation_batch > 0 ? dims->orientation_batch : 64;   // 0 = automatic: room to tune up to 64
     if (dims->histogram_bins <= 0 || dims->histogram_bins > 1024 || !(dims->histogram_step_scaled > 0)) {
         *out = c;
         return set_err(c, TM_ERR_INVALID, "histogram_bins must be 1..1024 and the step positive");
@@ -298,7 +300,15 @@ int tm_create(const tm_dims* dims, tm_ctx** out) {
         if (e == cudaSuccess) e = cudaEventCreate(&c->ev_end);
         if (e != cudaSuccess) { *out = c; return set_err(c, TM_ERR_CUDA, "stream/event creation: %s", cudaGetErrorString(e)); }
     }
-    const size_t T = c->T, X = c->X, Y = c->Y, XP = c->XP, TP = c->TP, B = c->B;
+    if (dims->orientation_batch <= 0) {
+        // automatic batch: keep the capacity for 64 orientations only if the
+        // correlation spectra of 64 fit in half of the free device memory
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
+            (size_t)64 * c->Y * c->XP * sizeof(float2) > free_b / 2)
+            c->Bcap = 32;
+    }
+    const size_t T = c->T, X = c->X, Y = c->Y, XP = c->XP, TP = c->TP, B = c->Bcap;
     TRY(dalloc(c, &c->tmpl, T * T * TP));
     TRY(dalloc(c, &c->Ip, Y * XP));
     TRY(dalloc(c, &c->S, B * T * TP));
@@ -586,6 +596,37 @@ int tm_debug_stage_buffers(tm_ctx* c, const float* projection_filter, const floa
     if (columns) TM_CUDA(c, cudaMemcpy2D(columns, hc * sizeof(float2), c->C, XP * sizeof(float2), hc * sizeof(float2), (size_t)c->Y, cudaMemcpyDeviceToHost));
     return TM_OK;
 }
+
+int tm_autotune_batch(tm_ctx* c, const float* projection_filter, const float* euler_angles, int n, int* chosen) {
+    if (!c || !projection_filter || !euler_angles || n <= 0) return TM_ERR_INVALID;
+    const int cands[3] = {16, 32, 64};
+    int best_b = c->B;
+    double best = 1e30;
+    bool warmed = false;
+    for (int b : cands) {
+        if (b > c->Bcap) continue;
+        c->B = b;
+        int rc = tm_reset_results(c);
+        if (rc != TM_OK) return rc;
+        if (!warmed) {   // first launches of a context pay one-time costs
+            rc = tm_run_plane(c, projection_filter, euler_angles, n < b ? n : b, 0.f, 0.f, nullptr, nullptr);
+            if (rc != TM_OK) return rc;
+            warmed = true;
+        }
+        rc = tm_run_plane(c, projection_filter, euler_angles, n, 0.f, 0.f, nullptr, nullptr);
+        if (rc != TM_OK) return rc;
+        const double per = c->last_total_ms / n;
+        if (per < best) {
+            best = per;
+            best_b = b;
+        }
+    }
+    c->B = best_b;
+    if (chosen) *chosen = best_b;
+    return tm_reset_results(c);
+}
+
+int tm_orientation_batch(const tm_ctx* c) { return c ? c->B : 0; }
 
 int tm_destroy(tm_ctx* c) {
     if (!c) return TM_ERR_INVALID;

@@ -144,6 +144,7 @@ void TemplateMatchingCore::Init(void*, Image& template_reconstruction, Image& in
     defocus_step_ = defocus_step;
     pixel_size_step_ = pixel_size_step;
     progress_ = my_progress;
+    tuned_ = false;
     // orientation order of RunInnerLoop: search position outer, psi inner,
     // psi accumulated in float (TemplateMatchingCore.cu:200-206)
     orientations_.clear();
@@ -194,8 +195,15 @@ void TemplateMatchingCore::RunInnerLoop(Image& projection_filter, float c_pixel,
     } else {
         for (size_t i = 0; i < filt.size(); i++) filt[i] = projection_filter.complex_values[i].real();
     }
-    check(tm_reset_results(ctx_), "tm_reset_results");
     const int n = (int)(orientations_.size() / 3);
+    if (!tuned_) {
+        // orientations per device pass, timed on the start of this core's range
+        int chosen = 0;
+        const int m = n < 256 ? n : 256;
+        if (m >= 64) check(tm_autotune_batch(ctx_, filt.data(), orientations_.data(), m, &chosen), "tm_autotune_batch");
+        tuned_ = true;
+    }
+    check(tm_reset_results(ctx_), "tm_reset_results");
     ProgressCtx pc{progress_, current_correlation_position};
     check(tm_run_plane(ctx_, filt.data(), orientations_.data(), n, c_defocus * defocus_step_, c_pixel * pixel_size_step_,
                        progress_cb, &pc),

@@ -149,6 +149,7 @@ private:
     std::vector<float> orientations_;   // (phi, theta, psi) in the reference's loop order
     ProgressBar* progress_ = nullptr;
     double last_ms_ = 0;
+    bool tuned_ = false;   // orientation batch picked at the first RunInnerLoop
     // host copies of the last plane's results
     std::vector<float> mip_, psi_, theta_, phi_, defocus_, pixel_;
     std::vector<double> sum_, sumsq_;

@@ -52,7 +52,8 @@ typedef struct tm_dims {
     int histogram_bins;            /* 512 in the reference */
     double histogram_min_scaled;   /* histogram_min / sqrt(X*Y) */
     double histogram_step_scaled;  /* histogram_step / sqrt(X*Y) */
-    int orientation_batch;         /* orientations per device pass; 0 = default */
+    int orientation_batch;         /* orientations per device pass; 0 = automatic (32 until
+                                      tm_autotune_batch picks 16, 32 or 64) */
     int device;                    /* CUDA device ordinal */
 } tm_dims;
 
@@ -156,6 +157,19 @@ TM_API int tm_run_plane_noalloc(int device, const tm_dims *dims, const float *d_
                                 const float *euler_angles, int n_orientations, int first_orientation_index,
                                 float *d_mip, int *d_best, double *d_sum, double *d_sum_of_squares,
                                 unsigned long long *d_histogram, void *stream);
+
+/* Automatic orientation batch (no counterpart in the reference, whose GPU
+ * path processes one orientation per launch).  For a context created with
+ * orientation_batch = 0, times tm_run_plane over the given orientations with
+ * 16, 32 and 64 orientations per device pass (64 only when its buffers fit in
+ * half of the free device memory at tm_create), keeps the fastest and clears
+ * the running results.  Use 128 or more orientations of the real search.
+ * chosen (may be NULL) receives the batch.  The template and image must be set. */
+TM_API int tm_autotune_batch(tm_ctx *ctx, const float *projection_filter, const float *euler_angles,
+                             int n_orientations, int *chosen);
+
+/* Orientations per device pass currently used by the context. */
+TM_API int tm_orientation_batch(const tm_ctx *ctx);
 
 /* Frees every device buffer of the context. */
 TM_API int tm_destroy(tm_ctx *ctx);

@@ -108,3 +108,17 @@ def test_planted_particles_are_found():
         y0, x0 = int(round(py)), int(round(px))
         win = z[max(0, y0 - 3):y0 + 4, max(0, x0 - 3):x0 + 4]
         assert win.max() > 4.0, (px, py, win.max())
+
+
+def test_autotuned_batch_keeps_parity():
+    case = make_case(T=32, X=256, Y=256, angular_step=30.0, psi_step=30.0)
+    with _core(case, batch=0) as sc:
+        b = sc.autotune(case["filt"], case["angles"][:160])
+        assert b in (16, 32, 64) and sc.orientation_batch() == b
+        assert sc.correlations_computed() == 0   # the tuning runs are cleared
+        sc.run_plane(case["filt"], case["angles"])
+        r = sc.results()
+    st = O.SearchState(256, 256)
+    O.search(st, case["tspec"], case["ispec"], case["filt"], case["angles"], hist_min_scaled=case["hmin"],
+             hist_step_scaled=case["hstep"])
+    assert np.abs(r["mip"] - st.mip).max() / np.abs(st.mip).max() < 1e-4
