@@ -11,6 +11,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <chrono>
 #include <string>
 #include <thread>
@@ -52,6 +53,7 @@ struct tm_ctx {
     double *sum = nullptr, *sumsq = nullptr;
     unsigned long long* hist = nullptr;
     int* err_flag = nullptr;
+    int* best_host = nullptr;   // page-locked copy of the best-orientation map (tm_get_results)
     long long rot_capacity = 0;
     bool has_template = false, has_image = false;
     // bookkeeping for decoding the argmax
@@ -193,6 +195,7 @@ void free_all(tm_ctx* c) {
                     c->rowstat, c->mip, c->best, c->sum, c->sumsq, c->hist, c->err_flag};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (c->best_host) cudaFreeHost(c->best_host);
     if (c->stream) cudaStreamDestroy(c->stream);
     cudaEvent_t evs[] = {c->ev_start, c->ev_prep, c->ev_b, c->ev_c, c->ev_end};
     for (cudaEvent_t e : evs)
@@ -371,27 +374,15 @@ int tm_set_image(tm_ctx* c, const float* spectrum, int image_x, int image_y) {
     TM_CUDA(c, cudaSetDevice(c->device));
     // I'[ky][kx] = I[ky][kx] * exp(+2 pi i (kx*x0/X + ky*y0/Y)) / N, with the
     // projection placed at (x0, y0) = (X/2 - T/2, Y/2 - T/2); I'[0][0] = 0.
+    // Computed on the device; the raw spectrum is staged in the correlation
+    // buffer C, which holds nothing between planes.
     const int X = c->X, Y = c->Y, hc = X / 2 + 1, XP = c->XP;
-    const long long x0 = X / 2 - c->T / 2, y0 = Y / 2 - c->T / 2;
-    const double invn = 1.0 / ((double)X * (double)Y);
-    std::vector<float2> ip((size_t)Y * XP, make_float2(0.f, 0.f));
-    std::vector<double> cx(hc), sx(hc);
-    for (int kx = 0; kx < hc; kx++) {
-        double a = 2.0 * M_PI * (double)((kx * x0) % X) / (double)X;
-        cx[kx] = cos(a);
-        sx[kx] = sin(a);
-    }
-    for (int ky = 0; ky < Y; ky++) {
-        double b = 2.0 * M_PI * (double)((ky * y0) % Y) / (double)Y;
-        double cy = cos(b), sy = sin(b);
-        for (int kx = 0; kx < hc; kx++) {
-            double pr = cx[kx] * cy - sx[kx] * sy, pi = cx[kx] * sy + sx[kx] * cy;
-            double ir = spectrum[2 * ((size_t)ky * hc + kx)], ii = spectrum[2 * ((size_t)ky * hc + kx) + 1];
-            ip[(size_t)ky * XP + kx] = make_float2((float)((ir * pr - ii * pi) * invn), (float)((ir * pi + ii * pr) * invn));
-        }
-    }
-    ip[0] = make_float2(0.f, 0.f);
-    TM_CUDA(c, cudaMemcpy(c->Ip, ip.data(), sizeof(float2) * ip.size(), cudaMemcpyHostToDevice));
+    float2* staging = c->C;
+    TM_CUDA(c, cudaMemcpyAsync(staging, spectrum, sizeof(float2) * (size_t)Y * hc, cudaMemcpyHostToDevice, c->stream));
+    tmk::k_prepare_image<<<dim3((XP + 127) / 128, Y), 128, 0, c->stream>>>(staging, c->Ip, X, Y, XP, c->T);
+    TM_CUDA(c, cudaGetLastError());
+    int rc = wait_stream(c, 600.0);
+    if (rc != TM_OK) return rc;
     c->has_image = true;
     return TM_OK;
 }
@@ -525,32 +516,47 @@ int tm_get_results(tm_ctx* c, float* mip, float* best_psi, float* best_theta, fl
         for (size_t i = 0; i < h.size(); i++) histogram[i] = (long long)h[i];
     }
     if (best_psi || best_theta || best_phi || best_defocus || best_pixel_size) {
-        std::vector<int> best(n);
-        TM_CUDA(c, cudaMemcpy(best.data(), c->best, sizeof(int) * n, cudaMemcpyDeviceToHost));
-        for (size_t i = 0; i < n; i++) {
-            const int g = best[i];
-            float psi = 0, th = 0, ph = 0, df = 0, px = 0;
-            if (g >= 0) {
-                // planes are few: linear scan from the back (most recent first)
-                for (size_t k = c->planes.size(); k-- > 0;) {
-                    const Plane& p = c->planes[k];
-                    if (g >= p.base && g < p.base + p.n) {
-                        const float* ang = c->angle_lists[p.angles_id].data() + 3 * (size_t)(g - p.base);
-                        ph = ang[0];
-                        th = ang[1];
-                        psi = ang[2];
-                        df = p.defocus;
-                        px = p.pixel;
-                        break;
+        if (!c->best_host) TM_CUDA(c, cudaMallocHost((void**)&c->best_host, sizeof(int) * n));
+        const int* best = c->best_host;
+        TM_CUDA(c, cudaMemcpy(c->best_host, c->best, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        // decode global orientation indices into angles and plane offsets, in parallel
+        auto decode = [&](size_t i0, size_t i1) {
+            for (size_t i = i0; i < i1; i++) {
+                const int g = best[i];
+                float psi = 0, th = 0, ph = 0, df = 0, px = 0;
+                if (g >= 0) {
+                    // planes are few: linear scan from the back (most recent first)
+                    for (size_t k = c->planes.size(); k-- > 0;) {
+                        const Plane& p = c->planes[k];
+                        if (g >= p.base && g < p.base + p.n) {
+                            const float* ang = c->angle_lists[p.angles_id].data() + 3 * (size_t)(g - p.base);
+                            ph = ang[0];
+                            th = ang[1];
+                            psi = ang[2];
+                            df = p.defocus;
+                            px = p.pixel;
+                            break;
+                        }
                     }
                 }
+                if (best_psi) best_psi[i] = psi;
+                if (best_theta) best_theta[i] = th;
+                if (best_phi) best_phi[i] = ph;
+                if (best_defocus) best_defocus[i] = df;
+                if (best_pixel_size) best_pixel_size[i] = px;
             }
-            if (best_psi) best_psi[i] = psi;
-            if (best_theta) best_theta[i] = th;
-            if (best_phi) best_phi[i] = ph;
-            if (best_defocus) best_defocus[i] = df;
-            if (best_pixel_size) best_pixel_size[i] = px;
+        };
+        unsigned nt = std::thread::hardware_concurrency();
+        nt = nt < 1 ? 1 : (nt > 32 ? 32 : nt);
+        if (n < ((size_t)1 << 16)) nt = 1;
+        std::vector<std::thread> pool;
+        const size_t chunk = (n + nt - 1) / nt;
+        for (unsigned k = 1; k < nt; k++) {
+            const size_t i0 = k * chunk, i1 = std::min(n, i0 + chunk);
+            if (i0 < i1) pool.emplace_back(decode, i0, i1);
         }
+        decode(0, std::min(n, chunk));
+        for (auto& th : pool) th.join();
     }
     return TM_OK;
 }

@@ -692,6 +692,30 @@ k_pass_c(BatchArgs a, int Y) {
 }
 
 // --------------------------------------------------------------------------------------
+// Prepared micrograph spectrum I'[ky][kx] = I[ky][kx] * exp(+2 pi i (kx*x0/X + ky*y0/Y)) / N
+// with the projection placed at (x0, y0) = (X/2 - T/2, Y/2 - T/2), I'[0][0] = 0, and zero
+// pitch padding (kx > X/2).  spec: Y*(X/2+1) complex; phases in double.
+__global__ void k_prepare_image(const float2* __restrict__ spec, float2* __restrict__ ip, int X, int Y, int XP, int T) {
+    const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ky = blockIdx.y;
+    if (kx >= XP) return;
+    const int hc = X / 2 + 1;
+    float2 out = make_float2(0.f, 0.f);
+    if (kx < hc && !(kx == 0 && ky == 0)) {
+        const long long x0 = X / 2 - T / 2, y0 = Y / 2 - T / 2;
+        double sx, cx, sy, cy;
+        sincospi(2.0 * (double)((kx * x0) % X) / (double)X, &sx, &cx);
+        sincospi(2.0 * (double)((ky * y0) % Y) / (double)Y, &sy, &cy);
+        const double pr = cx * cy - sx * sy, pi = cx * sy + sx * cy;
+        const float2 v = spec[(size_t)ky * hc + kx];
+        const double invn = 1.0 / ((double)X * (double)Y);
+        out = make_float2((float)(((double)v.x * pr - (double)v.y * pi) * invn),
+                          (float)(((double)v.x * pi + (double)v.y * pr) * invn));
+    }
+    ip[(size_t)ky * XP + kx] = out;
+}
+
+// --------------------------------------------------------------------------------------
 __global__ void k_reset_state(float* mip, int* best, double* sum, double* sumsq, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         mip[i] = -FLT_MAX;
