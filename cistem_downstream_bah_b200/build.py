@@ -22,7 +22,7 @@ CORE_LIB = os.path.join(LIB_DIR, "libtm_b200.so")
 HOST_DIR = os.path.join(PKG, "host")
 HOST_LIB = os.path.join(LIB_DIR, "libtm_host.so")
 CLI = os.path.join(LIB_DIR, "match_template")
-HOST_COMMON = ["host_fft.cpp", "mrc.cpp", "prep.cpp", "peaks.cpp"]
+HOST_COMMON = ["host_fft.cpp", "mrc.cpp", "prep.cpp", "peaks.cpp", "montage.cpp"]
 CXX_FLAGS = ["-std=c++17", "-O2", "-fopenmp", "-ffp-contract=off", "-fPIC", "-Wall", "-Wno-unused-parameter",
              "-I" + os.path.join(ROOT, "include"), "-I" + HOST_DIR]
 

@@ -116,3 +116,20 @@ TMH_API int tmh_find_peaks(int nx, int ny, const float* scaled_mip, const float*
     }
     return (int)pk.size();
 }
+
+// projection montage of peaks given as (x, y, psi, theta, phi) rows; volume T^3 [z][y][x]; out nx*ny
+TMH_API void tmh_projection_montage(int T, const float* volume, int n_peaks, const float* peaks, int nx, int ny,
+                                    float* out) {
+    std::vector<float> vol(volume, volume + (size_t)T * T * T);
+    std::vector<PeakInfo> pk(n_peaks);
+    for (int k = 0; k < n_peaks; k++) {
+        pk[k] = PeakInfo{};
+        pk[k].x = (int)peaks[5 * k];
+        pk[k].y = (int)peaks[5 * k + 1];
+        pk[k].psi = peaks[5 * k + 2];
+        pk[k].theta = peaks[5 * k + 3];
+        pk[k].phi = peaks[5 * k + 4];
+    }
+    auto m = projection_montage(vol, T, pk, nx, ny);
+    std::memcpy(out, m.data(), m.size() * sizeof(float));
+}

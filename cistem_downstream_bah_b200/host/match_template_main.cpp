@@ -465,25 +465,35 @@ int run(const JobArgs& a) {
     if (std::fclose(hf) != 0) throw CoreError(TM_ERR_INVALID, "write failed for " + a.output_histogram_file);
     std::printf("Expected threshold = %.2f\n", expected_threshold);
 
-    // Peak list (the reference's result aggregation, match_template.cpp:1838-1975):
-    // written when the result file argument (38) names a file.  The reference
-    // stores these records in its project database and draws a projection
-    // montage into that file; this program writes the records as text.
+    // Peaks and result image (the reference's result aggregation,
+    // match_template.cpp:1838-1975), when the result file argument (38) names a
+    // file: the projection montage is written there as MRC, and the peak
+    // records -- which the reference stores in its project database -- as text
+    // next to it (<result file without .mrc>_peaks.txt).
     if (!a.result_output_filename.empty() && a.result_output_filename != "/dev/null") {
         Image2 z = out(scaled, true), ps = out(best_psi, false), th = out(best_theta, false), ph = out(best_phi, false);
         Image2 df = out(best_defocus, false), px = out(best_pixel, false);
         const auto peaks = find_peaks(z.nx, z.ny, z.v, ps.v.data(), th.v.data(), ph.v.data(), df.v.data(), px.v.data(),
                                       expected_threshold, (int)a.min_peak_radius, T, a.pixel_size);
-        FILE* pf = std::fopen(a.result_output_filename.c_str(), "w");
-        if (!pf) throw CoreError(TM_ERR_INVALID, "cannot write " + a.result_output_filename);
+        std::string base = a.result_output_filename;
+        if (base.size() > 4 && base.compare(base.size() - 4, 4, ".mrc") == 0) base.resize(base.size() - 4);
+        const std::string peak_file = base + "_peaks.txt";
+        FILE* pf = std::fopen(peak_file.c_str(), "w");
+        if (!pf) throw CoreError(TM_ERR_INVALID, "cannot write " + peak_file);
         std::fprintf(pf, "# %zu peaks above the expected threshold %.2f (min peak radius %d px)\n", peaks.size(),
                      expected_threshold, (int)a.min_peak_radius);
         std::fprintf(pf, "# x (A), y (A), psi, theta, phi, defocus, pixel size, peak height\n");
         for (const PeakInfo& p : peaks)
             std::fprintf(pf, "%f %f %f %f %f %f %f %f\n", p.x_pos, p.y_pos, p.psi, p.theta, p.phi, p.defocus,
                          p.pixel_size, p.peak_height);
-        if (std::fclose(pf) != 0) throw CoreError(TM_ERR_INVALID, "write failed for " + a.result_output_filename);
-        std::printf("%zu peaks written to %s\n", peaks.size(), a.result_output_filename.c_str());
+        if (std::fclose(pf) != 0) throw CoreError(TM_ERR_INVALID, "write failed for " + peak_file);
+        Image2 montage;
+        montage.nx = z.nx;
+        montage.ny = z.ny;
+        montage.v = projection_montage(rec.data, T, peaks, z.nx, z.ny);
+        write_or_die(a.result_output_filename, montage, a.pixel_size);
+        std::printf("%zu peaks written to %s; result image %s\n", peaks.size(), peak_file.c_str(),
+                    a.result_output_filename.c_str());
     }
     return 0;
 }

@@ -25,3 +25,18 @@ std::vector<PeakInfo> find_peaks(int nx, int ny, std::vector<float>& scaled_mip,
                                  int min_peak_radius, int template_size, float pixel_size, int max_peaks = 1000);
 
 }  // namespace tmhost
+
+namespace tmhost {
+
+// The result image of the reference's aggregation (match_template.cpp:1845-1966):
+// the template (T^3 real volume, [z][y][x]) divided by the mean of its 100
+// largest values on the three central planes (Image::ReturnAverageOfMaxN,
+// image.cpp:11930-11974), transformed and scaled by sqrt(T*T*sqrt(T)), with
+// the central pixel zeroed and the quadrants swapped; for each peak its
+// Fourier slice at the peak's angles (ExtractSlice), scaled by T, transformed
+// back, less its edge mean, and added where positive into an nx x ny image
+// centred on the peak (InsertOtherImageAtSpecifiedPosition, image.cpp:8468-8520).
+std::vector<float> projection_montage(const std::vector<float>& volume, int T, const std::vector<PeakInfo>& peaks,
+                                      int nx, int ny);
+
+}  // namespace tmhost

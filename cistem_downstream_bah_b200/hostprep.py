@@ -22,6 +22,7 @@ EXPORTED = [
     "tmh_whiten", "tmh_template_spectrum", "tmh_projection_filter", "tmh_search_grid", "tmh_psi_list",
     "tmh_factorize_dimension", "tmh_is_power_of_two", "tmh_angular_step", "tmh_erfcinv", "tmh_edge_mean",
     "tmh_clip_into", "tmh_rotate90", "tmh_mrc_info", "tmh_mrc_read", "tmh_mrc_write", "tmh_find_peaks",
+    "tmh_projection_montage",
 ]
 
 
@@ -61,6 +62,7 @@ def lib() -> ctypes.CDLL:
         L.tmh_mrc_write.restype = i
         L.tmh_find_peaks.argtypes = [i, i, P, P, P, P, P, P, f, i, i, f, P, i]
         L.tmh_find_peaks.restype = i
+        L.tmh_projection_montage.argtypes = [i, P, i, P, i, i, P]
         _lib = L
     return _lib
 
@@ -170,3 +172,14 @@ def find_peaks(scaled_mip, psi, theta, phi, defocus, pixel, threshold, min_peak_
     n = lib().tmh_find_peaks(nx, ny, *[_p(a) for a in arrs], float(threshold), int(min_peak_radius),
                              int(template_size), float(pixel_size), _p(out), max_peaks)
     return out[:n].copy()
+
+
+def projection_montage(volume, peaks_xy_angles, nx, ny):
+    """Result image of the reference's aggregation: projections of the template
+    at each peak's angles, added where positive, centred on the peaks.
+    peaks_xy_angles: rows (x, y, psi, theta, phi), pixel coordinates."""
+    vol = _f32(volume)
+    pk = _f32(np.asarray(peaks_xy_angles, np.float32).reshape(-1, 5))
+    out = np.zeros((ny, nx), np.float32)
+    lib().tmh_projection_montage(vol.shape[0], _p(vol), len(pk), _p(pk), nx, ny, _p(out))
+    return out

@@ -28,7 +28,7 @@ def _run_cli(tmp, img_path, tpl_path):
     args = [img_path, tpl_path, PIXEL, 300.0, 2.7, 0.07, DEFOCUS, DEFOCUS, 0.0, 300.0, 8.0, STEP, 20,
             DF_RANGE, DF_STEP, 0.0, 0.0, 1.0, "no", 0.0, 0.0,
             f["mip"], f["psi"], f["theta"], f["phi"], f["defocus"], f["pixel"], f["scaled"], f["avg"], "C1",
-            PSI_STEP, str(tmp / "hist.txt"), -1, -1, 0, 0, f["std"], "/dev/null", str(tmp / "peaks.txt"), 10.0, "yes", 1]
+            PSI_STEP, str(tmp / "hist.txt"), -1, -1, 0, 0, f["std"], "/dev/null", str(tmp / "result.mrc"), 10.0, "yes", 1]
     assert len(args) == 42
     r = subprocess.run([H.CLI_PATH, *map(str, args)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
@@ -109,9 +109,10 @@ def test_match_template_program_matches_oracle(tmp_path):
         y, x = int(round(py)), int(round(px))
         win = got["scaled"][max(0, y - 3):y + 4, max(0, x - 3):x + 4]
         assert win.max() > 4.0, (px, py, win.max())
-    # the peak list (argument 38): the reference's peak loop on the written maps,
-    # and every planted particle away from the edges is among the peaks
-    rows = [ln.split() for ln in open(tmp_path / "peaks.txt").read().splitlines() if not ln.startswith("#")]
+    # the peak list next to the result image (argument 38): the reference's peak
+    # loop on the written maps, and every planted particle above the threshold
+    # and away from the edges is among the peaks
+    rows = [ln.split() for ln in open(tmp_path / "result_peaks.txt").read().splitlines() if not ln.startswith("#")]
     peaks = np.array(rows, np.float32).reshape(-1, 8)
     ref_peaks = H.find_peaks(got["scaled"], got["psi"], got["theta"], got["phi"], got["defocus"], got["pixel"],
                              threshold=float(np.float32(np.sqrt(np.float32(2.0))) *
@@ -127,3 +128,11 @@ def test_match_template_program_matches_oracle(tmp_path):
             continue   # near an edge, or not above the threshold
         d = np.hypot(peaks[:, 0] / PIXEL - px, peaks[:, 1] / PIXEL - py)
         assert d.min() < 3.0, (px, py, d.min())
+    # the result image: the template's projections at the peaks, positive values only
+    montage, px = H.read_mrc(tmp_path / "result.mrc")
+    montage = montage[0]
+    assert montage.shape == (250, 256) and abs(px - PIXEL) < 1e-6 and montage.min() >= 0.0
+    ref_montage = H.projection_montage(vol, [[p[8], p[9], p[2], p[3], p[4]] for p in ref_peaks], 256, 250)
+    assert np.allclose(montage, ref_montage, rtol=1e-4, atol=1e-4 * ref_montage.max())
+    for p in ref_peaks:
+        assert montage[int(p[9]) - 3:int(p[9]) + 4, int(p[8]) - 3:int(p[8]) + 4].max() > 0

@@ -216,3 +216,32 @@ def test_peak_list_matches_the_reference_loop():
     # (5, 75) lies within T/4+1 of an edge; (31, 44) is blanked by (30, 40)
     assert [tuple(int(v) for v in p) for p in got[:, 8:]] == [(10, 60), (40, 30), (100, 90)]
     assert np.array_equal(got[:, :8], ref)
+
+
+def test_projection_montage_is_the_projection_at_zero_angles():
+    """At (psi, theta, phi) = 0 the Fourier slice samples the grid exactly, so
+    the montage tile is the z-projection of the normalised template,
+    scaled by sqrt(T*T*sqrt(T)) * T * T^2 / T^3 = T^1.25, less its edge mean,
+    kept where positive."""
+    T = 32
+    c = np.arange(T) - T // 2
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    vol = (np.exp(-((x - 2) ** 2 + y ** 2 + (z + 1) ** 2) / 18.0) +
+           0.5 * np.exp(-((x + 5) ** 2 + (y - 4) ** 2 + z ** 2) / 8.0)).astype(np.float32)
+    planes = np.concatenate([vol[T // 2].ravel(), vol[:, T // 2].ravel(), vol[:, :, T // 2].ravel()])
+    # voxels on the central planes, each once: the union of the three planes
+    mask = np.zeros(vol.shape, bool)
+    mask[T // 2] = mask[:, T // 2] = mask[:, :, T // 2] = True
+    m = np.sort(vol[mask])[-100:].astype(np.float64).mean()
+    proj = (vol / np.float32(m)).astype(np.float64).sum(axis=0)
+    # the DC term is zeroed: subtract the volume mean along the projection
+    proj = proj - proj.mean()
+    proj = proj * T ** 1.25
+    edge = np.concatenate([proj[0], proj[1:-1, 0], proj[1:-1, -1], proj[-1]]).mean()
+    expect = np.clip(proj - edge, 0, None)
+    nx, ny = 100, 90
+    got = H.projection_montage(vol, [[50, 40, 0.0, 0.0, 0.0]], nx, ny)
+    tile = got[40 - T // 2:40 + T // 2, 50 - T // 2:50 + T // 2]
+    assert np.abs(tile - expect).max() < 1e-3 * expect.max()
+    assert np.count_nonzero(got) == np.count_nonzero(tile)
+    assert planes.size == 3 * T * T
