@@ -354,10 +354,11 @@ struct Plan {
 };
 
 // One cooperative FFT.  `sync` is a callable barrier over all threads that
-// use `buf`.  buf has padded_len(L) float2 entries.  The caller must ensure no
-// other thread still reads buf from a previous use before calling (the first
-// exchange begins with a barrier).
-template <int L, int R, int DIR, class Sync>
+// use `buf`.  buf has padded_len(L) float2 entries.  The first exchange begins
+// with a barrier so that no thread still reads buf from a previous use; a
+// caller whose threads have all passed a barrier since buf was last read
+// passes FIRST_SYNC = false to skip it.
+template <int L, int R, int DIR, bool FIRST_SYNC = true, class Sync>
 __device__ __forceinline__ void fft(float2 (&v)[R], int t, float2* buf, const Twiddles& tw, Sync sync) {
     using PL = Plan<L, R>;
     constexpr int P = PL::P;
@@ -399,7 +400,7 @@ __device__ __forceinline__ void fft(float2 (&v)[R], int t, float2* buf, const Tw
 #pragma unroll
                 for (int r = 0; r < RS; r++) v[u + r * (R / RS)] = e[r];
             } else {
-                if (u == 0) sync();  // previous readers of buf are done
+                if (u == 0 && (FIRST_SYNC || s > 0)) sync();  // previous readers of buf are done
                 // base + compile-time offsets equal pad16(idxD + r*Ns) when no
                 // 16-element boundary falls inside a butterfly (Ns == 1, R | 16)
                 // or every stride is a whole number of 16-blocks (16 | Ns)

@@ -517,7 +517,8 @@ k_pass_b(BatchArgs a, int n_items) {
                     w = cmul(w, w1);
                 }
             }
-            tmfft::fft<L, V, -1>(v, tp, fwdbuf, a.twy, sync);
+            // every thread passed the item barrier since the buffers were last read
+            tmfft::fft<L, V, -1, false>(v, tp, fwdbuf, a.twy, sync);
             // thread (s, tp) holds F[k], k = s + MY*(tp + PT*r) = j + P*r
             if (tmem_warp) {
                 float iv[16];
@@ -650,7 +651,8 @@ k_pass_c(BatchArgs a, int Y) {
             const float2 od = cmul(d, a.tw.template w<+1>(k, X));
             v[r] = make_float2(e.x - od.y, e.y + od.x);
         }
-        tmfft::fft<H, 8, +1>(v, t, fbuf, a.tw, sync);
+        // the barrier at the top of the iteration follows the last reads of fbuf
+        tmfft::fft<H, 8, +1, false>(v, t, fbuf, a.tw, sync);
         const int g = (int)(a.gidx0 + o);
 #pragma unroll
         for (int r = 0; r < 8; r++) {
