@@ -15,6 +15,9 @@ e2e   : the same steps through the C ABI with host buffers: per step the
         prepared spectra and filter are copied host->device (pinned memory),
         the plane is searched, and MIP / best angles / sums / histogram are
         copied device->host and decoded; timed by the host clock.
+accuracy_vs_fp64_oracle: after timing, the CPU-baseline leg searches a few
+        orientations of the workload with the FP64 oracle as the checker and
+        reports the MIP (relative) and z-score (absolute) errors.
 
 --impl reference times the reference CPU algorithm (the FP32 build of the
 oracle's restatement, all host threads) on a bounded sample of the same
@@ -370,7 +373,11 @@ def run_ours(args):
         ach = alg_c / (c_launch_ms * 1e-3) / 1e9
         traffic = args.traffic_c if args.traffic_c is not None else (prof["k_pass_c"] if prof else None)
 
-    cpu = cpu_baseline(inp, sample=args.cpu_sample) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
+    # the CPU-baseline leg (rank 0, N=1): the oracle timed on the host cores,
+    # then the FP64 oracle as the checker of a few orientations after timing
+    cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
+    cpu = cpu_baseline(inp, sample=args.cpu_sample) if cpu_leg else None
+    acc = accuracy_vs_fp64(sc, inp, args.accuracy) if (cpu_leg and args.accuracy > 0) else None
     sc.close()
     if rank == 0:
         line = {
@@ -394,6 +401,8 @@ def run_ours(args):
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if acc is not None:
+            line["accuracy_vs_fp64_oracle"] = acc
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -405,6 +414,30 @@ PROFILED_TRAFFIC = {
     32: {"k_pass_b": 0.869e9 + 2.142e9, "k_pass_c": 2.555e9 + 0.382e9},
     64: {"k_pass_b": 1.408e9 + 4.292e9, "k_pass_c": 4.707e9 + 0.388e9},
 }
+
+
+def accuracy_vs_fp64(sc, inp, k):
+    """MIP and z-score error of the search against the FP64 oracle on k
+    orientations spread over the grid (same prepared inputs on both sides)."""
+    from oracle import oracle as O
+    n = len(inp["angles"])
+    ang = inp["angles"][np.linspace(0, n - 1, k).astype(np.int64)]
+    sc.reset()
+    sc.run_plane(inp["filt"], ang)
+    r = sc.results()
+    st = O.SearchState(inp["X"], inp["Y"])
+    O.search(st, inp["tspec"].astype(np.complex128), inp["ispec"].astype(np.complex128), inp["filt"], ang,
+             hist_min_scaled=inp["hmin"], hist_step_scaled=inp["hstep"], bits=64)
+    sq = float(np.sqrt(float(inp["X"] * inp["Y"])))
+    mip_ref, z_ref, _, _ = O.finalize(st, k, sq)
+    gpu = O.SearchState(inp["X"], inp["Y"])
+    gpu.mip[:], gpu.sum[:], gpu.sumsq[:] = r["mip"], r["sum"], r["sumsq"]
+    mip_got, z_got, _, _ = O.finalize(gpu, k, sq)
+    scale = float(np.abs(mip_ref).max())
+    return {"orientations": int(k),
+            "mip_max_rel_err": float(np.abs(mip_got - mip_ref).max() / scale),
+            "z_max_abs_err": float(np.abs(z_got - z_ref).max()),
+            "note": "FP32 search vs FP64 oracle, MIP error relative to the MIP scale"}
 
 
 def _oracle_sample(inp, n_orient, bits=32):
@@ -469,6 +502,8 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="orientations per device pass; 0 = autotuned")
     ap.add_argument("--cpu-sample", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--accuracy", type=int, default=4,
+                    help="orientations compared with the FP64 oracle after timing, in the CPU-baseline leg (0 = skip)")
     ap.add_argument("--workload", default="full", choices=sorted(WORKLOADS) + ["batched"],
                     help="full = the metric's 4096^2 configuration; the others are the uneven and stress geometries")
     ap.add_argument("--traffic-b", type=float, default=None, help="ncu DRAM bytes per pass-B launch")
