@@ -179,34 +179,18 @@ def pinned_copy(a):
 
 
 def dist_init(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    return world, rank, local
+    from cistem_downstream_bah_b200 import distributed as D
+    return D.init_from_env("nccl")
 
 
 def barrier(world):
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        dist.barrier()
-        torch.cuda.synchronize()
+    from cistem_downstream_bah_b200 import distributed as D
+    D.barrier(world)
 
 
 def max_over_ranks(world, v):
-    if world <= 1:
-        return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from cistem_downstream_bah_b200 import distributed as D
+    return D.max_over_ranks(world, v)
 
 
 BATCHED = dict(name="batched: 8 micrographs (3838x3710, 4096^2 x3, 5760x4092 x2, 2048^2 x2) x 13 defocus planes, "

@@ -6,7 +6,9 @@
   * ``lib/libtm_host.so`` -- the C++ host preparation (whitening, template
     spectrum, projection filter, search grid, MRC I/O) with C entry points;
   * ``lib/match_template`` -- the match_template program (C++ host over the
-    C ABI, linked against libtm_b200.so with an $ORIGIN rpath).
+    C ABI, linked against libtm_b200.so with an $ORIGIN rpath);
+  * ``lib/match_template_merge`` -- the master side of a distributed run
+    (merges worker result arrays; host only).
 """
 from __future__ import annotations
 
@@ -22,7 +24,8 @@ CORE_LIB = os.path.join(LIB_DIR, "libtm_b200.so")
 HOST_DIR = os.path.join(PKG, "host")
 HOST_LIB = os.path.join(LIB_DIR, "libtm_host.so")
 CLI = os.path.join(LIB_DIR, "match_template")
-HOST_COMMON = ["host_fft.cpp", "mrc.cpp", "prep.cpp", "peaks.cpp", "montage.cpp"]
+MERGE_CLI = os.path.join(LIB_DIR, "match_template_merge")
+HOST_COMMON = ["host_fft.cpp", "mrc.cpp", "prep.cpp", "peaks.cpp", "montage.cpp", "result_array.cpp"]
 CXX_FLAGS = ["-std=c++17", "-O2", "-fopenmp", "-ffp-contract=off", "-fPIC", "-Wall", "-Wno-unused-parameter",
              "-I" + os.path.join(ROOT, "include"), "-I" + HOST_DIR]
 
@@ -88,6 +91,11 @@ def build_host(force: bool = False, verbose: bool = False) -> None:
         cmd = [_cxx(), *CXX_FLAGS, "-o", CLI, *common,
                os.path.join(HOST_DIR, "template_matching_core.cpp"), os.path.join(HOST_DIR, "match_template_main.cpp"),
                "-L" + LIB_DIR, "-ltm_b200", "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+    if force or _stale(MERGE_CLI, _host_deps()):
+        cmd = [_cxx(), *CXX_FLAGS, "-o", MERGE_CLI, *common, os.path.join(HOST_DIR, "match_template_merge.cpp")]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)

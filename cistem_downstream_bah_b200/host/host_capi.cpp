@@ -6,6 +6,7 @@
 
 #include "mrc.hpp"
 #include "peaks.hpp"
+#include "result_array.hpp"
 #include "prep.hpp"
 
 #define TMH_API extern "C" __attribute__((visibility("default")))
@@ -132,4 +133,58 @@ TMH_API void tmh_projection_montage(int T, const float* volume, int n_peaks, con
     }
     auto m = projection_montage(vol, T, pk, nx, ny);
     std::memcpy(out, m.data(), m.size() * sizeof(float));
+}
+
+// search-position ranges of n_jobs jobs: out receives first, last per job
+TMH_API int tmh_job_search_ranges(int n_positions, int n_jobs, int* out) {
+    const auto r = job_search_ranges(n_positions, n_jobs);
+    for (size_t k = 0; k < r.size(); k++) {
+        out[2 * k] = r[k].first;
+        out[2 * k + 1] = r[k].second;
+    }
+    return (int)r.size();
+}
+
+// worker result array from 8 compact nx*ny maps (MIP, psi, theta, phi,
+// defocus, pixel size, sum, sum of squares); returns its length in floats
+// (written when it fits `cap`), -1 on bad arguments
+TMH_API long tmh_pack_worker_result(int nx, int ny, const float* maps, long original_x, long original_y, int remove,
+                                    float ccs, double sqrt_input_pixels, const long* histogram, int bins, float* out,
+                                    long cap) {
+    try {
+        WorkerMaps m;
+        m.nx = nx;
+        m.ny = ny;
+        const size_t n = (size_t)nx * ny;
+        std::vector<float>* dst[8] = {&m.mip, &m.psi, &m.theta, &m.phi, &m.defocus, &m.pixel, &m.sum, &m.sumsq};
+        for (int k = 0; k < 8; k++) dst[k]->assign(maps + n * k, maps + n * (k + 1));
+        const auto r = pack_worker_result(m, original_x, original_y, remove, ccs, sqrt_input_pixels, histogram, bins);
+        if ((long)r.size() <= cap) std::memcpy(out, r.data(), r.size() * sizeof(float));
+        return (long)r.size();
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+// the master over n result arrays: maps_out receives 9 compact images of the
+// first array's size (MIP x sqrt(N), psi, theta, phi, defocus, pixel size,
+// scaled MIP, average x sqrt(N), standard deviation x sqrt(N)), rows_out the
+// 512 x 4 histogram table, stats_out {expected threshold, correlation maps}
+TMH_API int tmh_merge_results(int n, const float* const* arrays, const long* sizes, int use_gpu, float* maps_out,
+                              double* rows_out, double* stats_out) {
+    try {
+        AggregatedTemplateResult agg;
+        for (int i = 0; i < n; i++) agg.AddResult(arrays[i], sizes[i]);
+        const MasterOutputs o = finalize_master(agg, use_gpu != 0);
+        const size_t npix = (size_t)o.nx * o.ny;
+        const Image2* ims[9] = {&o.mip, &o.psi, &o.theta, &o.phi, &o.defocus, &o.pixel, &o.scaled_mip, &o.avg,
+                                &o.std_dev};
+        for (int k = 0; k < 9; k++) std::memcpy(maps_out + npix * k, ims[k]->v.data(), npix * sizeof(float));
+        std::memcpy(rows_out, o.histogram_rows.data(), o.histogram_rows.size() * sizeof(double));
+        stats_out[0] = o.expected_threshold;
+        stats_out[1] = agg.total_number_of_ccs;
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
 }

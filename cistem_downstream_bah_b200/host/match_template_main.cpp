@@ -12,8 +12,18 @@
 // files land in argument slots 36 and 28, which DoCalculation reads as the
 // variance and average files: the two outputs are swapped in interactive use,
 // as in the reference.  The search always runs on the GPU; use_gpu (40) and
-// max_threads (41) are accepted and reported.  The distributed worker mode
-// (<address> <port> <job code> <threads>) is not provided: every run is local.
+// max_threads (41) are accepted and reported.
+//
+//   match_template ARG0 ... ARG41 RESULT_ARRAY
+//                                  a worker job of a distributed run: the
+//                                  search covers search positions ARG32-ARG33
+//                                  (not the whole grid) and, instead of the
+//                                  output files, writes the flat result array
+//                                  the reference's worker sends to its master
+//                                  (:1373-1530) to RESULT_ARRAY; the program
+//                                  match_template_merge plays the master.
+// The reference's socket transport (<address> <port> <job code> <threads>) is
+// replaced by these files.
 #include <unistd.h>
 
 #include <cfloat>
@@ -26,7 +36,9 @@
 #include <string>
 #include <vector>
 
+#include "job_args.hpp"
 #include "mrc.hpp"
+#include "result_array.hpp"
 #include "peaks.hpp"
 #include "prep.hpp"
 #include "template_matching_core.hpp"
@@ -41,62 +53,7 @@ constexpr int kHistogramBins = 512;
 constexpr double kPi = 3.14159265359;
 constexpr float kPif = 3.14159265359f;
 
-int myroundint(float a) { return a > 0 ? (int)(a + 0.5f) : (int)(a - 0.5f); }
 float rad_2_deg(float r) { return (float)((double)r / ((double)kPif / 180.)); }
-
-// The job arguments, indexed as DoCalculation reads them.
-struct JobArgs {
-    std::string input_search_images, input_reconstruction;                   // 0, 1
-    float pixel_size = 1, voltage_kV = 300, spherical_aberration_mm = 2.7f;   // 2-4
-    float amplitude_contrast = 0.07f, defocus1 = 10000, defocus2 = 10000;     // 5-7
-    float defocus_angle = 0, low_resolution_limit = 300;                      // 8, 9
-    float high_resolution_limit_search = 8, angular_step = 0;                 // 10, 11
-    int best_parameters_to_keep = 20;                                         // 12
-    float defocus_search_range = 500, defocus_step = 50;                      // 13, 14
-    float pixel_size_search_range = 0.1f, pixel_size_step = 0.02f;            // 15, 16
-    float padding = 1;                                                        // 17
-    bool ctf_refinement = false;                                              // 18
-    float particle_radius_angstroms = 0, phase_shift = 0;                     // 19, 20
-    std::string mip_output_file, best_psi_output_file, best_theta_output_file; // 21-23
-    std::string best_phi_output_file, best_defocus_output_file;               // 24, 25
-    std::string best_pixel_size_output_file, scaled_mip_output_file;          // 26, 27
-    std::string correlation_avg_output_file, my_symmetry = "C1";              // 28, 29
-    float in_plane_angular_step = 0;                                          // 30
-    std::string output_histogram_file;                                        // 31
-    int first_search_position = -1, last_search_position = -1;                // 32, 33
-    int image_number_for_gui = 0, number_of_jobs_per_image_in_gui = 0;        // 34, 35
-    std::string correlation_std_output_file, directory_for_results;           // 36, 37
-    std::string result_output_filename;                                       // 38
-    float min_peak_radius = 10;                                               // 39
-    bool use_gpu = true;                                                      // 40
-    int max_threads = 1;                                                      // 41
-};
-
-bool parse_bool(const std::string& s) {
-    return !s.empty() && (s[0] == 'y' || s[0] == 'Y' || s[0] == 't' || s[0] == 'T' || s[0] == '1');
-}
-
-bool parse_positional(int argc, char** argv, JobArgs& a) {
-    if (argc != 43) return false;
-    auto S = [&](int i) { return std::string(argv[1 + i]); };
-    auto F = [&](int i) { return (float)std::atof(argv[1 + i]); };
-    auto I = [&](int i) { return std::atoi(argv[1 + i]); };
-    a.input_search_images = S(0); a.input_reconstruction = S(1);
-    a.pixel_size = F(2); a.voltage_kV = F(3); a.spherical_aberration_mm = F(4); a.amplitude_contrast = F(5);
-    a.defocus1 = F(6); a.defocus2 = F(7); a.defocus_angle = F(8); a.low_resolution_limit = F(9);
-    a.high_resolution_limit_search = F(10); a.angular_step = F(11); a.best_parameters_to_keep = I(12);
-    a.defocus_search_range = F(13); a.defocus_step = F(14); a.pixel_size_search_range = F(15);
-    a.pixel_size_step = F(16); a.padding = F(17); a.ctf_refinement = parse_bool(S(18));
-    a.particle_radius_angstroms = F(19); a.phase_shift = F(20);
-    a.mip_output_file = S(21); a.best_psi_output_file = S(22); a.best_theta_output_file = S(23);
-    a.best_phi_output_file = S(24); a.best_defocus_output_file = S(25); a.best_pixel_size_output_file = S(26);
-    a.scaled_mip_output_file = S(27); a.correlation_avg_output_file = S(28); a.my_symmetry = S(29);
-    a.in_plane_angular_step = F(30); a.output_histogram_file = S(31); a.first_search_position = I(32);
-    a.last_search_position = I(33); a.image_number_for_gui = I(34); a.number_of_jobs_per_image_in_gui = I(35);
-    a.correlation_std_output_file = S(36); a.directory_for_results = S(37); a.result_output_filename = S(38);
-    a.min_peak_radius = F(39); a.use_gpu = parse_bool(S(40)); a.max_threads = I(41);
-    return true;
-}
 
 // UserInput (src/core/userinput.cpp:40-110): question [default] padded to 50
 // columns, " : ", one line from stdin; empty = default on a terminal and an
@@ -232,11 +189,6 @@ JobArgs interactive() {
     return a;
 }
 
-void write_or_die(const std::string& path, const Image2& im, float pixel_size) {
-    std::string err;
-    if (!write_mrc(path, im.nx, im.ny, 1, im.v.data(), pixel_size, err)) throw CoreError(TM_ERR_INVALID, err);
-}
-
 Image2 as_image2(const std::vector<float>& v, int nx, int ny) {
     Image2 im;
     im.nx = nx;
@@ -304,7 +256,18 @@ int run(const JobArgs& a) {
     input_image.complex_values = std::move(w.spectrum);
 
     // counts (:733-772)
-    const int first = 0, last = euler.number_of_search_positions - 1;
+    // a local run searches the whole grid (:735-739); a worker its range
+    const bool worker = !a.worker_result_file.empty();
+    int first = 0, last = euler.number_of_search_positions - 1;
+    if (worker) {
+        if (a.first_search_position < 0 || a.last_search_position >= euler.number_of_search_positions ||
+            a.first_search_position > a.last_search_position)
+            throw CoreError(TM_ERR_INVALID, "search positions " + std::to_string(a.first_search_position) + "-" +
+                                                std::to_string(a.last_search_position) + " outside the grid of " +
+                                                std::to_string(euler.number_of_search_positions));
+        first = a.first_search_position;
+        last = a.last_search_position;
+    }
     long total_correlation_positions = 0;
     int number_of_rotations = 0;
     for (float psi = psi_start; psi <= psi_max; psi += psi_step) number_of_rotations++;
@@ -337,6 +300,7 @@ int run(const JobArgs& a) {
     long current_correlation_position = 0;
     bool first_loop = true;
     double device_ms = 0;
+    float actual_number_of_ccs_calculated = 0.0f;
     Image mip_buffer, psi_buffer, theta_buffer, phi_buffer;
     const int n_size = myroundint(float(pixel_size_search_range) / float(pixel_size_step));
     const int n_defocus = myroundint(float(defocus_search_range) / float(defocus_step));
@@ -366,6 +330,7 @@ int run(const JobArgs& a) {
             projection_filter.real_values = tmhost::projection_filter(T, w.curve, ctf, float(defocus_i) * defocus_step);
             core.RunInnerLoop(projection_filter, (float)size_i, (float)defocus_i, 0, current_correlation_position);
             device_ms += core.last_device_ms();
+            actual_number_of_ccs_calculated += core.total_number_of_cccs_calculated;   // :984
             // host merge of the plane (match_template.cpp:918-984)
             core.d_max_intensity_projection.CopyDeviceToHost(mip_buffer, true, false);
             core.d_best_psi.CopyDeviceToHost(psi_buffer, true, false);
@@ -404,6 +369,27 @@ int run(const JobArgs& a) {
         rot(fs); rot(fq);
         for (size_t p = 0; p < npix; p++) { sum[p] = (double)fs[p]; sumsq[p] = (double)fq[p]; }
         std::swap(ox, oy);
+    }
+
+    if (worker) {
+        // the worker's result array (:1373-1530): raw MIP, best parameters and
+        // the sums as float images, on the rotated-back box
+        WorkerMaps m;
+        m.nx = ox;
+        m.ny = oy;
+        m.mip = mip; m.psi = best_psi; m.theta = best_theta; m.phi = best_phi;
+        m.defocus = best_defocus; m.pixel = best_pixel;
+        m.sum.assign(sum.begin(), sum.end());
+        m.sumsq.assign(sumsq.begin(), sumsq.end());
+        const int remove_npix_from_edge = myroundint(a.particle_radius_angstroms / a.pixel_size);   // :494
+        const std::vector<float> result =
+            pack_worker_result(m, original_x, original_y, remove_npix_from_edge, actual_number_of_ccs_calculated,
+                               sqrt_input_pixels, histogram_data.data(), kHistogramBins);
+        if (!write_result_array(a.worker_result_file, result))
+            throw CoreError(TM_ERR_INVALID, "cannot write " + a.worker_result_file);
+        std::printf("Result array of %zu floats (search positions %i-%i, %.0f correlation maps) written to %s\n",
+                    result.size(), first, last, (double)actual_number_of_ccs_calculated, a.worker_result_file.c_str());
+        return 0;
     }
 
     // statistics (:1215-1245)
@@ -475,18 +461,10 @@ int run(const JobArgs& a) {
         Image2 df = out(best_defocus, false), px = out(best_pixel, false);
         const auto peaks = find_peaks(z.nx, z.ny, z.v, ps.v.data(), th.v.data(), ph.v.data(), df.v.data(), px.v.data(),
                                       expected_threshold, (int)a.min_peak_radius, T, a.pixel_size);
-        std::string base = a.result_output_filename;
-        if (base.size() > 4 && base.compare(base.size() - 4, 4, ".mrc") == 0) base.resize(base.size() - 4);
-        const std::string peak_file = base + "_peaks.txt";
-        FILE* pf = std::fopen(peak_file.c_str(), "w");
-        if (!pf) throw CoreError(TM_ERR_INVALID, "cannot write " + peak_file);
-        std::fprintf(pf, "# %zu peaks above the expected threshold %.2f (min peak radius %d px)\n", peaks.size(),
-                     expected_threshold, (int)a.min_peak_radius);
-        std::fprintf(pf, "# x (A), y (A), psi, theta, phi, defocus, pixel size, peak height\n");
-        for (const PeakInfo& p : peaks)
-            std::fprintf(pf, "%f %f %f %f %f %f %f %f\n", p.x_pos, p.y_pos, p.psi, p.theta, p.phi, p.defocus,
-                         p.pixel_size, p.peak_height);
-        if (std::fclose(pf) != 0) throw CoreError(TM_ERR_INVALID, "write failed for " + peak_file);
+        const std::string peak_file = write_peak_records(a.result_output_filename, peaks, expected_threshold,
+                                                         (int)a.min_peak_radius);
+        if (peak_file.empty()) throw CoreError(TM_ERR_INVALID, "cannot write the peak records next to " +
+                                                                   a.result_output_filename);
         Image2 montage;
         montage.nx = z.nx;
         montage.ny = z.ny;
@@ -504,13 +482,15 @@ int main(int argc, char** argv) {
     JobArgs a;
     if (argc == 1) {
         a = interactive();
-    } else if (!parse_positional(argc, argv, a)) {
+    } else if ((argc != 43 && argc != 44) || !parse_job_args(argc, argv, 1, a)) {
         std::fprintf(stderr,
                      "usage: %s                 (interactive)\n"
-                     "       %s ARG0 ... ARG41  (the 42 match_template job arguments)\n",
-                     argv[0], argv[0]);
+                     "       %s ARG0 ... ARG41  (the 42 match_template job arguments)\n"
+                     "       %s ARG0 ... ARG41 RESULT_ARRAY  (worker job over search positions ARG32-ARG33)\n",
+                     argv[0], argv[0], argv[0]);
         return 2;
     }
+    if (argc == 44) a.worker_result_file = argv[43];
     try {
         return run(a);
     } catch (const CoreError& e) {

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdio>
 
 namespace tmhost {
 
@@ -59,6 +60,22 @@ std::vector<PeakInfo> find_peaks(int nx, int ny, std::vector<float>& mip, const 
         out.push_back(p);
     }
     return out;
+}
+
+std::string write_peak_records(const std::string& result_file, const std::vector<PeakInfo>& peaks, float threshold,
+                               int min_peak_radius) {
+    std::string base = result_file;
+    if (base.size() > 4 && base.compare(base.size() - 4, 4, ".mrc") == 0) base.resize(base.size() - 4);
+    const std::string path = base + "_peaks.txt";
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) return std::string();
+    std::fprintf(f, "# %zu peaks above the expected threshold %.2f (min peak radius %d px)\n", peaks.size(), threshold,
+                 min_peak_radius);
+    std::fprintf(f, "# x (A), y (A), psi, theta, phi, defocus, pixel size, peak height\n");
+    for (const PeakInfo& p : peaks)
+        std::fprintf(f, "%f %f %f %f %f %f %f %f\n", p.x_pos, p.y_pos, p.psi, p.theta, p.phi, p.defocus, p.pixel_size,
+                     p.peak_height);
+    return std::fclose(f) == 0 ? path : std::string();
 }
 
 }  // namespace tmhost

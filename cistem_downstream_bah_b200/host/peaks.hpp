@@ -3,6 +3,7 @@
 // over the scaled MIP, with Image::FindPeakWithIntegerCoordinates
 // (src/core/image.cpp:9961-10110) as the peak search.
 #pragma once
+#include <string>
 #include <vector>
 
 namespace tmhost {
@@ -23,6 +24,13 @@ struct PeakInfo {
 std::vector<PeakInfo> find_peaks(int nx, int ny, std::vector<float>& scaled_mip, const float* psi, const float* theta,
                                  const float* phi, const float* defocus, const float* pixel, float threshold,
                                  int min_peak_radius, int template_size, float pixel_size, int max_peaks = 1000);
+
+// The peak records as text -- the values the reference stores in its project
+// database -- next to the result image: <result file without .mrc>_peaks.txt,
+// two comment lines, then x (A), y (A), psi, theta, phi, defocus, pixel size,
+// peak height per line.  Returns the path written, empty on failure.
+std::string write_peak_records(const std::string& result_file, const std::vector<PeakInfo>& peaks, float threshold,
+                               int min_peak_radius);
 
 }  // namespace tmhost
 

@@ -16,13 +16,14 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libtm_host.so")
 CLI_PATH = os.path.join(_HERE, "lib", "match_template")
+MERGE_CLI_PATH = os.path.join(_HERE, "lib", "match_template_merge")
 _lib = None
 
 EXPORTED = [
     "tmh_whiten", "tmh_template_spectrum", "tmh_projection_filter", "tmh_search_grid", "tmh_psi_list",
     "tmh_factorize_dimension", "tmh_is_power_of_two", "tmh_angular_step", "tmh_erfcinv", "tmh_edge_mean",
     "tmh_clip_into", "tmh_rotate90", "tmh_mrc_info", "tmh_mrc_read", "tmh_mrc_write", "tmh_find_peaks",
-    "tmh_projection_montage",
+    "tmh_projection_montage", "tmh_job_search_ranges", "tmh_pack_worker_result", "tmh_merge_results",
 ]
 
 
@@ -63,6 +64,13 @@ def lib() -> ctypes.CDLL:
         L.tmh_find_peaks.argtypes = [i, i, P, P, P, P, P, P, f, i, i, f, P, i]
         L.tmh_find_peaks.restype = i
         L.tmh_projection_montage.argtypes = [i, P, i, P, i, i, P]
+        L.tmh_job_search_ranges.argtypes = [i, i, P]
+        L.tmh_job_search_ranges.restype = i
+        lg = ctypes.c_long
+        L.tmh_pack_worker_result.argtypes = [i, i, P, lg, lg, i, f, d, P, i, P, lg]
+        L.tmh_pack_worker_result.restype = lg
+        L.tmh_merge_results.argtypes = [i, P, P, i, P, P, P]
+        L.tmh_merge_results.restype = i
         _lib = L
     return _lib
 
@@ -183,3 +191,54 @@ def projection_montage(volume, peaks_xy_angles, nx, ny):
     out = np.zeros((ny, nx), np.float32)
     lib().tmh_projection_montage(vol.shape[0], _p(vol), len(pk), _p(pk), nx, ny, _p(out))
     return out
+
+
+def job_search_ranges(n_positions, n_jobs):
+    """[(first, last)] search positions of each job, as the reference's panel
+    splits one image's search (MatchTemplatePanel.cpp:674-784)."""
+    out = np.zeros(2 * max(n_jobs, 0), np.int32)
+    n = lib().tmh_job_search_ranges(int(n_positions), int(n_jobs), _p(out))
+    return [(int(out[2 * k]), int(out[2 * k + 1])) for k in range(n)]
+
+
+WORKER_MAPS = ("mip", "psi", "theta", "phi", "defocus", "pixel", "sum", "sumsq")
+
+
+def pack_worker_result(maps, original_x, original_y, remove_npix_from_edge, number_of_ccs, sqrt_input_pixels,
+                       histogram):
+    """The flat float32 result array a worker job sends to its master.
+    maps: dict of the 8 WORKER_MAPS, each (ny, nx) on the worker's padded box."""
+    m = np.stack([_f32(maps[k]) for k in WORKER_MAPS])
+    _, ny, nx = m.shape
+    m = np.ascontiguousarray(m)
+    h = np.ascontiguousarray(histogram, dtype=np.int64)
+    n = lib().tmh_pack_worker_result(nx, ny, _p(m), int(original_x), int(original_y), int(remove_npix_from_edge),
+                                     float(number_of_ccs), float(sqrt_input_pixels), _p(h), len(h), None, 0)
+    if n < 0:
+        raise ValueError("bad worker maps")
+    out = np.zeros(n, np.float32)
+    lib().tmh_pack_worker_result(nx, ny, _p(m), int(original_x), int(original_y), int(remove_npix_from_edge),
+                                 float(number_of_ccs), float(sqrt_input_pixels), _p(h), len(h), _p(out), n)
+    return out
+
+
+MASTER_MAPS = ("mip", "psi", "theta", "phi", "defocus", "pixel", "scaled_mip", "avg", "std")
+
+
+def merge_results(arrays, use_gpu=True):
+    """The master over worker result arrays (in order): dict of the 9
+    MASTER_MAPS, the 512 x 4 histogram table ("rows"), the expected threshold
+    and the number of correlation maps."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in arrays]
+    nx, ny = int(arrs[0][0]), int(arrs[0][1])
+    ptrs = (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+    sizes = np.array([a.size for a in arrs], np.int64)
+    maps = np.zeros((9, ny, nx), np.float32)
+    rows = np.zeros((512, 4), np.float64)
+    stats = np.zeros(2, np.float64)
+    if lib().tmh_merge_results(len(arrs), ptrs, _p(sizes), 1 if use_gpu else 0, _p(maps), _p(rows), _p(stats)) != 0:
+        raise ValueError("malformed or mismatching result arrays")
+    out = {k: maps[i] for i, k in enumerate(MASTER_MAPS)}
+    out.update(rows=rows, expected_threshold=float(stats[0]), number_of_ccs=float(stats[1]))
+    return out
+

@@ -23,16 +23,31 @@ def _files(tmp):
     return {n: str(tmp / f"{n}.mrc") for n in names}
 
 
-def _run_cli(tmp, img_path, tpl_path):
+def _job_args(tmp, img_path, tpl_path, first=-1, last=-1):
     f = _files(tmp)
     args = [img_path, tpl_path, PIXEL, 300.0, 2.7, 0.07, DEFOCUS, DEFOCUS, 0.0, 300.0, 8.0, STEP, 20,
             DF_RANGE, DF_STEP, 0.0, 0.0, 1.0, "no", 0.0, 0.0,
             f["mip"], f["psi"], f["theta"], f["phi"], f["defocus"], f["pixel"], f["scaled"], f["avg"], "C1",
-            PSI_STEP, str(tmp / "hist.txt"), -1, -1, 0, 0, f["std"], "/dev/null", str(tmp / "result.mrc"), 10.0, "yes", 1]
+            PSI_STEP, str(tmp / "hist.txt"), first, last, 0, 0, f["std"], "/dev/null", str(tmp / "result.mrc"), 10.0,
+            "yes", 1]
     assert len(args) == 42
-    r = subprocess.run([H.CLI_PATH, *map(str, args)], capture_output=True, text=True, timeout=600)
+    return f, [str(a) for a in args]
+
+
+def _run_cli(tmp, img_path, tpl_path):
+    f, args = _job_args(tmp, img_path, tpl_path)
+    r = subprocess.run([H.CLI_PATH, *args], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     return f, r.stdout
+
+
+def _inputs(tmp_path):
+    vol = synthetic.template_volume(T, PIXEL, n_atoms=600, radius_A=T * PIXEL * 0.3, seed=21)
+    img, truth = synthetic.micrograph(250, 256, PIXEL, n_atoms=600, radius_A=T * PIXEL * 0.3, n_particles=3,
+                                      snr=2.0, defocus_A=DEFOCUS, seed=22, atom_seed=21)
+    H.write_mrc(tmp_path / "img.mrc", img, PIXEL)
+    H.write_mrc(tmp_path / "tpl.mrc", vol, PIXEL)
+    return vol, img, truth
 
 
 def _oracle_pipeline(img, vol):
@@ -69,11 +84,7 @@ def _oracle_pipeline(img, vol):
 
 
 def test_match_template_program_matches_oracle(tmp_path):
-    vol = synthetic.template_volume(T, PIXEL, n_atoms=600, radius_A=T * PIXEL * 0.3, seed=21)
-    img, truth = synthetic.micrograph(250, 256, PIXEL, n_atoms=600, radius_A=T * PIXEL * 0.3, n_particles=3,
-                                      snr=2.0, defocus_A=DEFOCUS, seed=22, atom_seed=21)
-    H.write_mrc(tmp_path / "img.mrc", img, PIXEL)
-    H.write_mrc(tmp_path / "tpl.mrc", vol, PIXEL)
+    vol, img, truth = _inputs(tmp_path)
     files, stdout = _run_cli(tmp_path, str(tmp_path / "img.mrc"), str(tmp_path / "tpl.mrc"))
     assert "old x, y; new x, y = 256 250 256 256" in stdout
     ref = _oracle_pipeline(img.astype(np.float32), vol.astype(np.float32))
@@ -136,3 +147,53 @@ def test_match_template_program_matches_oracle(tmp_path):
     assert np.allclose(montage, ref_montage, rtol=1e-4, atol=1e-4 * ref_montage.max())
     for p in ref_peaks:
         assert montage[int(p[9]) - 3:int(p[9]) + 4, int(p[8]) - 3:int(p[8]) + 4].max() > 0
+
+
+def test_worker_jobs_merged_by_the_master_match_the_local_run(tmp_path):
+    """The distributed form: two worker jobs over the reference's split of the
+    search positions write result arrays; match_template_merge merges them as
+    the master does.  The merged maps equal the local run's (MIP and best
+    parameters exactly where the local MIP is positive and decided; the float
+    sums of the result arrays to 1e-4 of the deviation scale)."""
+    _inputs(tmp_path)
+    img, tpl = str(tmp_path / "img.mrc"), str(tmp_path / "tpl.mrc")
+    (tmp_path / "local").mkdir()
+    f_local, _ = _run_cli(tmp_path / "local", img, tpl)
+    n_positions = len(H.search_grid(STEP))
+    ranges = H.job_search_ranges(n_positions, 2)
+    assert ranges[0][0] == 0 and ranges[1][1] == n_positions - 1
+    arrays = []
+    for j, (first, last) in enumerate(ranges):
+        d = tmp_path / f"w{j}"
+        d.mkdir()
+        _, args = _job_args(d, img, tpl, first, last)
+        r = subprocess.run([H.CLI_PATH, *args, str(d / "result.bin")], capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+        assert "Result array of" in r.stdout
+        assert not os.path.exists(d / "mip.mrc")   # a worker writes only its array
+        arrays.append(str(d / "result.bin"))
+    (tmp_path / "merged").mkdir()
+    f_m, args = _job_args(tmp_path / "merged", img, tpl)
+    r = subprocess.run([H.MERGE_CLI_PATH, *args, *arrays], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    local = {k: H.read_mrc(v)[0][0] for k, v in f_local.items()}
+    merged = {k: H.read_mrc(v)[0][0] for k, v in f_m.items()}
+    pos = local["mip"] > 0
+    assert pos.mean() > 0.99
+    assert np.array_equal(merged["mip"][pos], local["mip"][pos])
+    # decided pixels: the runner-up over the whole search is not within 1e-4
+    # of the MIP; the merged argmax then equals the local one
+    ref = _oracle_pipeline(H.read_mrc(img)[0][0], H.read_mrc(tpl)[0])
+    d = ref["decided"] & pos
+    for k in ("psi", "theta", "phi", "defocus"):
+        assert np.array_equal(merged[k][d], local[k][d]), k
+    scale = np.abs(local["std"]).max()
+    assert np.abs(merged["avg"] - local["avg"]).max() <= 1e-4 * scale
+    assert np.abs(merged["std"] - local["std"]).max() <= 1e-4 * scale
+    assert np.abs(merged["scaled"] - local["scaled"]).max() <= 2e-3
+    h_local = np.array([[float(v) for v in ln.split()] for ln in open(tmp_path / "local" / "hist.txt").read().splitlines()[2:]])
+    lines = open(tmp_path / "merged" / "hist.txt").read().splitlines()
+    h_m = np.array([[float(v) for v in ln.split()] for ln in lines[2:]])
+    assert np.array_equal(h_m[:, :2], h_local[:, :2])
+    assert lines[0] == open(tmp_path / "local" / "hist.txt").readline().rstrip("\n")
+
