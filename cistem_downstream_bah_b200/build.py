@@ -8,7 +8,9 @@
   * ``lib/match_template`` -- the match_template program (C++ host over the
     C ABI, linked against libtm_b200.so with an $ORIGIN rpath);
   * ``lib/match_template_merge`` -- the master side of a distributed run
-    (merges worker result arrays; host only).
+    (merges worker result arrays; host only);
+  * ``lib/refine_template`` -- the refine_template program (C++ host over the
+    C ABI's batched TemplateScore).
 """
 from __future__ import annotations
 
@@ -25,7 +27,8 @@ HOST_DIR = os.path.join(PKG, "host")
 HOST_LIB = os.path.join(LIB_DIR, "libtm_host.so")
 CLI = os.path.join(LIB_DIR, "match_template")
 MERGE_CLI = os.path.join(LIB_DIR, "match_template_merge")
-HOST_COMMON = ["host_fft.cpp", "mrc.cpp", "prep.cpp", "peaks.cpp", "montage.cpp", "result_array.cpp"]
+REFINE_CLI = os.path.join(LIB_DIR, "refine_template")
+HOST_COMMON = ["host_fft.cpp", "mrc.cpp", "prep.cpp", "peaks.cpp", "montage.cpp", "result_array.cpp", "refine.cpp"]
 CXX_FLAGS = ["-std=c++17", "-O2", "-fopenmp", "-ffp-contract=off", "-fPIC", "-Wall", "-Wno-unused-parameter",
              "-I" + os.path.join(ROOT, "include"), "-I" + HOST_DIR]
 
@@ -58,7 +61,8 @@ def _stale(target, deps):
 def build_core(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(LIB_DIR, exist_ok=True)
     if force or _stale(CORE_LIB, _sources()):
-        cmd = [_nvcc(), *NVCC_FLAGS, "-o", CORE_LIB, os.path.join(CSRC, "tm_capi.cu"), os.path.join(CSRC, "tm_noalloc.cu")]
+        cmd = [_nvcc(), *NVCC_FLAGS, "-o", CORE_LIB, os.path.join(CSRC, "tm_capi.cu"), os.path.join(CSRC, "tm_noalloc.cu"),
+               os.path.join(CSRC, "tm_refine.cu")]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd), file=sys.stderr)
@@ -90,6 +94,12 @@ def build_host(force: bool = False, verbose: bool = False) -> None:
     if force or _stale(CLI, _host_deps() + [CORE_LIB]):
         cmd = [_cxx(), *CXX_FLAGS, "-o", CLI, *common,
                os.path.join(HOST_DIR, "template_matching_core.cpp"), os.path.join(HOST_DIR, "match_template_main.cpp"),
+               "-L" + LIB_DIR, "-ltm_b200", "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+    if force or _stale(REFINE_CLI, _host_deps() + [CORE_LIB]):
+        cmd = [_cxx(), *CXX_FLAGS, "-pthread", "-o", REFINE_CLI, *common, os.path.join(HOST_DIR, "refine_template_main.cpp"),
                "-L" + LIB_DIR, "-ltm_b200", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)

@@ -31,6 +31,8 @@ EXPORTED = [
     "tm_create", "tm_set_template", "tm_set_image", "tm_reset_results", "tm_run_plane",
     "tm_get_results", "tm_correlations_computed", "tm_last_timing", "tm_debug_stage_buffers", "tm_destroy",
     "tm_last_error", "tm_version", "tm_run_plane_noalloc", "tm_autotune_batch", "tm_orientation_batch",
+    "tm_refine_create", "tm_refine_set_particle", "tm_refine_set_filter", "tm_refine_set_operator",
+    "tm_refine_score", "tm_refine_last_error", "tm_refine_destroy",
 ]
 
 
@@ -88,6 +90,14 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.tm_last_error.argtypes = [vp]
     L.tm_last_error.restype = ctypes.c_char_p
     L.tm_version.restype = ctypes.c_char_p
+    L.tm_refine_create.argtypes = [ip, ip, ip, vp, ip, ip, ip, ip, ctypes.POINTER(vp)]
+    L.tm_refine_set_particle.argtypes = [vp, ip, vp]
+    L.tm_refine_set_filter.argtypes = [vp, ip, vp]
+    L.tm_refine_set_operator.argtypes = [vp, ip, vp, vp, vp, vp, ip]
+    L.tm_refine_score.argtypes = [vp, ip, vp, vp, vp, vp, vp]
+    L.tm_refine_last_error.argtypes = [vp]
+    L.tm_refine_last_error.restype = ctypes.c_char_p
+    L.tm_refine_destroy.argtypes = [vp]
     _LIB = L
     return L
 
@@ -263,3 +273,61 @@ class TemplateMatchingCore:
         self.histogram = r["hist"]
         self.total_number_of_cccs_calculated = len(self.orientations)
         return current_correlation_position + len(self.orientations)
+
+
+class RefineCore:
+    """Batched TemplateScore of refine_template on one GPU (tm_refine_create ...
+    tm_refine_destroy): the template spectrum of the projection box TP, particle
+    window spectra, projection filters and pixel-size operators in slots."""
+
+    def __init__(self, template_spectrum, T, max_batch=64, max_particles=16, max_filters=64, max_operators=8,
+                 device=0):
+        self._L = load()
+        spec = np.ascontiguousarray(template_spectrum, dtype=np.complex64)
+        self.T, self.TP = int(T), int(spec.shape[0])
+        self._ctx = ctypes.c_void_p()
+        rc = self._L.tm_refine_create(device, self.T, self.TP, _ptr(spec), max_batch, max_particles, max_filters,
+                                      max_operators, ctypes.byref(self._ctx))
+        self._check(rc, "tm_refine_create")
+
+    def _check(self, rc, what):
+        if rc != TM_OK:
+            msg = self._L.tm_refine_last_error(self._ctx).decode() if self._ctx else ""
+            raise TmError(rc, f"{what}: {msg}")
+
+    def set_particle(self, slot, spectrum):
+        a = np.ascontiguousarray(spectrum, dtype=np.complex64)
+        self._check(self._L.tm_refine_set_particle(self._ctx, int(slot), _ptr(a)), "tm_refine_set_particle")
+
+    def set_filter(self, slot, filt):
+        a = np.ascontiguousarray(filt, dtype=np.float32)
+        self._check(self._L.tm_refine_set_filter(self._ctx, int(slot), _ptr(a)), "tm_refine_set_filter")
+
+    def set_operator(self, slot, ar, ai, brt, bit, has_pad_value):
+        arrs = [np.ascontiguousarray(x, dtype=np.float32) for x in (ar, ai, brt, bit)]
+        self._check(self._L.tm_refine_set_operator(self._ctx, int(slot), *[_ptr(x) for x in arrs],
+                                                   1 if has_pad_value else 0), "tm_refine_set_operator")
+
+    def score(self, euler, particle, filt, op):
+        """(n, 3) array of (value, x, y)."""
+        e = np.ascontiguousarray(euler, dtype=np.float32).reshape(-1, 3)
+        n = len(e)
+        p = np.ascontiguousarray(particle, dtype=np.int32)
+        f = np.ascontiguousarray(filt, dtype=np.int32)
+        o = np.ascontiguousarray(op, dtype=np.int32)
+        out = np.zeros((n, 3), np.float32)
+        self._check(self._L.tm_refine_score(self._ctx, n, _ptr(e), _ptr(p), _ptr(f), _ptr(o), _ptr(out)),
+                    "tm_refine_score")
+        return out
+
+    def close(self):
+        if self._ctx:
+            self._L.tm_refine_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

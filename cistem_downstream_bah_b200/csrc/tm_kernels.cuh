@@ -157,7 +157,7 @@ struct SliceCol {
     static constexpr int V = T % 3 == 0 ? 24 : 16;   // values per thread
     static constexpr int PT = T / V;                 // threads per column
     static constexpr int RS = skewed(tmfft::padded_len(T), 1);
-    static constexpr int CB = (16 * RS * 8 <= 48 * 1024) ? 16 : 8;   // columns per block
+    static constexpr int CB = (16 * RS * 8 <= 48 * 1024) ? 16 : (8 * RS * 8 <= 48 * 1024) ? 8 : 4;   // columns per block
     static constexpr int NT = CB * PT;
 };
 

@@ -1,11 +1,15 @@
 // host_capi.cpp -- C entry points of the host preparation library
 // (libtm_host.so), so that tests can hold the C++ preparation against the
 // oracle and against numpy.  Complex arrays are interleaved float pairs.
+#include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 
+#include "host_fft.hpp"
 #include "mrc.hpp"
 #include "peaks.hpp"
+#include "refine.hpp"
 #include "result_array.hpp"
 #include "prep.hpp"
 
@@ -188,3 +192,141 @@ TMH_API int tmh_merge_results(int n, const float* const* arrays, const long* siz
         return -1;
     }
 }
+
+// ---------------------------------------------------------------------------- refine_template
+// whitened real micrograph of refine_template (whitening without the quadrant swap, back to real space)
+TMH_API int tmh_refine_whiten(int nx, int ny, const float* image, float* out) {
+    Whitened w = whiten(wrap(nx, ny, image), false);
+    std::vector<std::complex<double>> spec(w.spectrum.begin(), w.spectrum.end());
+    std::vector<double> real((size_t)nx * ny);
+    irfft2(nx, ny, spec.data(), real.data());
+    for (size_t i = 0; i < real.size(); i++) out[i] = (float)real[i];
+    return (int)w.curve.size();
+}
+
+// peaks as refine_template picks them: out receives x, y (relative to the centre), value per peak
+TMH_API int tmh_refine_find_peaks(int nx, int ny, const float* scaled_mip, float threshold, float min_peak_radius,
+                                  float* out, int max_out) {
+    RefineMaps m;
+    m.nx = nx;
+    m.ny = ny;
+    m.scaled_mip.assign(scaled_mip, scaled_mip + (size_t)nx * ny);
+    const auto pk = refine_find_peaks(m, threshold, min_peak_radius);
+    const int n = (int)std::min<size_t>(pk.size(), (size_t)max_out);
+    for (int k = 0; k < n; k++) {
+        out[3 * k] = pk[k].x;
+        out[3 * k + 1] = pk[k].y;
+        out[3 * k + 2] = pk[k].value;
+    }
+    return (int)pk.size();
+}
+
+TMH_API void tmh_window_particle(int nx, int ny, const float* image, int px, int py, int T, float* out) {
+    const auto w = window_particle(wrap(nx, ny, image), px, py, T);
+    std::memcpy(out, w.data(), w.size() * sizeof(float));
+}
+
+TMH_API void tmh_cosine_mask(int T, float* image, float radius, float edge) {
+    std::vector<float> v(image, image + (size_t)T * T);
+    cosine_mask(v, T, radius, edge);
+    std::memcpy(image, v.data(), v.size() * sizeof(float));
+}
+
+// info: identity, pad, new size, has pad value; matrices as in PixelSizeOperator (when not identity)
+TMH_API int tmh_pixel_size_operator(int nin, int nout, float factor, float* ar, float* ai, float* brt, float* bit,
+                                    int* info) {
+    try {
+        const PixelSizeOperator o = pixel_size_operator(nin, nout, factor);
+        info[0] = o.identity ? 1 : 0;
+        info[1] = o.pad;
+        info[2] = o.new_size;
+        info[3] = o.has_pad_value ? 1 : 0;
+        if (!o.identity) {
+            std::memcpy(ar, o.ar.data(), o.ar.size() * sizeof(float));
+            std::memcpy(ai, o.ai.data(), o.ai.size() * sizeof(float));
+            std::memcpy(brt, o.brt.data(), o.brt.size() * sizeof(float));
+            std::memcpy(bit, o.bit.data(), o.bit.size() * sizeof(float));
+        }
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+TMH_API void tmh_padded_template_spectrum(int T, int TP, const float* volume, float* out) {
+    std::vector<float> vol(volume, volume + (size_t)T * T * T);
+    const auto spec = padded_template_spectrum(vol, T, TP);
+    std::memcpy(out, spec.data(), spec.size() * sizeof(std::complex<float>));
+}
+
+// the descent of refine_template over `n_peaks` peaks with a synthetic score:
+// value = 10 - ((phi - a)/3)^2 - ((theta - b)/3)^2 - ((psi - c)/3)^2
+//         - ((defocus1 - d)/300)^2 - ((factor - e) 50)^2   (double, squares as products, per peak k: target[5k..5k+4])
+// x = (int)floor(|phi - a| 10) % 3 - 1, y = (int)floor(|psi - c| 10) % 3 - 1.
+// maps: 7 compact nx*ny images (mip, scaled mip, psi, theta, phi, defocus,
+// pixel size); params: pixel size, defocus1, defocus2, angular step, in-plane
+// step, defocus range, defocus step, pixel-size range, pixel-size step,
+// xy threshold, exclude (0/1), threads.  maps_out: 7 images; per_peak: 16
+// floats per peak (x, y, psi, theta, phi, defocus, pixel size, height, dx, dy,
+// dpsi, dtheta, dphi, ddefocus, dpixel, dheight); log: the candidates scored,
+// 6 floats each (phi, theta, psi, defocus1, factor, particle), up to max_log.
+TMH_API long tmh_refine_synthetic(int nx, int ny, const float* maps, int n_peaks, const float* peaks_xy,
+                                  const double* target, const float* params, float* maps_out, float* per_peak,
+                                  float* log, long max_log) {
+    RefineMaps m;
+    m.nx = nx;
+    m.ny = ny;
+    const size_t np = (size_t)nx * ny;
+    std::vector<float>* dst[7] = {&m.mip, &m.scaled_mip, &m.psi, &m.theta, &m.phi, &m.defocus, &m.pixel_size};
+    for (int k = 0; k < 7; k++) dst[k]->assign(maps + np * k, maps + np * (k + 1));
+    std::vector<FoundPeak> pk(n_peaks);
+    for (int k = 0; k < n_peaks; k++) {
+        pk[k].x = peaks_xy[2 * k];
+        pk[k].y = peaks_xy[2 * k + 1];
+    }
+    RefineParams p;
+    p.pixel_size = params[0];
+    p.defocus1 = params[1];
+    p.defocus2 = params[2];
+    p.angular_step = params[3];
+    p.in_plane_angular_step = params[4];
+    p.defocus_search_range = params[5];
+    p.defocus_search_step = params[6];
+    p.pixel_size_search_range = params[7];
+    p.pixel_size_search_step = params[8];
+    p.xy_change_threshold = params[9];
+    p.exclude_above_xy_threshold = params[10] != 0.0f;
+    p.max_threads = (int)params[11];
+    std::mutex log_mu;
+    long n_log = 0;
+    auto score = [&](const RefineCandidate& c) {
+        const double* t = target + 5 * c.particle;
+        const double a = (c.phi - t[0]) / 3.0, b = (c.theta - t[1]) / 3.0, d = (c.psi - t[2]) / 3.0;
+        const double e = (c.defocus1 - t[3]) / 300.0, f = (c.pixel_size_factor - t[4]) * 50.0;
+        const double v = 10.0 - a * a - b * b - d * d - e * e - f * f;
+        RefineScore s;
+        s.value = (float)v;
+        s.x = (float)((int)std::floor(std::fabs(c.phi - t[0]) * 10.0) % 3 - 1);
+        s.y = (float)((int)std::floor(std::fabs(c.psi - t[2]) * 10.0) % 3 - 1);
+        std::lock_guard<std::mutex> lock(log_mu);
+        if (n_log < max_log) {
+            float* l = log + 6 * n_log;
+            l[0] = c.phi; l[1] = c.theta; l[2] = c.psi; l[3] = c.defocus1; l[4] = c.pixel_size_factor;
+            l[5] = (float)c.particle;
+        }
+        n_log++;
+        return s;
+    };
+    const RefineOutputs out = refine_peaks(m, pk, p, 32, score);
+    const std::vector<float>* src[7] = {&out.maps.mip, &out.maps.scaled_mip, &out.maps.psi, &out.maps.theta,
+                                        &out.maps.phi, &out.maps.defocus, &out.maps.pixel_size};
+    for (int k = 0; k < 7; k++) std::memcpy(maps_out + np * k, src[k]->data(), np * sizeof(float));
+    for (int k = 0; k < n_peaks; k++) {
+        const RefinedPeak& r = out.refined[k];
+        const float v[16] = {r.x, r.y, r.psi, r.theta, r.phi, r.defocus, r.pixel_size, r.peak_height,
+                             r.dx, r.dy, r.dpsi, r.dtheta, r.dphi, r.ddefocus, r.dpixel_size, r.dpeak_height};
+        std::memcpy(per_peak + 16 * k, v, sizeof v);
+    }
+    return n_log;
+}
+

@@ -267,7 +267,7 @@ int factorize_dimension(int original, int template_size) {
     return original;
 }
 
-Whitened whiten(const Image2& micrograph) {
+Whitened whiten(const Image2& micrograph, bool swap) {
     const int nx = micrograph.nx, ny = micrograph.ny, hc = nx / 2 + 1;
     const long n = (long)nx * ny;
     std::vector<double> img(micrograph.v.begin(), micrograph.v.end());
@@ -283,7 +283,7 @@ Whitened whiten(const Image2& micrograph) {
     rfft2(nx, ny, img.data(), spec.data());
     const double inv = 1.0 / (double)n;
     for (cplx& c : spec) c *= inv;
-    swap_quadrants_centred(nx, ny, 1, spec.data());
+    if (swap) swap_quadrants_centred(nx, ny, 1, spec.data());
     spec[0] = 0;
     // Compute1DPowerSpectrumCurve (image.cpp:7135-7201)
     const int npts = curve_points(nx);
@@ -483,6 +483,45 @@ double erfcinv_approx(double x) {
     const double tt1 = 2 / (kPi * 0.147) + 0.5 * lnx;
     const double tt2 = 1 / 0.147 * lnx;
     return sgn * std::sqrt(-tt1 + std::sqrt(tt1 * tt1 - tt2));
+}
+
+void swap_quadrants(int nx, int ny, int nz, std::complex<double>* spec) { swap_quadrants_centred(nx, ny, nz, spec); }
+
+std::vector<std::complex<float>> padded_template_spectrum(const std::vector<float>& volume, int T, int TP) {
+    if (TP == T) return template_spectrum(volume, T, 1.0f);
+    // ReturnAverageOfRealValuesOnEdges, 3-D (image.cpp:5951-6004): first and
+    // last planes whole, the other planes' first and last rows and the first
+    // and last pixel of their other rows
+    double sum = 0.0;
+    long n = 0;
+    auto at = [&](int i, int j, int k) { return (double)volume[((size_t)k * T + j) * T + i]; };
+    for (int k : {0, T - 1})
+        for (int j = 0; j < T; j++)
+            for (int i = 0; i < T; i++) sum += at(i, j, k);
+    n += 2L * T * T;
+    for (int k = 1; k < T - 1; k++)
+        for (int j = 0; j < T; j++) {
+            if (j == 0 || j == T - 1) {
+                for (int i = 0; i < T; i++) sum += at(i, j, k);
+                n += T;
+            } else {
+                sum += at(0, j, k) + at(T - 1, j, k);
+                n += 2;
+            }
+        }
+    const float edge = (float)(sum / (float)n);
+    std::vector<double> vol(volume.begin(), volume.end());
+    std::vector<double> big = clip3(vol, T, TP, edge);
+    const int hc = TP / 2 + 1;
+    std::vector<cplx> spec((size_t)TP * TP * hc);
+    rfft3(TP, TP, TP, big.data(), spec.data());
+    const double inv = 1.0 / ((double)TP * TP * TP);
+    for (cplx& c : spec) c *= inv;
+    spec[0] = 0;
+    swap_quadrants_centred(TP, TP, TP, spec.data());
+    std::vector<std::complex<float>> out(spec.size());
+    for (size_t i = 0; i < spec.size(); i++) out[i] = std::complex<float>(spec[i]);
+    return out;
 }
 
 }  // namespace tmhost

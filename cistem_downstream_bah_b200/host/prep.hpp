@@ -32,8 +32,17 @@ struct Whitened {
     std::vector<std::complex<float>> spectrum;   // ny*(nx/2+1)
     std::vector<double> curve;                    // whitening filter on [0, sqrt(2)/2]
 };
-// match_template.cpp:711-724
-Whitened whiten(const Image2& micrograph);
+// match_template.cpp:711-724; refine_template.cpp:617-629 whitens the same way
+// without the quadrant swap (swap_quadrants = false)
+Whitened whiten(const Image2& micrograph, bool swap_quadrants = true);
+
+// Image::SwapRealSpaceQuadrants of a half spectrum (object centred in the box)
+void swap_quadrants(int nx, int ny, int nz, std::complex<double>* spec);
+
+// The refine_template template spectrum (refine_template.cpp:586-599): the
+// T^3 volume resized to TP^3 with its edge mean (padding factor TP/T), then
+// ForwardFFT, ZeroCentralPixel and SwapRealSpaceQuadrants.
+std::vector<std::complex<float>> padded_template_spectrum(const std::vector<float>& volume, int T, int TP);
 
 // Template spectrum for the pixel-size factor (ChangePixelSize with
 // return_fft, image.cpp:8705-8822, then ZeroCentralPixel and

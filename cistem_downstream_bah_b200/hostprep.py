@@ -17,6 +17,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libtm_host.so")
 CLI_PATH = os.path.join(_HERE, "lib", "match_template")
 MERGE_CLI_PATH = os.path.join(_HERE, "lib", "match_template_merge")
+REFINE_CLI_PATH = os.path.join(_HERE, "lib", "refine_template")
 _lib = None
 
 EXPORTED = [
@@ -24,6 +25,8 @@ EXPORTED = [
     "tmh_factorize_dimension", "tmh_is_power_of_two", "tmh_angular_step", "tmh_erfcinv", "tmh_edge_mean",
     "tmh_clip_into", "tmh_rotate90", "tmh_mrc_info", "tmh_mrc_read", "tmh_mrc_write", "tmh_find_peaks",
     "tmh_projection_montage", "tmh_job_search_ranges", "tmh_pack_worker_result", "tmh_merge_results",
+    "tmh_refine_whiten", "tmh_refine_find_peaks", "tmh_window_particle", "tmh_cosine_mask", "tmh_pixel_size_operator",
+    "tmh_padded_template_spectrum", "tmh_refine_synthetic",
 ]
 
 
@@ -71,6 +74,17 @@ def lib() -> ctypes.CDLL:
         L.tmh_pack_worker_result.restype = lg
         L.tmh_merge_results.argtypes = [i, P, P, i, P, P, P]
         L.tmh_merge_results.restype = i
+        L.tmh_refine_whiten.argtypes = [i, i, P, P]
+        L.tmh_refine_whiten.restype = i
+        L.tmh_refine_find_peaks.argtypes = [i, i, P, f, f, P, i]
+        L.tmh_refine_find_peaks.restype = i
+        L.tmh_window_particle.argtypes = [i, i, P, i, i, i, P]
+        L.tmh_cosine_mask.argtypes = [i, P, f, f]
+        L.tmh_pixel_size_operator.argtypes = [i, i, f, P, P, P, P, P]
+        L.tmh_pixel_size_operator.restype = i
+        L.tmh_padded_template_spectrum.argtypes = [i, i, P, P]
+        L.tmh_refine_synthetic.argtypes = [i, i, P, i, P, P, P, P, P, P, lg]
+        L.tmh_refine_synthetic.restype = lg
         _lib = L
     return _lib
 
@@ -241,4 +255,74 @@ def merge_results(arrays, use_gpu=True):
     out = {k: maps[i] for i, k in enumerate(MASTER_MAPS)}
     out.update(rows=rows, expected_threshold=float(stats[0]), number_of_ccs=float(stats[1]))
     return out
+
+
+# ----------------------------------------------------------------------------- refine_template
+def refine_whiten(image):
+    """Whitened micrograph of refine_template, in real space."""
+    img = _f32(image)
+    ny, nx = img.shape
+    out = np.zeros((ny, nx), np.float32)
+    lib().tmh_refine_whiten(nx, ny, _p(img), _p(out))
+    return out
+
+
+def refine_find_peaks(scaled_mip, threshold, min_peak_radius, max_out=100000):
+    z = _f32(scaled_mip)
+    ny, nx = z.shape
+    out = np.zeros((max_out, 3), np.float32)
+    n = lib().tmh_refine_find_peaks(nx, ny, _p(z), float(threshold), float(min_peak_radius), _p(out), max_out)
+    return out[:min(n, max_out)].copy()
+
+
+def window_particle(image, peak_x, peak_y, T):
+    img = _f32(image)
+    ny, nx = img.shape
+    out = np.zeros((T, T), np.float32)
+    lib().tmh_window_particle(nx, ny, _p(img), int(peak_x), int(peak_y), int(T), _p(out))
+    return out
+
+
+def cosine_mask(image, radius, edge):
+    img = np.array(image, dtype=np.float32)
+    lib().tmh_cosine_mask(img.shape[0], _p(img), float(radius), float(edge))
+    return img
+
+
+def pixel_size_operator(nin, nout, factor):
+    """(info dict, ar, ai, brt, bit) of the host's ChangePixelSize operator."""
+    ar = np.zeros((nout, nin), np.float32)
+    ai = np.zeros((nout, nin), np.float32)
+    brt = np.zeros((nin, nout), np.float32)
+    bit = np.zeros((nin, nout), np.float32)
+    info = np.zeros(4, np.int32)
+    if lib().tmh_pixel_size_operator(int(nin), int(nout), float(factor), _p(ar), _p(ai), _p(brt), _p(bit), _p(info)):
+        raise ValueError("unsupported pixel-size change")
+    return dict(identity=bool(info[0]), pad=int(info[1]), new=int(info[2]), has_pad_value=bool(info[3])), ar, ai, brt, bit
+
+
+def padded_template_spectrum(volume, TP):
+    vol = _f32(volume)
+    T = vol.shape[0]
+    out = np.zeros((TP, TP, TP // 2 + 1), np.complex64)
+    lib().tmh_padded_template_spectrum(T, int(TP), _p(vol), _p(out))
+    return out
+
+
+REFINE_MAPS = ("mip", "scaled_mip", "psi", "theta", "phi", "defocus", "pixel_size")
+
+
+def refine_synthetic(maps, peaks_xy, targets, params, max_log=2000000):
+    """refine_template's descent with the synthetic score of
+    tmh_refine_synthetic: (maps out, per-peak rows, log of scored candidates)."""
+    m = np.ascontiguousarray(np.stack([_f32(maps[k]) for k in REFINE_MAPS]))
+    _, ny, nx = m.shape
+    pk = np.ascontiguousarray(peaks_xy, dtype=np.float32)
+    tg = np.ascontiguousarray(targets, dtype=np.float64)
+    pr = np.ascontiguousarray(params, dtype=np.float32)
+    out = np.zeros_like(m)
+    per = np.zeros((len(pk), 16), np.float32)
+    log = np.zeros((max_log, 6), np.float32)
+    n = lib().tmh_refine_synthetic(nx, ny, _p(m), len(pk), _p(pk), _p(tg), _p(pr), _p(out), _p(per), _p(log), max_log)
+    return {k: out[i] for i, k in enumerate(REFINE_MAPS)}, per, log[:min(n, max_log)].copy()
 

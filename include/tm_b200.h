@@ -180,6 +180,56 @@ TM_API const char *tm_last_error(const tm_ctx *ctx);
 /* Version string of the library build. */
 TM_API const char *tm_version(void);
 
+/* ---------------------------------------------------------------------------
+ * refine_template scoring.  Replaces TemplateScore
+ * (src/programs/refine_template/refine_template.cpp:24-80), which the
+ * reference evaluates one candidate at a time on the CPU inside OpenMP threads;
+ * here a batch of candidates is scored in one call.  A candidate's score is
+ * the peak (value, x, y relative to the box centre) of the correlation between
+ * a particle window and the projection of the template at the candidate's
+ * Euler angles: Fourier slice (ExtractSlice), quadrant swap, inverse FFT,
+ * optional pixel-size change (ChangePixelSize with return_fft), forward FFT,
+ * projection filter, zeroed central pixel, division by the square root of
+ * ReturnSumOfSquares, product with the conjugate into the particle spectrum,
+ * inverse FFT, FindPeakWithIntegerCoordinates. */
+typedef struct tm_refine_ctx tm_refine_ctx;
+
+/* template_box T: the scored box; projection_box TP: T or 2T (the reference's
+ * padding factor 1 or 2).  template_spectrum: TP*TP*(TP/2+1) complex (float
+ * pairs, [z][y][x]) -- the TP^3 template after ForwardFFT, ZeroCentralPixel
+ * and SwapRealSpaceQuadrants (refine_template.cpp:586-599).  Capacities: the
+ * candidates per device pass and the slots of particle windows, filters and
+ * pixel-size operators.  TM_ERR_UNSUPPORTED for boxes without a compiled
+ * variant (T in 32, 48, 64, 128, 256, 384). */
+TM_API int tm_refine_create(int device, int template_box, int projection_box, const float *template_spectrum,
+                            int max_batch, int max_particles, int max_filters, int max_operators,
+                            tm_refine_ctx **out);
+
+/* Particle window slot: T*(T/2+1) complex, the forward FFT (any scale) of the
+ * T x T window of the whitened micrograph with quadrants swapped
+ * (refine_template.cpp:720-724). */
+TM_API int tm_refine_set_particle(tm_refine_ctx *ctx, int slot, const float *spectrum);
+
+/* Projection filter slot: T*(T/2+1) reals (CTF image x whitening curve). */
+TM_API int tm_refine_set_filter(tm_refine_ctx *ctx, int slot, const float *filter);
+
+/* Pixel-size operator slot (ChangePixelSize of the TP x TP projection into
+ * T x T written as out = Ar (P - pv) Brt - Ai (P - pv) Bit + pv, pv = mean of
+ * P within 0.45 TP of its centre when has_pad_value): ar, ai T*TP; brt, bit
+ * TP*T, row-major. */
+TM_API int tm_refine_set_operator(tm_refine_ctx *ctx, int slot, const float *ar, const float *ai, const float *brt,
+                                  const float *bit, int has_pad_value);
+
+/* Scores n candidates: euler 3n (phi, theta, psi in degrees), particle and
+ * filter slots, operator slot or -1 (pixel-size factor within the 0.001
+ * tolerance: the projection is only clipped to T).  out: 3n floats (value,
+ * x, y).  Returns when the scores are on the host. */
+TM_API int tm_refine_score(tm_refine_ctx *ctx, int n, const float *euler, const int *particle, const int *filter,
+                           const int *op, float *out);
+
+TM_API const char *tm_refine_last_error(const tm_refine_ctx *ctx);
+TM_API int tm_refine_destroy(tm_refine_ctx *ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -119,7 +119,7 @@ static void cfft(const fft_plan *p, real *x, real *work, int sign)
         for (int j = 0; j < nr; j++) {
             const int jm = j % ns;
             const int tstep = jm * (n / (ns * R));
-            double ur[64], ui[64];   /* radices are at most 13 here */
+            double ur[R], ui[R];   /* any radix: the generic branch is a direct DFT */
             for (int r = 0; r < R; r++) {
                 double xr = a[2 * (j + r * nr)], xi = a[2 * (j + r * nr) + 1];
                 int m = (tstep * r) % n;
