@@ -434,6 +434,70 @@ def _oracle_sample(inp, n_orient, bits=32):
     return time.perf_counter() - t0
 
 
+def run_refine(args, seed=20261215):
+    """refine_template's TemplateScore on the GPU: batches of candidates (one
+    per refined peak, as the program's workers hand them over) on a 256^3
+    template, a quarter of them with a pixel-size change.  metric: scored
+    candidates per second of tm_refine_score calls (synchronous: candidate
+    upload, scoring and the scores back on the host)."""
+    world, rank, local = dist_init(args)
+    from cistem_downstream_bah_b200 import core, hostprep, synthetic
+    T, nb, n_part = 256, args.refine_batch, 64
+    vol = synthetic.template_volume(T, 1.0, 120000, 110.0, seed=seed)
+    mic, truth = synthetic.micrograph(1024, 1024, 1.0, 120000, 110.0, 4, 0.05, 12000.0, seed=seed + 1, atom_seed=seed)
+    white = hostprep.refine_whiten(mic)
+    tspec = hostprep.padded_template_spectrum(vol, T)
+    rng = np.random.default_rng(seed)
+    rc = core.RefineCore(tspec, T, max_batch=nb, max_particles=n_part, max_filters=8, max_operators=4, device=local)
+    for k in range(n_part):
+        w = hostprep.window_particle(white, int(rng.integers(-300, 300)), int(rng.integers(-300, 300)), T)
+        sp = np.fft.rfft2(w.astype(np.float64)) / (T * T)
+        sp *= np.where((np.arange(T)[:, None] + np.arange(T // 2 + 1)[None, :]) % 2 == 0, 1.0, -1.0)
+        rc.set_particle(k, sp)
+    from cistem_downstream_bah_b200 import prep
+    _, curve = prep.whiten(mic)
+    for k in range(8):
+        rc.set_filter(k, prep.projection_filter(T, curve, kv=300.0, cs_mm=2.7, amplitude_contrast=0.07,
+                                                defocus1=11800.0 + 50.0 * k, defocus2=11800.0 + 50.0 * k,
+                                                pixel_size=1.0))
+    for k, f in enumerate((0.98, 0.99, 1.01, 1.02)):
+        info, ar, ai, brt, bit = hostprep.pixel_size_operator(T, T, f)
+        rc.set_operator(k, ar, ai, brt, bit, info["has_pad_value"])
+
+    def batch(i):
+        r = np.random.default_rng(seed + i)
+        e = np.stack([r.uniform(0, 360, nb), r.uniform(0, 180, nb), r.uniform(0, 360, nb)], 1).astype(np.float32)
+        op = np.where(r.uniform(size=nb) < 0.25, r.integers(0, 4, nb), -1)
+        return e, r.integers(0, n_part, nb), r.integers(0, 8, nb), op
+
+    batches = [batch(i) for i in range(args.warmup + args.steps)]
+    for i in range(args.warmup):
+        rc.score(*batches[i])
+    barrier(world)
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            rc.score(*batches[args.warmup + i])
+        el = time.perf_counter() - t0
+    el = max_over_ranks(world, el)
+    rc.close()
+    if rank == 0:
+        rate = nb * args.steps * world / el
+        print(json.dumps({
+            "metric": "refine_template TemplateScore candidates/s", "value": rate, "unit": "candidates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"refine: {nb} candidates per batch (one per peak), 256^3 template, 256x256 "
+                                   "windows of a 1024^2 micrograph, 1/4 with a pixel-size change",
+                       "flush_l2": "inputs > L2 not needed: each batch reads its own candidates"},
+            "e2e": {"value": rate, "unit": "candidates/s", "h2d_bytes_per_step": nb * 6 * 4,
+                    "d2h_bytes_per_step": nb * 3 * 4},
+            "gpu_launches": args.steps * 11, "clocks": clk.summary()}), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def _cpu_threads():
     """Host threads for the CPU legs (each thread holds ~0.6 GB of 4096^2 buffers)."""
     threads = min(os.cpu_count() or 1, 32)
@@ -488,8 +552,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--accuracy", type=int, default=4,
                     help="orientations compared with the FP64 oracle after timing, in the CPU-baseline leg (0 = skip)")
-    ap.add_argument("--workload", default="full", choices=sorted(WORKLOADS) + ["batched"],
+    ap.add_argument("--workload", default="full", choices=sorted(WORKLOADS) + ["batched", "refine"],
                     help="full = the metric's 4096^2 configuration; the others are the uneven and stress geometries")
+    ap.add_argument("--refine-batch", type=int, default=256, help="candidates per TemplateScore batch (--workload refine)")
     ap.add_argument("--traffic-b", type=float, default=None, help="ncu DRAM bytes per pass-B launch")
     ap.add_argument("--traffic-c", type=float, default=None, help="ncu DRAM bytes per pass-C launch")
     args = ap.parse_args()
@@ -501,6 +566,8 @@ def main():
         run_reference(args)
     elif args.workload == "batched":
         run_batched(args)
+    elif args.workload == "refine":
+        run_refine(args)
     else:
         run_ours(args)
 

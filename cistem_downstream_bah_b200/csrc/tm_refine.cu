@@ -467,18 +467,29 @@ int run_batch(tm_refine_ctx* c, int n, int n_jobs) {
     a.twt.lmax = TP;
     using SC = tmrk::tmk::SliceCol<TP>;
     using RC = tmrk::tmk::RowC2R<TP>;
+#define TR_LAUNCHED(name)                                                                                   \
+    do {                                                                                                    \
+        cudaError_t e_ = cudaGetLastError();                                                                \
+        if (e_ != cudaSuccess) return rset_err(c, TM_ERR_CUDA, "%s launch failed: %s", name, cudaGetErrorString(e_)); \
+    } while (0)
     tmrk::tmk::k_slice_colfft<TP><<<dim3((TP / 2 + 1 + SC::CB - 1) / SC::CB, n), SC::NT, 0, s>>>(a);
+    TR_LAUNCHED("k_slice_colfft");
     tmrk::tmk::k_row_c2r<TP><<<dim3(TP / RC::ROWS, n), RC::NT, 0, s>>>(a);
+    TR_LAUNCHED("k_row_c2r");
     if (n_jobs > 0) {
         tmr::k_disc_mean<<<n_jobs, 256, 0, s>>>(c->P, c->jobs, c->has_pad, c->pv, TP);
+        TR_LAUNCHED("k_disc_mean");
         // Z = (P - pv) [brt | bit]            (TP x 2T)
         tmr::k_gemm<<<dim3((2 * T + 63) / 64, (TP + 63) / 64, n_jobs), 256, 0, s>>>(c->gjobs, TP, 2 * T, TP, TP,
                                                                                     2 * T, 2 * T, 0);
+        TR_LAUNCHED("k_gemm (1)");
         // Q = Ar Z[:, :T] + (-Ai) Z[:, T:]     (T x T)
         tmr::k_gemm<<<dim3((T + 63) / 64, (T + 63) / 64, n_jobs), 256, 0, s>>>(c->gjobs + n_jobs, T, T, TP, 2 * TP,
                                                                               2 * T, T, 0);
+        TR_LAUNCHED("k_gemm (2)");
         tmr::k_gemm<<<dim3((T + 63) / 64, (T + 63) / 64, n_jobs), 256, 0, s>>>(c->gjobs + 2 * n_jobs, T, T, TP,
                                                                               2 * TP, 2 * T, T, 1);
+        TR_LAUNCHED("k_gemm (3)");
     }
     TR_CUDA(c, cudaMemsetAsync(c->sumsq, 0, sizeof(double) * n, s));
     tmr::ScoreArgs sa{};
@@ -503,11 +514,14 @@ int run_batch(tm_refine_ctx* c, int n, int n_jobs) {
     using CS = tmr::ColS<T>;
     using R2 = tmr::RowC2RMax<T>;
     tmr::k_score_row_r2c<T><<<dim3(T / R1::ROWS, n), R1::NT, 0, s>>>(sa);
+    TR_LAUNCHED("k_score_row_r2c");
     tmr::k_score_col<T><<<dim3((T / 2 + 1 + CS::CB - 1) / CS::CB, n), CS::NT, 0, s>>>(sa);
+    TR_LAUNCHED("k_score_col");
     tmr::k_score_row_c2r_max<T><<<dim3(T / R2::ROWS, n), R2::NT, 0, s>>>(sa);
+    TR_LAUNCHED("k_score_row_c2r_max");
     tmr::k_score_peak<T><<<(n + 7) / 8, 256, 0, s>>>(sa);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return rset_err(c, TM_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+    TR_LAUNCHED("k_score_peak");
+#undef TR_LAUNCHED
     return TM_OK;
 }
 
@@ -526,7 +540,7 @@ const RefineVariant kRefineVariants[] = {
 void rfree(tm_refine_ctx* c) {
     void* d[] = {c->tmpl, c->particles, c->S, c->R, c->tw_tp, c->tw_t, c->filters, c->ops, c->ones, c->rot, c->P,
                  c->Z, c->Q, c->pv, c->rowmax, c->out, c->rowstat, c->sumsq, c->cand, c->rowarg, c->jobs,
-                 c->has_pad, c->gjobs};
+                 c->gjobs};   // has_pad lives inside jobs
     for (void* p : d)
         if (p) cudaFree(p);
     void* h[] = {c->h_rot, c->h_cand, c->h_jobs, c->h_gjobs, c->h_out, c->op_has_pad_host};
