@@ -32,7 +32,7 @@ EXPORTED = [
     "tm_get_results", "tm_correlations_computed", "tm_last_timing", "tm_debug_stage_buffers", "tm_destroy",
     "tm_last_error", "tm_version", "tm_run_plane_noalloc", "tm_autotune_batch", "tm_orientation_batch",
     "tm_refine_create", "tm_refine_set_particle", "tm_refine_set_filter", "tm_refine_set_operator",
-    "tm_refine_score", "tm_refine_last_error", "tm_refine_destroy",
+    "tm_refine_score", "tm_refine_last_error", "tm_refine_destroy", "tm_set_micrograph", "tm_whiten_micrograph",
 ]
 
 
@@ -98,6 +98,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.tm_refine_last_error.argtypes = [vp]
     L.tm_refine_last_error.restype = ctypes.c_char_p
     L.tm_refine_destroy.argtypes = [vp]
+    L.tm_set_micrograph.argtypes = [vp, vp, ip, ip, vp, ip, ctypes.POINTER(ctypes.c_int)]
+    L.tm_whiten_micrograph.argtypes = [ip, vp, ip, ip, vp, vp, ip, ctypes.POINTER(ctypes.c_int)]
     _LIB = L
     return L
 
@@ -139,6 +141,17 @@ class SearchCore:
         s = np.ascontiguousarray(spectrum, dtype=np.complex64)
         assert s.shape == (self.Y, self.X // 2 + 1), s.shape
         self._check(self.L.tm_set_image(self.h, _ptr(s), self.X, self.Y))
+
+    def set_micrograph(self, image):
+        """Whitens the padded micrograph on the device and makes it the
+        context's image; returns the whitening curve."""
+        img = np.ascontiguousarray(image, dtype=np.float32)
+        assert img.shape == (self.Y, self.X), img.shape
+        cap = int((self.X / 2.0 + 1.0) * float(np.sqrt(np.float32(2.0))) + 1.0) + 8
+        curve = np.zeros(cap, np.float64)
+        n = ctypes.c_int()
+        self._check(self.L.tm_set_micrograph(self.h, _ptr(img), self.X, self.Y, _ptr(curve), cap, ctypes.byref(n)))
+        return curve[:n.value].copy()
 
     def reset(self):
         self._check(self.L.tm_reset_results(self.h))
@@ -330,4 +343,20 @@ class RefineCore:
             self.close()
         except Exception:
             pass
+
+
+def whiten_micrograph(image, device=0):
+    """Device whitening of a padded micrograph (tm_whiten_micrograph):
+    (half spectrum complex64 (ny, nx//2+1), whitening curve)."""
+    L = load()
+    img = np.ascontiguousarray(image, dtype=np.float32)
+    ny, nx = img.shape
+    spec = np.zeros((ny, nx // 2 + 1), np.complex64)
+    cap = int((nx / 2.0 + 1.0) * float(np.sqrt(np.float32(2.0))) + 1.0) + 8
+    curve = np.zeros(cap, np.float64)
+    n = ctypes.c_int()
+    rc = L.tm_whiten_micrograph(device, _ptr(img), nx, ny, _ptr(spec), _ptr(curve), cap, ctypes.byref(n))
+    if rc != TM_OK:
+        raise TmError(rc, "tm_whiten_micrograph failed")
+    return spec, curve[:n.value].copy()
 

@@ -19,6 +19,7 @@
 
 #include "../../include/tm_b200.h"
 #include "tm_kernels.cuh"
+#include "tm_whiten.cuh"
 
 #define TM_VERSION "tm_b200 0.1 (sm_100a, fp32 search path)"
 
@@ -90,13 +91,97 @@ int set_err(tm_ctx* c, int code, const char* fmt, ...) {
 // ---------------------------------------------------------------------------------------------
 // Kernel variants per geometry.
 
+// Device whitening of an X x Y micrograph into its half spectrum (tm_whiten.cuh).
+struct WhitenBuffers {
+    const float* img;     // X * Y reals
+    float2* spec;         // Y * (X/2+1)
+    double* scratch;      // 3 + 3 * npts doubles
+    float* xs;            // npts abscissae
+    tmfft::Twiddles twx, twy;
+};
+using WhitenFn = int (*)(cudaStream_t, int nsm, const WhitenBuffers&, std::vector<double>& curve, std::string& err);
+
 struct Variant {
     int T, X, Y;
     int W;   // row pitch alignment of the pass-B column chunks (columns)
     int (*run_batch)(tm_ctx*, tmk::BatchArgs&, bool timing);
     int (*configure)(tm_ctx*);
     int (*run_stages)(tm_ctx*, tmk::BatchArgs&);   // every kernel before the MIP epilogue
+    WhitenFn whiten;
 };
+
+// number of points of the whitening curve (match_template.cpp:702)
+int curve_points(int X) { return (int)((X / 2.0 + 1.0) * sqrtf(2.0f) + 1.0); }
+
+#define TW_CHECK(call)                                                               \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess) {                                                     \
+            err = std::string(#call) + ": " + cudaGetErrorString(e_);                \
+            return e_ == cudaErrorMemoryAllocation ? TM_ERR_OOM : TM_ERR_CUDA;      \
+        }                                                                            \
+    } while (0)
+
+template <int X, int Y>
+int whiten_on_device(cudaStream_t s, int nsm, const WhitenBuffers& b, std::vector<double>& curve, std::string& err) {
+    const int hc = X / 2 + 1;
+    const long long n = (long long)X * Y;
+    const int npts = curve_points(X);
+    double* stats = b.scratch;                 // sum, sum of squares, whitened sum of squares
+    double* pw = b.scratch + 3;
+    double* cnt = pw + npts;
+    double* wf = cnt + npts;
+    TW_CHECK(cudaMemsetAsync(b.scratch, 0, sizeof(double) * (3 + 2 * (size_t)npts), s));
+    tmw::k_w_stats<<<nsm * 4, 256, 0, s>>>(b.img, n, stats);
+    TW_CHECK(cudaGetLastError());
+    double st[2];
+    TW_CHECK(cudaMemcpyAsync(st, stats, sizeof st, cudaMemcpyDeviceToHost, s));
+    TW_CHECK(cudaStreamSynchronize(s));
+    // ReplaceOutliersWithMean(5) (image.cpp:986-1007), float as the host restatement forms it
+    const float mean = (float)(st[0] / n);
+    const float sigma = sqrtf(fabsf((float)(st[1] / n - (st[0] / n) * (st[0] / n))));
+    const float vmax = mean + 5.0f * sigma, vmin = mean - 5.0f * sigma;
+    using R = tmw::WRows<X>;
+    using C = tmw::WCols<Y>;
+    tmw::k_w_rows<X><<<(Y + R::ROWS - 1) / R::ROWS, R::NT, 0, s>>>(b.img, b.spec, Y, mean, vmin, vmax, b.twx);
+    TW_CHECK(cudaGetLastError());
+    if (C::SMEM > 48 * 1024) TW_CHECK(cudaFuncSetAttribute(tmw::k_w_cols<Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+    tmw::k_w_cols<Y><<<(hc + C::CB - 1) / C::CB, C::NT, C::SMEM, s>>>(b.spec, X, b.twy);
+    TW_CHECK(cudaGetLastError());
+    // the curve's abscissae (Curve::SetupXAxis(0, sqrt(2)/2, npts)), float
+    const float hi = 0.5f * sqrtf(2.0f);
+    std::vector<float> xs(npts);
+    for (int i = 0; i < npts; i++) xs[i] = i * (hi - 0.0f) / (float)(npts - 1) + 0.0f;
+    TW_CHECK(cudaMemcpyAsync(b.xs, xs.data(), sizeof(float) * npts, cudaMemcpyHostToDevice, s));
+    tmw::CurveArgs ca{b.xs, npts, xs[0], xs[1]};
+    const int curve_smem = (int)(2 * sizeof(double) * npts);
+    if (curve_smem > 48 * 1024)
+        TW_CHECK(cudaFuncSetAttribute(tmw::k_w_curve, cudaFuncAttributeMaxDynamicSharedMemorySize, curve_smem));
+    tmw::k_w_curve<<<nsm * 2, 256, curve_smem, s>>>(b.spec, X, Y, ca, pw, cnt);
+    TW_CHECK(cudaGetLastError());
+    std::vector<double> hpw(npts), hcnt(npts);
+    TW_CHECK(cudaMemcpyAsync(hpw.data(), pw, sizeof(double) * npts, cudaMemcpyDeviceToHost, s));
+    TW_CHECK(cudaMemcpyAsync(hcnt.data(), cnt, sizeof(double) * npts, cudaMemcpyDeviceToHost, s));
+    TW_CHECK(cudaStreamSynchronize(s));
+    // SquareRoot, Reciprocal, MultiplyByConstant(1 / max) (match_template.cpp:716-718)
+    curve.assign(npts, 0.0);
+    double mx = -DBL_MAX;
+    for (int i = 0; i < npts; i++) {
+        double v = hcnt[i] > 0 ? hpw[i] / hcnt[i] : 0.0;
+        v = sqrt(v);
+        if (v != 0.0) v = 1.0 / v;
+        curve[i] = v;
+        mx = std::max(mx, v);
+    }
+    for (double& v : curve) v *= 1.0 / mx;
+    TW_CHECK(cudaMemcpyAsync(wf, curve.data(), sizeof(double) * npts, cudaMemcpyHostToDevice, s));
+    tmw::k_w_apply<<<nsm * 4, 256, 0, s>>>(b.spec, X, Y, ca, wf, stats + 2);
+    TW_CHECK(cudaGetLastError());
+    tmw::k_w_scale<<<nsm * 4, 256, 0, s>>>(b.spec, (long long)Y * hc, stats + 2);
+    TW_CHECK(cudaGetLastError());
+    TW_CHECK(cudaStreamSynchronize(s));
+    return TM_OK;
+}
 
 template <int T, int X, int Y>
 struct Impl {
@@ -129,8 +214,9 @@ struct Impl {
     }
 };
 
-#define TM_VARIANT(T, X, Y) \
-    {T, X, Y, tmk::Launch<T, X, Y>::pass_b_width, &Impl<T, X, Y>::run_batch, &Impl<T, X, Y>::configure, &Impl<T, X, Y>::run_stages}
+#define TM_VARIANT(T, X, Y)                                                                                 \
+    {T, X, Y, tmk::Launch<T, X, Y>::pass_b_width, &Impl<T, X, Y>::run_batch, &Impl<T, X, Y>::configure,          \
+     &Impl<T, X, Y>::run_stages, &whiten_on_device<X, Y>}
 
 // Geometries with compiled kernels: template box T on a padded X x Y
 // micrograph.  X is a power of two (the reference turns a micrograph whose
@@ -384,6 +470,111 @@ int tm_set_image(tm_ctx* c, const float* spectrum, int image_x, int image_y) {
     int rc = wait_stream(c, 600.0);
     if (rc != TM_OK) return rc;
     c->has_image = true;
+    return TM_OK;
+}
+
+int tm_set_micrograph(tm_ctx* c, const float* image, int image_x, int image_y, double* curve, int curve_capacity,
+                      int* curve_points_out) {
+    if (!c || !image) return TM_ERR_INVALID;
+    if (image_x != c->X || image_y != c->Y)
+        return set_err(c, TM_ERR_INVALID, "image %d x %d differs from the context's %d x %d", image_x, image_y, c->X, c->Y);
+    TM_CUDA(c, cudaSetDevice(c->device));
+    const int X = c->X, Y = c->Y, XP = c->XP;
+    const int npts = curve_points(X);
+    if (curve && curve_capacity < npts)
+        return set_err(c, TM_ERR_INVALID, "curve capacity %d below the %d points of the whitening filter", curve_capacity, npts);
+    float* d_img = nullptr;
+    double* d_scratch = nullptr;
+    float* d_xs = nullptr;
+    int rc = dalloc(c, &d_img, (size_t)X * Y);
+    if (rc == TM_OK) rc = dalloc(c, &d_scratch, (size_t)3 + 3 * npts);
+    if (rc == TM_OK) rc = dalloc(c, &d_xs, (size_t)npts);
+    std::vector<double> h_curve;
+    if (rc == TM_OK) {
+        cudaError_t e = cudaMemcpyAsync(d_img, image, sizeof(float) * (size_t)X * Y, cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) rc = set_err(c, TM_ERR_CUDA, "micrograph upload: %s", cudaGetErrorString(e));
+    }
+    if (rc == TM_OK) {
+        // the whitened spectrum is staged in the correlation buffer C, as tm_set_image stages its input
+        WhitenBuffers wb{d_img, c->C, d_scratch, d_xs, make_args(c).tw, make_args(c).twy};
+        std::string err;
+        rc = c->var->whiten(c->stream, c->nsm, wb, h_curve, err);
+        if (rc != TM_OK) set_err(c, rc, "whitening: %s", err.c_str());
+    }
+    if (rc == TM_OK) {
+        tmk::k_prepare_image<<<dim3((XP + 127) / 128, Y), 128, 0, c->stream>>>(c->C, c->Ip, X, Y, XP, c->T);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = set_err(c, TM_ERR_CUDA, "k_prepare_image: %s", cudaGetErrorString(e));
+        if (rc == TM_OK) rc = wait_stream(c, 600.0);
+    }
+    if (d_img) cudaFree(d_img);
+    if (d_scratch) cudaFree(d_scratch);
+    if (d_xs) cudaFree(d_xs);
+    if (rc != TM_OK) return rc;
+    if (curve) memcpy(curve, h_curve.data(), sizeof(double) * npts);
+    if (curve_points_out) *curve_points_out = npts;
+    c->has_image = true;
+    return TM_OK;
+}
+
+int tm_whiten_micrograph(int device, const float* image, int image_x, int image_y, float* spectrum, double* curve,
+                         int curve_capacity, int* curve_points_out) {
+    if (!image || !spectrum || image_x <= 0 || image_y <= 0) return TM_ERR_INVALID;
+    const Variant* var = nullptr;
+    for (const Variant& v : kVariants)
+        if (v.X == image_x && v.Y == image_y) var = &v;
+    if (!var) return TM_ERR_UNSUPPORTED;
+    const int X = image_x, Y = image_y, hc = X / 2 + 1;
+    const int npts = curve_points(X);
+    if (curve && curve_capacity < npts) return TM_ERR_INVALID;
+    if (cudaSetDevice(device) != cudaSuccess) return TM_ERR_CUDA;
+    int dev_sms = 0;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
+    cudaStream_t s = nullptr;
+    float *d_img = nullptr, *d_xs = nullptr;
+    float2 *d_spec = nullptr, *d_twx = nullptr, *d_twy = nullptr;
+    double* d_scratch = nullptr;
+    int rc = TM_OK;
+    auto fail = [&](cudaError_t e) {
+        if (e != cudaSuccess && rc == TM_OK) rc = e == cudaErrorMemoryAllocation ? TM_ERR_OOM : TM_ERR_CUDA;
+    };
+    fail(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    if (rc == TM_OK) fail(cudaMalloc((void**)&d_img, sizeof(float) * (size_t)X * Y));
+    if (rc == TM_OK) fail(cudaMalloc((void**)&d_spec, sizeof(float2) * (size_t)Y * hc));
+    if (rc == TM_OK) fail(cudaMalloc((void**)&d_scratch, sizeof(double) * (3 + 3 * (size_t)npts)));
+    if (rc == TM_OK) fail(cudaMalloc((void**)&d_xs, sizeof(float) * npts));
+    if (rc == TM_OK) fail(cudaMalloc((void**)&d_twx, sizeof(float2) * X));
+    if (rc == TM_OK) fail(cudaMalloc((void**)&d_twy, sizeof(float2) * Y));
+    if (rc == TM_OK) {
+        for (int k = 0; k < 2 && rc == TM_OK; k++) {
+            const int L = k == 0 ? X : Y;
+            std::vector<float2> tw(L);
+            for (int m = 0; m < L; m++) {
+                const double ang = -2.0 * M_PI * (double)m / (double)L;
+                tw[m] = make_float2((float)cos(ang), (float)sin(ang));
+            }
+            fail(cudaMemcpy(k == 0 ? d_twx : d_twy, tw.data(), sizeof(float2) * L, cudaMemcpyHostToDevice));
+        }
+    }
+    if (rc == TM_OK) fail(cudaMemcpyAsync(d_img, image, sizeof(float) * (size_t)X * Y, cudaMemcpyHostToDevice, s));
+    std::vector<double> h_curve;
+    if (rc == TM_OK) {
+        tmfft::Twiddles twx{d_twx, X}, twy{d_twy, Y};
+        WhitenBuffers wb{d_img, d_spec, d_scratch, d_xs, twx, twy};
+        std::string err;
+        rc = var->whiten(s, dev_sms > 0 ? dev_sms : 148, wb, h_curve, err);
+    }
+    if (rc == TM_OK) {
+        fail(cudaMemcpyAsync(spectrum, d_spec, sizeof(float2) * (size_t)Y * hc, cudaMemcpyDeviceToHost, s));
+        if (rc == TM_OK) fail(cudaStreamSynchronize(s));
+    }
+    void* ptrs[] = {d_img, d_xs, d_spec, d_twx, d_twy, d_scratch};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (s) cudaStreamDestroy(s);
+    if (rc != TM_OK) return rc;
+    if (curve) memcpy(curve, h_curve.data(), sizeof(double) * npts);
+    if (curve_points_out) *curve_points_out = npts;
     return TM_OK;
 }
 

@@ -8,7 +8,7 @@
 //                        Hermitian mirror) x (-1)^(i+j), inverse FFT of
 //                        each column (shared with the search)
 //   k_row_c2r<TP>        inverse c2r of each row -> TP x TP projection
-//   [pixel-size change]  k_disc_mean + three batched GEMMs: the
+//   [pixel-size change]  k_disc_sum / k_disc_mean + three batched GEMMs: the
 //                        ChangePixelSize chain as out = Ar U Brt - Ai U Bit + pv,
 //                        U = projection - pv (operators built on the host)
 //   k_score_row_r2c<T>   r2c of each row of the T x T projection (or of the
@@ -300,46 +300,45 @@ __global__ void __launch_bounds__(256) k_score_peak(ScoreArgs a) {
 // pixel-size change
 //
 // pad value: mean of the projection within 0.45 TP of its centre
-// (ReturnAverageOfRealValues, image.cpp:6263-6300); one block per job
-__global__ void __launch_bounds__(256) k_disc_mean(const float* __restrict__ P, const int* __restrict__ jobs,
-                                                   const int* __restrict__ has_pad, float* pv, int TP) {
+// (ReturnAverageOfRealValues, image.cpp:6263-6300).  The squared distances
+// are sums of squared integers, exact in float, so the disc is the set the
+// reference's powf test selects; its pixel count is fixed per box.  Grid
+// (jobs, DISC_SPLIT): each block sums a band of rows into pvsum (double).
+constexpr int DISC_SPLIT = 8;
+
+__global__ void __launch_bounds__(256) k_disc_sum(const float* __restrict__ P, const int* __restrict__ jobs,
+                                                  const int* __restrict__ has_pad, double* pvsum, int TP) {
+    if (!has_pad[blockIdx.x]) return;
     const int b = jobs[blockIdx.x];
     __shared__ double rs[8];
-    __shared__ long long rc[8];
+    const float r2 = powf(0.45f * (float)TP, 2);
+    const int c = TP / 2;
+    const int rows = (TP + DISC_SPLIT - 1) / DISC_SPLIT;
+    const int j0 = blockIdx.y * rows, j1 = min(TP, j0 + rows);
+    const float* p = P + (size_t)b * TP * TP;
     double s = 0.0;
-    long long cnt = 0;
-    if (has_pad[blockIdx.x]) {
-        const float r2 = powf(0.45f * (float)TP, 2);
-        const int c = TP / 2;
-        const float* p = P + (size_t)b * TP * TP;
-        for (int idx = threadIdx.x; idx < TP * TP; idx += blockDim.x) {
-            const int j = idx / TP, i = idx % TP;
-            const float d = powf((float)(i - c), 2) + powf((float)(j - c), 2) + powf(0.0f, 2);
-            if (d <= r2) {
-                s += p[idx];
-                cnt++;
-            }
-        }
+    for (int idx = j0 * TP + threadIdx.x; idx < j1 * TP; idx += blockDim.x) {
+        const int j = idx / TP, i = idx % TP;
+        const float d = (float)((i - c) * (i - c) + (j - c) * (j - c));
+        if (d <= r2) s += p[idx];
     }
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        s += __shfl_xor_sync(0xffffffffu, s, off);
-        cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        rs[threadIdx.x >> 5] = s;
-        rc[threadIdx.x >> 5] = cnt;
-    }
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if ((threadIdx.x & 31) == 0) rs[threadIdx.x >> 5] = s;
     __syncthreads();
     if (threadIdx.x == 0) {
         double ts = 0.0;
-        long long tc = 0;
-        for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
-            ts += rs[k];
-            tc += rc[k];
-        }
-        pv[b] = tc > 0 ? (float)(ts / (double)tc) : 0.0f;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) ts += rs[k];
+        atomicAdd(pvsum + b, ts);
     }
+}
+
+__global__ void k_disc_mean(const int* __restrict__ jobs, const int* __restrict__ has_pad,
+                            const double* __restrict__ pvsum, float* pv, int n_jobs, double inv_count) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n_jobs) return;
+    const int b = jobs[j];
+    pv[b] = has_pad[j] ? (float)(pvsum[b] * inv_count) : 0.0f;
 }
 
 // C = (A - s) B (+ C): row-major, per job pointers; 64 x 64 tiles, 4 x 4 per thread
@@ -411,7 +410,8 @@ struct tm_refine_ctx {
     float2 *tmpl = nullptr, *particles = nullptr, *S = nullptr, *R = nullptr, *tw_tp = nullptr, *tw_t = nullptr;
     float *filters = nullptr, *ops = nullptr, *ones = nullptr, *rot = nullptr, *P = nullptr, *Z = nullptr, *Q = nullptr;
     float *pv = nullptr, *rowmax = nullptr, *out = nullptr;
-    double *rowstat = nullptr, *sumsq = nullptr;
+    double *rowstat = nullptr, *sumsq = nullptr, *pvsum = nullptr;
+    long long disc_count = 1;
     int *cand = nullptr, *rowarg = nullptr, *jobs = nullptr, *has_pad = nullptr;
     tmr::GemmJob* gjobs = nullptr;
     int* op_has_pad_host = nullptr;
@@ -477,7 +477,11 @@ int run_batch(tm_refine_ctx* c, int n, int n_jobs) {
     tmrk::tmk::k_row_c2r<TP><<<dim3(TP / RC::ROWS, n), RC::NT, 0, s>>>(a);
     TR_LAUNCHED("k_row_c2r");
     if (n_jobs > 0) {
-        tmr::k_disc_mean<<<n_jobs, 256, 0, s>>>(c->P, c->jobs, c->has_pad, c->pv, TP);
+        TR_CUDA(c, cudaMemsetAsync(c->pvsum, 0, sizeof(double) * n, s));
+        tmr::k_disc_sum<<<dim3(n_jobs, tmr::DISC_SPLIT), 256, 0, s>>>(c->P, c->jobs, c->has_pad, c->pvsum, TP);
+        TR_LAUNCHED("k_disc_sum");
+        tmr::k_disc_mean<<<(n_jobs + 127) / 128, 128, 0, s>>>(c->jobs, c->has_pad, c->pvsum, c->pv, n_jobs,
+                                                              1.0 / (double)c->disc_count);
         TR_LAUNCHED("k_disc_mean");
         // Z = (P - pv) [brt | bit]            (TP x 2T)
         tmr::k_gemm<<<dim3((2 * T + 63) / 64, (TP + 63) / 64, n_jobs), 256, 0, s>>>(c->gjobs, TP, 2 * T, TP, TP,
@@ -539,8 +543,8 @@ const RefineVariant kRefineVariants[] = {
 
 void rfree(tm_refine_ctx* c) {
     void* d[] = {c->tmpl, c->particles, c->S, c->R, c->tw_tp, c->tw_t, c->filters, c->ops, c->ones, c->rot, c->P,
-                 c->Z, c->Q, c->pv, c->rowmax, c->out, c->rowstat, c->sumsq, c->cand, c->rowarg, c->jobs,
-                 c->gjobs};   // has_pad lives inside jobs
+                 c->Z, c->Q, c->pv, c->rowmax, c->out, c->rowstat, c->sumsq, c->pvsum, c->cand, c->rowarg,
+                 c->jobs, c->gjobs};   // has_pad lives inside jobs
     for (void* p : d)
         if (p) cudaFree(p);
     void* h[] = {c->h_rot, c->h_cand, c->h_jobs, c->h_gjobs, c->h_out, c->op_has_pad_host};
@@ -626,6 +630,16 @@ int tm_refine_create(int device, int template_box, int projection_box, const flo
     TRY(dalloc(c, &c->Z, (size_t)TP * 2 * T * max_batch));
     TRY(dalloc(c, &c->Q, (size_t)T * T * max_batch));
     TRY(dalloc(c, &c->pv, (size_t)max_batch));
+    TRY(dalloc(c, &c->pvsum, (size_t)max_batch));
+    {
+        // pixels of the pad-value disc (0.45 TP around the centre)
+        const float r2 = powf(0.45f * (float)TP, 2);
+        long long cnt = 0;
+        for (int j = 0; j < TP; j++)
+            for (int i = 0; i < TP; i++)
+                if ((float)((i - TP / 2) * (i - TP / 2) + (j - TP / 2) * (j - TP / 2)) <= r2) cnt++;
+        c->disc_count = cnt > 0 ? cnt : 1;
+    }
     TRY(dalloc(c, &c->R, hc_size(T) * max_batch));
     TRY(dalloc(c, &c->sumsq, (size_t)max_batch));
     TRY(dalloc(c, &c->rowmax, (size_t)T * max_batch));

@@ -247,8 +247,17 @@ int run(const JobArgs& a) {
     EulerSearch euler;
     if (!euler.InitGrid(a.my_symmetry, angular_step)) throw CoreError(TM_ERR_INVALID, "unrecognised symmetry " + a.my_symmetry);
 
-    // micrograph whitening (:699-724)
-    Whitened w = whiten(input);
+    // micrograph whitening (:699-724), on the GPU
+    Whitened w;
+    {
+        const int npts = (int)((X / 2.0 + 1.0) * sqrtf(2.0f) + 1.0);
+        w.spectrum.resize((size_t)Y * (X / 2 + 1));
+        w.curve.resize(npts);
+        int got = 0;
+        const int rc = tm_whiten_micrograph(0, input.v.data(), X, Y, reinterpret_cast<float*>(w.spectrum.data()),
+                                            w.curve.data(), npts, &got);
+        if (rc != TM_OK) throw CoreError(rc, "micrograph whitening on the GPU failed");
+    }
     Image input_image;
     input_image.logical_x_dimension = X;
     input_image.logical_y_dimension = Y;

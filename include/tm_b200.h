@@ -78,6 +78,25 @@ TM_API int tm_set_template(tm_ctx *ctx, const float *spectrum, int template_size
  * interleaved float pairs, layout [y][x]. */
 TM_API int tm_set_image(tm_ctx *ctx, const float *spectrum, int image_x, int image_y);
 
+/* Micrograph whitening on the device (no counterpart in the reference, whose
+ * DoCalculation whitens on the CPU, match_template.cpp:699-724): the padded
+ * (and, where the reference rotates it, rotated) image_x x image_y micrograph,
+ * [y][x] floats, goes through ReplaceOutliersWithMean(5), ForwardFFT,
+ * SwapRealSpaceQuadrants, ZeroCentralPixel, Compute1DPowerSpectrumCurve, the
+ * square root / reciprocal / 1/max of the curve, ApplyCurveFilter,
+ * ZeroCentralPixel and the division by sqrt(ReturnSumOfSquares) -- the
+ * spectrum tm_set_image takes -- and becomes the context's micrograph.  curve
+ * (may be NULL) receives the whitening filter the projection filters use,
+ * int((image_x/2+1) sqrt(2) + 1) points on [0, sqrt(2)/2]; curve_points (may
+ * be NULL) that count. */
+TM_API int tm_set_micrograph(tm_ctx *ctx, const float *image, int image_x, int image_y, double *curve,
+                             int curve_capacity, int *curve_points);
+
+/* The same whitening without a search context, for the sizes the search has
+ * kernels for: spectrum receives image_y*(image_x/2+1) complex (float pairs). */
+TM_API int tm_whiten_micrograph(int device, const float *image, int image_x, int image_y, float *spectrum,
+                                double *curve, int curve_capacity, int *curve_points);
+
 /* Clears the running MIP (to -FLT_MAX), best-orientation, sum, sum-of-squares
  * and histogram state, as RunInnerLoop does at entry (TemplateMatchingCore.cu:143-155). */
 TM_API int tm_reset_results(tm_ctx *ctx);
