@@ -33,6 +33,7 @@ EXPORTED = [
     "tm_last_error", "tm_version", "tm_run_plane_noalloc", "tm_autotune_batch", "tm_orientation_batch",
     "tm_refine_create", "tm_refine_set_particle", "tm_refine_set_filter", "tm_refine_set_operator",
     "tm_refine_score", "tm_refine_last_error", "tm_refine_destroy", "tm_set_micrograph", "tm_whiten_micrograph",
+    "tm_set_template_volume", "tm_template_spectrum",
 ]
 
 
@@ -100,6 +101,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.tm_refine_destroy.argtypes = [vp]
     L.tm_set_micrograph.argtypes = [vp, vp, ip, ip, vp, ip, ctypes.POINTER(ctypes.c_int)]
     L.tm_whiten_micrograph.argtypes = [ip, vp, ip, ip, vp, vp, ip, ctypes.POINTER(ctypes.c_int)]
+    L.tm_set_template_volume.argtypes = [vp, vp, ip, fp]
+    L.tm_template_spectrum.argtypes = [ip, vp, ip, fp, vp]
     _LIB = L
     return L
 
@@ -141,6 +144,12 @@ class SearchCore:
         s = np.ascontiguousarray(spectrum, dtype=np.complex64)
         assert s.shape == (self.Y, self.X // 2 + 1), s.shape
         self._check(self.L.tm_set_image(self.h, _ptr(s), self.X, self.Y))
+
+    def set_template_volume(self, volume, pixel_size_factor=1.0):
+        """Prepares the template spectrum on the device from the T^3 volume."""
+        v = np.ascontiguousarray(volume, dtype=np.float32)
+        assert v.shape == (self.T, self.T, self.T), v.shape
+        self._check(self.L.tm_set_template_volume(self.h, _ptr(v), self.T, float(pixel_size_factor)))
 
     def set_micrograph(self, image):
         """Whitens the padded micrograph on the device and makes it the
@@ -359,4 +368,16 @@ def whiten_micrograph(image, device=0):
     if rc != TM_OK:
         raise TmError(rc, "tm_whiten_micrograph failed")
     return spec, curve[:n.value].copy()
+
+
+def template_spectrum_device(volume, pixel_size_factor=1.0, device=0):
+    """Template spectrum prepared on the device (tm_template_spectrum)."""
+    L = load()
+    v = np.ascontiguousarray(volume, dtype=np.float32)
+    T = v.shape[0]
+    out = np.zeros((T, T, T // 2 + 1), np.complex64)
+    rc = L.tm_template_spectrum(device, _ptr(v), T, float(pixel_size_factor), _ptr(out))
+    if rc != TM_OK:
+        raise TmError(rc, "tm_template_spectrum failed")
+    return out
 

@@ -20,6 +20,11 @@
 #include "../../include/tm_b200.h"
 #include "tm_kernels.cuh"
 #include "tm_whiten.cuh"
+#include "tm_template.cuh"
+
+namespace tmcg {
+#include "tm_gemm.cuh"
+}  // namespace tmcg
 
 #define TM_VERSION "tm_b200 0.1 (sm_100a, fp32 search path)"
 
@@ -341,6 +346,219 @@ tmk::BatchArgs make_args(tm_ctx* c) {
 
 }  // namespace
 
+namespace {
+
+// ---------------------------------------------------------------------------------------------
+// Template spectrum on the device (tm_template.cuh).
+
+// The axis operators of the pixel-size change (image.cpp:8741-8822) for a
+// T^3 volume padded to P^3 and resampled to N^3: m[t][i] = sum_k w(k)
+// exp(2 pi i k (q/N - p/P)), q = N/2 + t - T/2, p = P/2 + i - T/2, as closed
+// geometric sums (x axis: half-spectrum weights; y and z: the full axis).
+void axis_operators(int T, int P, int N, std::vector<double>& mxr, std::vector<double>& mxi, std::vector<double>& myr,
+                    std::vector<double>& myi) {
+    const bool grow = N > P;
+    const long kx_hi = grow ? P / 2 : N / 2;
+    const long k_lo = grow ? -(P / 2) : -(N / 2), k_hi = grow ? P / 2 : N / 2 - 1;
+    const long NP = (long)N * P;
+    auto geo = [NP](long num, long a, long b, double& re, double& im) {
+        num %= NP;
+        if (num < 0) num += NP;
+        const long cnt = b - a + 1;
+        if (cnt <= 0) { re = im = 0.0; return; }
+        if (num == 0) { re = (double)cnt; im = 0.0; return; }
+        const double th = 2.0 * M_PI * (double)num / (double)NP;
+        // e^{i th a} (1 - e^{i th cnt}) / (1 - e^{i th})
+        const double ar = cos(th * a), ai = sin(th * a);
+        const double nr = 1.0 - cos(th * cnt), ni = -sin(th * cnt);
+        const double dr = 1.0 - cos(th), di = -sin(th);
+        const double qr = (nr * dr + ni * di) / (dr * dr + di * di), qi = (ni * dr - nr * di) / (dr * dr + di * di);
+        re = ar * qr - ai * qi;
+        im = ar * qi + ai * qr;
+    };
+    mxr.assign((size_t)T * T, 0.0); mxi.assign((size_t)T * T, 0.0);
+    myr.assign((size_t)T * T, 0.0); myi.assign((size_t)T * T, 0.0);
+    for (int t = 0; t < T; t++) {
+        const long q = N / 2 + t - T / 2;
+        for (int i = 0; i < T; i++) {
+            const long pp = P / 2 + i - T / 2;
+            const long num = q * P - pp * N;
+            double r0, i0, r1, i1;
+            geo(num, 0, kx_hi, r0, i0);
+            double xr = 2.0 * r0 - 1.0, xi = 2.0 * i0;
+            if (!grow) {
+                geo(num, N / 2, N / 2, r1, i1);
+                xr -= r1;
+                xi -= i1;
+            }
+            geo(num, k_lo, k_hi, r1, i1);
+            mxr[(size_t)t * T + i] = xr;
+            mxi[(size_t)t * T + i] = xi;
+            myr[(size_t)t * T + i] = r1;
+            myi[(size_t)t * T + i] = i1;
+        }
+    }
+}
+
+struct TemplateBuffers {
+    const float* vol;     // T^3 reals
+    float2* spec;         // T*T*(T/2+1)
+    float* work;          // 5 T^3 floats (pixel-size change only)
+    float* ops;           // 6 T*T floats
+    double* acc;          // 2 doubles
+    float* pad;           // 1 float
+    tmcg::GemmJob* jobs;  // 4 + 4 T jobs
+    tmfft::Twiddles tw;   // lmax = T
+};
+using TemplateFn = int (*)(cudaStream_t, int nsm, const TemplateBuffers&, float factor, std::string& err);
+
+template <int T>
+int template_on_device(cudaStream_t s, int nsm, const TemplateBuffers& b, float factor, std::string& err) {
+    constexpr int HC = T / 2 + 1;
+    const size_t n3 = (size_t)T * T * T;
+    const float tol = 0.001f;
+    const float* rows_src = b.vol;
+    float add = 0.0f;
+    if (!(fabsf(factor - 1.0f) < tol)) {
+        // sizes (image.cpp:8741-8775), cubic volume
+        const int old = T, min_dim = T;
+        int pad, nw;
+        if (tol < 1.0f / (min_dim * factor)) {
+            const float inter = 1.0f / (tol * min_dim);
+            pad = (int)(old * inter);
+            if ((old % 2 == 0) != (pad % 2 == 0)) pad++;
+            nw = (int)(pad / factor);
+            if ((old % 2 == 0) != (nw % 2 == 0)) nw++;
+        } else {
+            pad = (int)(old * factor);
+            if ((old % 2 == 0) != (pad % 2 == 0)) pad++;
+            nw = old;
+        }
+        if (nw <= T) {
+            err = "pixel-size change to a resampled box not larger than the template is not supported";
+            return TM_ERR_UNSUPPORTED;
+        }
+        float padding_value = 0.0f;
+        if (pad > old) {
+            TW_CHECK(cudaMemsetAsync(b.acc, 0, 2 * sizeof(double), s));
+            tmt::k_t_disc_sum<<<nsm * 4, 256, 0, s>>>(b.vol, T, b.acc);
+            TW_CHECK(cudaGetLastError());
+            double acc[2];
+            TW_CHECK(cudaMemcpyAsync(acc, b.acc, sizeof acc, cudaMemcpyDeviceToHost, s));
+            TW_CHECK(cudaStreamSynchronize(s));
+            padding_value = acc[1] > 0 ? (float)(acc[0] / acc[1]) : 0.0f;
+        }
+        std::vector<double> mxr, mxi, myr, myi;
+        axis_operators(T, pad, nw, mxr, mxi, myr, myi);
+        // ops: mxr^T, mxi^T (B operands of the x pass), myr, -myi, myi (y pass),
+        // myr / P^3 and -myi / P^3 (z pass)
+        const size_t t2 = (size_t)T * T;
+        std::vector<float> ops(7 * t2);
+        const double inv = 1.0 / ((double)pad * pad * pad);
+        for (int t = 0; t < T; t++)
+            for (int i = 0; i < T; i++) {
+                const size_t ti = (size_t)t * T + i, it = (size_t)i * T + t;
+                ops[0 * t2 + it] = (float)mxr[ti];
+                ops[1 * t2 + it] = (float)mxi[ti];
+                ops[2 * t2 + ti] = (float)myr[ti];
+                ops[3 * t2 + ti] = (float)-myi[ti];
+                ops[4 * t2 + ti] = (float)myi[ti];
+                ops[5 * t2 + ti] = (float)(myr[ti] * inv);
+                ops[6 * t2 + ti] = (float)(-myi[ti] * inv);
+            }
+        TW_CHECK(cudaMemcpyAsync(b.ops, ops.data(), sizeof(float) * ops.size(), cudaMemcpyHostToDevice, s));
+        TW_CHECK(cudaMemcpyAsync(b.pad, &padding_value, sizeof(float), cudaMemcpyHostToDevice, s));
+        float *Ar = b.work, *Ai = Ar + n3, *Br = Ai + n3, *Bi = Br + n3, *out = Bi + n3;
+        const float* op = b.ops;
+        std::vector<tmcg::GemmJob> jobs;
+        // x pass: A = (vol - pad) mx^T (T^2 x T)
+        jobs.push_back({b.vol, op + 0 * t2, Ar, b.pad});
+        jobs.push_back({b.vol, op + 1 * t2, Ai, b.pad});
+        // z pass: out = myr/P^3 Br - myi/P^3 Bi (T x T^2)
+        jobs.push_back({op + 5 * t2, Br, out, nullptr});
+        jobs.push_back({op + 6 * t2, Bi, out, nullptr});
+        // y pass per z plane: Br = myr Ar - myi Ai, Bi = myr Ai + myi Ar
+        for (int pass = 0; pass < 4; pass++)
+            for (int z = 0; z < T; z++) {
+                const size_t o = (size_t)z * t2;
+                const float* A = op + (pass == 0 || pass == 2 ? 2 : pass == 1 ? 3 : 4) * t2;
+                const float* Bm = (pass == 0 || pass == 3) ? Ar + o : Ai + o;
+                float* Cm = (pass < 2) ? Br + o : Bi + o;
+                jobs.push_back({A, Bm, Cm, nullptr});
+            }
+        TW_CHECK(cudaMemcpyAsync(b.jobs, jobs.data(), sizeof(tmcg::GemmJob) * jobs.size(), cudaMemcpyHostToDevice, s));
+        const int TT = T * T;
+        tmcg::k_gemm<<<dim3((T + 63) / 64, (TT + 63) / 64, 2), 256, 0, s>>>(b.jobs, TT, T, T, T, T, T, 0);
+        TW_CHECK(cudaGetLastError());
+        for (int pass = 0; pass < 4; pass++) {
+            tmcg::k_gemm<<<dim3((T + 63) / 64, (T + 63) / 64, T), 256, 0, s>>>(b.jobs + 4 + pass * T, T, T, T, T, T, T,
+                                                                              pass % 2);
+            TW_CHECK(cudaGetLastError());
+        }
+        tmcg::k_gemm<<<dim3((TT + 63) / 64, (T + 63) / 64, 1), 256, 0, s>>>(b.jobs + 2, T, TT, T, T, TT, TT, 0);
+        TW_CHECK(cudaGetLastError());
+        tmcg::k_gemm<<<dim3((TT + 63) / 64, (T + 63) / 64, 1), 256, 0, s>>>(b.jobs + 3, T, TT, T, T, TT, TT, 1);
+        TW_CHECK(cudaGetLastError());
+        rows_src = out;
+        add = padding_value;
+    }
+    using R = tmt::TRows<T>;
+    using C = tmt::TCols<T>;
+    tmt::k_t_rows<T><<<(T * T + R::ROWS - 1) / R::ROWS, R::NT, 0, s>>>(rows_src, add, b.spec, b.tw);
+    TW_CHECK(cudaGetLastError());
+    const long long ncols = (long long)T * HC;
+    tmt::k_t_cols<T><<<(unsigned)((ncols + C::CB - 1) / C::CB), C::NT, 0, s>>>(b.spec, ncols, HC, (long long)T * HC, HC, 0,
+                                                                              b.tw);
+    TW_CHECK(cudaGetLastError());
+    tmt::k_t_cols<T><<<(unsigned)((ncols + C::CB - 1) / C::CB), C::NT, 0, s>>>(b.spec, ncols, ncols, 0, ncols, 1, b.tw);
+    TW_CHECK(cudaGetLastError());
+    TW_CHECK(cudaStreamSynchronize(s));
+    return TM_OK;
+}
+
+struct TemplateVariant {
+    int T;
+    TemplateFn fn;
+};
+const TemplateVariant kTemplateVariants[] = {
+    {32, template_on_device<32>},   {48, template_on_device<48>},   {64, template_on_device<64>},
+    {128, template_on_device<128>}, {256, template_on_device<256>}, {384, template_on_device<384>},
+};
+
+TemplateFn find_template_fn(int T) {
+    for (const TemplateVariant& v : kTemplateVariants)
+        if (v.T == T) return v.fn;
+    return nullptr;
+}
+
+// device buffers of one template preparation (freed by the caller)
+struct TemplateScratch {
+    float* vol = nullptr;
+    float* work = nullptr;
+    float* ops = nullptr;
+    double* acc = nullptr;
+    float* pad = nullptr;
+    tmcg::GemmJob* jobs = nullptr;
+    void release() {
+        void* p[] = {vol, work, ops, acc, pad, jobs};
+        for (void* q : p)
+            if (q) cudaFree(q);
+        *this = TemplateScratch{};
+    }
+    cudaError_t alloc(int T, bool resample) {
+        const size_t n3 = (size_t)T * T * T;
+        cudaError_t e = cudaMalloc((void**)&vol, sizeof(float) * n3);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&acc, 2 * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&pad, sizeof(float));
+        if (e == cudaSuccess && resample) e = cudaMalloc((void**)&work, sizeof(float) * 5 * n3);
+        if (e == cudaSuccess && resample) e = cudaMalloc((void**)&ops, sizeof(float) * 7 * (size_t)T * T);
+        if (e == cudaSuccess && resample) e = cudaMalloc((void**)&jobs, sizeof(tmcg::GemmJob) * (4 + 4 * (size_t)T));
+        return e;
+    }
+};
+
+}  // namespace
+
 extern "C" {
 
 const char* tm_version(void) { return TM_VERSION; }
@@ -576,6 +794,77 @@ int tm_whiten_micrograph(int device, const float* image, int image_x, int image_
     if (curve) memcpy(curve, h_curve.data(), sizeof(double) * npts);
     if (curve_points_out) *curve_points_out = npts;
     return TM_OK;
+}
+
+int tm_set_template_volume(tm_ctx* c, const float* volume, int template_size, float pixel_size_factor) {
+    if (!c || !volume) return TM_ERR_INVALID;
+    if (template_size != c->T) return set_err(c, TM_ERR_INVALID, "template size %d differs from the context's %d", template_size, c->T);
+    TemplateFn fn = find_template_fn(c->T);
+    if (!fn) return set_err(c, TM_ERR_UNSUPPORTED, "no template kernels for box %d", c->T);
+    TM_CUDA(c, cudaSetDevice(c->device));
+    const bool resample = !(fabsf(pixel_size_factor - 1.0f) < 0.001f);
+    TemplateScratch sc;
+    cudaError_t e = sc.alloc(c->T, resample);
+    if (e != cudaSuccess) {
+        sc.release();
+        return set_err(c, e == cudaErrorMemoryAllocation ? TM_ERR_OOM : TM_ERR_CUDA, "template buffers: %s", cudaGetErrorString(e));
+    }
+    int rc = TM_OK;
+    e = cudaMemcpyAsync(sc.vol, volume, sizeof(float) * (size_t)c->T * c->T * c->T, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) rc = set_err(c, TM_ERR_CUDA, "template upload: %s", cudaGetErrorString(e));
+    if (rc == TM_OK) {
+        TemplateBuffers tb{sc.vol, c->tmpl, sc.work, sc.ops, sc.acc, sc.pad, sc.jobs, make_args(c).twt};
+        std::string err;
+        rc = fn(c->stream, c->nsm, tb, pixel_size_factor, err);
+        if (rc != TM_OK) set_err(c, rc, "template preparation: %s", err.c_str());
+    }
+    sc.release();
+    if (rc == TM_OK) c->has_template = true;
+    return rc;
+}
+
+int tm_template_spectrum(int device, const float* volume, int template_size, float pixel_size_factor, float* spectrum) {
+    if (!volume || !spectrum) return TM_ERR_INVALID;
+    const int T = template_size;
+    TemplateFn fn = find_template_fn(T);
+    if (!fn) return TM_ERR_UNSUPPORTED;
+    if (cudaSetDevice(device) != cudaSuccess) return TM_ERR_CUDA;
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    const bool resample = !(fabsf(pixel_size_factor - 1.0f) < 0.001f);
+    const size_t nspec = (size_t)T * T * (T / 2 + 1);
+    TemplateScratch sc;
+    cudaStream_t s = nullptr;
+    float2 *d_spec = nullptr, *d_tw = nullptr;
+    int rc = TM_OK;
+    auto fail = [&](cudaError_t e) {
+        if (e != cudaSuccess && rc == TM_OK) rc = e == cudaErrorMemoryAllocation ? TM_ERR_OOM : TM_ERR_CUDA;
+    };
+    fail(sc.alloc(T, resample));
+    if (rc == TM_OK) fail(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    if (rc == TM_OK) fail(cudaMalloc((void**)&d_spec, sizeof(float2) * nspec));
+    if (rc == TM_OK) fail(cudaMalloc((void**)&d_tw, sizeof(float2) * T));
+    if (rc == TM_OK) {
+        std::vector<float2> tw(T);
+        for (int m = 0; m < T; m++) {
+            const double ang = -2.0 * M_PI * (double)m / (double)T;
+            tw[m] = make_float2((float)cos(ang), (float)sin(ang));
+        }
+        fail(cudaMemcpy(d_tw, tw.data(), sizeof(float2) * T, cudaMemcpyHostToDevice));
+    }
+    if (rc == TM_OK) fail(cudaMemcpyAsync(sc.vol, volume, sizeof(float) * (size_t)T * T * T, cudaMemcpyHostToDevice, s));
+    if (rc == TM_OK) {
+        TemplateBuffers tb{sc.vol, d_spec, sc.work, sc.ops, sc.acc, sc.pad, sc.jobs, tmfft::Twiddles{d_tw, T}};
+        std::string err;
+        rc = fn(s, nsm > 0 ? nsm : 148, tb, pixel_size_factor, err);
+    }
+    if (rc == TM_OK) fail(cudaMemcpyAsync(spectrum, d_spec, sizeof(float2) * nspec, cudaMemcpyDeviceToHost, s));
+    if (rc == TM_OK) fail(cudaStreamSynchronize(s));
+    sc.release();
+    if (d_spec) cudaFree(d_spec);
+    if (d_tw) cudaFree(d_tw);
+    if (s) cudaStreamDestroy(s);
+    return rc;
 }
 
 int tm_reset_results(tm_ctx* c) {

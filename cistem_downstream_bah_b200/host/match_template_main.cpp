@@ -319,8 +319,14 @@ int run(const JobArgs& a) {
         template_reconstruction.logical_y_dimension = T;
         template_reconstruction.logical_z_dimension = T;
         template_reconstruction.is_in_real_space = false;
-        template_reconstruction.complex_values =
-            template_spectrum(rec.data, T, (a.pixel_size + float(size_i) * pixel_size_step) / a.pixel_size);
+        // the template spectrum of this pixel size (:842-845), prepared on the GPU
+        template_reconstruction.complex_values.resize((size_t)T * T * (T / 2 + 1));
+        {
+            const float factor = (a.pixel_size + float(size_i) * pixel_size_step) / a.pixel_size;
+            const int rc = tm_template_spectrum(0, rec.data.data(), T, factor,
+                                                reinterpret_cast<float*>(template_reconstruction.complex_values.data()));
+            if (rc != TM_OK) throw CoreError(rc, "template preparation on the GPU failed");
+        }
         if (first_loop) {
             core.Init(nullptr, template_reconstruction, input_image, current_projection, pixel_size_search_range,
                       pixel_size_step, a.pixel_size, defocus_search_range, defocus_step, a.defocus1, a.defocus2,

@@ -97,6 +97,20 @@ TM_API int tm_set_micrograph(tm_ctx *ctx, const float *image, int image_x, int i
 TM_API int tm_whiten_micrograph(int device, const float *image, int image_x, int image_y, float *spectrum,
                                 double *curve, int curve_capacity, int *curve_points);
 
+/* Template spectrum on the device (the reference prepares it on the CPU,
+ * match_template.cpp:842-845): the T^3 real volume ([z][y][x]) goes through
+ * ChangePixelSize(pixel_size_factor, tolerance 0.001, return_fft),
+ * ZeroCentralPixel and SwapRealSpaceQuadrants -- the spectrum tm_set_template
+ * takes -- and becomes the context's template.  Boxes 32, 48, 64, 128, 256,
+ * 384; a factor whose resampled box is not larger than T returns
+ * TM_ERR_UNSUPPORTED. */
+TM_API int tm_set_template_volume(tm_ctx *ctx, const float *volume, int template_size, float pixel_size_factor);
+
+/* The same without a search context: spectrum receives T*T*(T/2+1) complex
+ * (float pairs). */
+TM_API int tm_template_spectrum(int device, const float *volume, int template_size, float pixel_size_factor,
+                                float *spectrum);
+
 /* Clears the running MIP (to -FLT_MAX), best-orientation, sum, sum-of-squares
  * and histogram state, as RunInnerLoop does at entry (TemplateMatchingCore.cu:143-155). */
 TM_API int tm_reset_results(tm_ctx *ctx);
