@@ -49,6 +49,7 @@ struct tm_ctx {
     const Variant* var = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_prep = nullptr, ev_b = nullptr, ev_c = nullptr, ev_end = nullptr;
+    cudaEvent_t ev_batch[2][4] = {};   // first / last batch of a plane: begin, after prep, pass B, pass C
     // device buffers
     float2 *tmpl = nullptr, *Ip = nullptr, *S = nullptr, *A = nullptr, *C = nullptr, *norm = nullptr;
     float2 *twx = nullptr, *twy = nullptr, *twt = nullptr;   // twiddle tables of the x, y and template lengths
@@ -109,7 +110,7 @@ using WhitenFn = int (*)(cudaStream_t, int nsm, const WhitenBuffers&, std::vecto
 struct Variant {
     int T, X, Y;
     int W;   // row pitch alignment of the pass-B column chunks (columns)
-    int (*run_batch)(tm_ctx*, tmk::BatchArgs&, bool timing);
+    int (*run_batch)(tm_ctx*, tmk::BatchArgs&, cudaEvent_t* ev);   // ev: 4 events to record (or null)
     int (*configure)(tm_ctx*);
     int (*run_stages)(tm_ctx*, tmk::BatchArgs&);   // every kernel before the MIP epilogue
     WhitenFn whiten;
@@ -205,14 +206,15 @@ struct Impl {
         return TM_OK;
     }
 
-    static int run_batch(tm_ctx* c, tmk::BatchArgs& a, bool timing) {
+    static int run_batch(tm_ctx* c, tmk::BatchArgs& a, cudaEvent_t* ev) {
         cudaStream_t s = c->stream;
+        if (ev) cudaEventRecord(ev[0], s);
         LN::prep(a, s);
-        if (timing) cudaEventRecord(c->ev_prep, s);
+        if (ev) cudaEventRecord(ev[1], s);
         LN::pass_b(a, s, c->nsm);
-        if (timing) cudaEventRecord(c->ev_b, s);
+        if (ev) cudaEventRecord(ev[2], s);
         LN::pass_c(a, s);
-        if (timing) cudaEventRecord(c->ev_c, s);
+        if (ev) cudaEventRecord(ev[3], s);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return set_err(c, TM_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
         return TM_OK;
@@ -277,7 +279,9 @@ int wait_stream(tm_ctx* c, double limit_s) {
         if (e != cudaErrorNotReady) return set_err(c, TM_ERR_CUDA, "device error: %s", cudaGetErrorString(e));
         double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (el > limit_s) return set_err(c, TM_ERR_TIMEOUT, "stream did not finish within %.0f s", limit_s);
-        std::this_thread::sleep_for(std::chrono::microseconds(200));
+        // yield for the first milliseconds (a plane's tail), then poll every 20 us
+        if (el < 2e-3) std::this_thread::yield();
+        else std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
 }
 
@@ -291,6 +295,9 @@ void free_all(tm_ctx* c) {
     cudaEvent_t evs[] = {c->ev_start, c->ev_prep, c->ev_b, c->ev_c, c->ev_end};
     for (cudaEvent_t e : evs)
         if (e) cudaEventDestroy(e);
+    for (auto& set : c->ev_batch)
+        for (cudaEvent_t e : set)
+            if (e) cudaEventDestroy(e);
 }
 
 // The two used columns of RotationMatrix::SetToEulerRotation (matrix.cpp:490-510)
@@ -605,6 +612,9 @@ int tm_create(const tm_dims* dims, tm_ctx** out) {
         if (e == cudaSuccess) e = cudaEventCreate(&c->ev_b);
         if (e == cudaSuccess) e = cudaEventCreate(&c->ev_c);
         if (e == cudaSuccess) e = cudaEventCreate(&c->ev_end);
+        for (auto& set : c->ev_batch)
+            for (cudaEvent_t& ev : set)
+                if (e == cudaSuccess) e = cudaEventCreate(&ev);
         if (e != cudaSuccess) { *out = c; return set_err(c, TM_ERR_CUDA, "stream/event creation: %s", cudaGetErrorString(e)); }
     }
     if (dims->orientation_batch <= 0) {
@@ -922,32 +932,17 @@ int tm_run_plane(tm_ctx* c, const float* projection_filter, const float* euler_a
     TM_CUDA(c, cudaEventRecord(c->ev_start, c->stream));
     double b_ms = 0, c_ms = 0, prep_ms = 0;
     const int nbatch = (n + c->B - 1) / c->B;
+    int timed_nb[2] = {0, 0};
     for (int bi = 0; bi < nbatch; bi++) {
         a.orient0 = bi * c->B;
         a.nb = n - a.orient0 < c->B ? n - a.orient0 : c->B;
         a.gidx0 = pl.base + a.orient0;
-        // time the kernel families on the first and last batch only (events
-        // cost a little; the split is for roofline accounting)
-        const bool timing = (bi == 0 || bi == nbatch - 1);
-        cudaEvent_t evb0 = nullptr;
-        if (timing) {
-            TM_CUDA(c, cudaEventRecord(c->ev_end, c->stream));
-            evb0 = c->ev_end;
-        }
-        int rc = c->var->run_batch(c, a, timing);
+        // the kernel families are timed on the first and last batch (events
+        // read after the plane, so the stream never stalls for them)
+        const int set = bi == 0 ? 0 : (bi == nbatch - 1 ? 1 : -1);
+        if (set >= 0) timed_nb[set] = a.nb;
+        int rc = c->var->run_batch(c, a, set >= 0 ? c->ev_batch[set] : nullptr);
         if (rc != TM_OK) return rc;
-        if (timing) {
-            int w = wait_stream(c, 600.0);
-            if (w != TM_OK) return w;
-            float t_prep = 0, t_b = 0, t_c = 0;
-            cudaEventElapsedTime(&t_prep, evb0, c->ev_prep);
-            cudaEventElapsedTime(&t_b, c->ev_prep, c->ev_b);
-            cudaEventElapsedTime(&t_c, c->ev_b, c->ev_c);
-            const double scale = (double)a.nb;
-            prep_ms += t_prep / scale;
-            b_ms += t_b / scale;
-            c_ms += t_c / scale;
-        }
         if (progress) {
             if (progress((long long)(a.orient0 + a.nb), (long long)n, user) != 0) {
                 int w = wait_stream(c, 600.0);
@@ -969,6 +964,17 @@ int tm_run_plane(tm_ctx* c, const float* projection_filter, const float* euler_a
     }
     float tot = 0;
     cudaEventElapsedTime(&tot, c->ev_start, c->ev_c);
+    for (int set = 0; set < (nbatch > 1 ? 2 : 1); set++) {
+        float t_prep = 0, t_b = 0, t_c = 0;
+        cudaEvent_t* ev = c->ev_batch[set];
+        cudaEventElapsedTime(&t_prep, ev[0], ev[1]);
+        cudaEventElapsedTime(&t_b, ev[1], ev[2]);
+        cudaEventElapsedTime(&t_c, ev[2], ev[3]);
+        const double scale = (double)timed_nb[set];
+        prep_ms += t_prep / scale;
+        b_ms += t_b / scale;
+        c_ms += t_c / scale;
+    }
     // per-orientation averages of the sampled batches, scaled to the plane
     const int sampled = nbatch > 1 ? 2 : 1;
     c->last_total_ms = tot;
@@ -987,20 +993,16 @@ int tm_get_results(tm_ctx* c, float* mip, float* best_psi, float* best_theta, fl
     const size_t n = (size_t)c->X * c->Y;
     int rc = wait_stream(c, 3600.0);
     if (rc != TM_OK) return rc;
-    if (mip) TM_CUDA(c, cudaMemcpy(mip, c->mip, sizeof(float) * n, cudaMemcpyDeviceToHost));
-    if (sum) TM_CUDA(c, cudaMemcpy(sum, c->sum, sizeof(double) * n, cudaMemcpyDeviceToHost));
-    if (sum_of_squares) TM_CUDA(c, cudaMemcpy(sum_of_squares, c->sumsq, sizeof(double) * n, cudaMemcpyDeviceToHost));
-    if (histogram) {
-        std::vector<unsigned long long> h(c->d.histogram_bins);
-        TM_CUDA(c, cudaMemcpy(h.data(), c->hist, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost));
-        for (size_t i = 0; i < h.size(); i++) histogram[i] = (long long)h[i];
-    }
-    if (best_psi || best_theta || best_phi || best_defocus || best_pixel_size) {
+    // the best-orientation map first: host threads decode it while this
+    // thread copies the other maps
+    std::vector<std::thread> pool;
+    const bool want_angles = best_psi || best_theta || best_phi || best_defocus || best_pixel_size;
+    if (want_angles) {
         if (!c->best_host) TM_CUDA(c, cudaMallocHost((void**)&c->best_host, sizeof(int) * n));
-        const int* best = c->best_host;
         TM_CUDA(c, cudaMemcpy(c->best_host, c->best, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        const int* best = c->best_host;
         // decode global orientation indices into angles and plane offsets, in parallel
-        auto decode = [&](size_t i0, size_t i1) {
+        auto decode = [c, best, best_psi, best_theta, best_phi, best_defocus, best_pixel_size](size_t i0, size_t i1) {
             for (size_t i = i0; i < i1; i++) {
                 const int g = best[i];
                 float psi = 0, th = 0, ph = 0, df = 0, px = 0;
@@ -1029,15 +1031,29 @@ int tm_get_results(tm_ctx* c, float* mip, float* best_psi, float* best_theta, fl
         unsigned nt = std::thread::hardware_concurrency();
         nt = nt < 1 ? 1 : (nt > 32 ? 32 : nt);
         if (n < ((size_t)1 << 16)) nt = 1;
-        std::vector<std::thread> pool;
         const size_t chunk = (n + nt - 1) / nt;
-        for (unsigned k = 1; k < nt; k++) {
+        for (unsigned k = 0; k < nt; k++) {
             const size_t i0 = k * chunk, i1 = std::min(n, i0 + chunk);
             if (i0 < i1) pool.emplace_back(decode, i0, i1);
         }
-        decode(0, std::min(n, chunk));
-        for (auto& th : pool) th.join();
     }
+    auto join = [&pool] {
+        for (auto& th : pool) th.join();
+        pool.clear();
+    };
+    cudaError_t e = cudaSuccess;
+    if (mip && e == cudaSuccess) e = cudaMemcpy(mip, c->mip, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    if (sum && e == cudaSuccess) e = cudaMemcpy(sum, c->sum, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    if (sum_of_squares && e == cudaSuccess)
+        e = cudaMemcpy(sum_of_squares, c->sumsq, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    if (histogram && e == cudaSuccess) {
+        std::vector<unsigned long long> h(c->d.histogram_bins);
+        e = cudaMemcpy(h.data(), c->hist, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess)
+            for (size_t i = 0; i < h.size(); i++) histogram[i] = (long long)h[i];
+    }
+    join();
+    if (e != cudaSuccess) return set_err(c, TM_ERR_CUDA, "result copy: %s", cudaGetErrorString(e));
     return TM_OK;
 }
 
