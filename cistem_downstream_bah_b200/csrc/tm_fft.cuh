@@ -316,6 +316,9 @@ struct Twiddles {
 
 // Radix plan of an L-point transform with R values per thread: R while R
 // divides what is left, then the largest divisors of R that divide the rest.
+// Butterflies are at most radix 24: with R = 32 every stage is a divisor
+// (16, ...) and a thread does R / radix butterflies per stage.
+constexpr int kMaxRadix = 24;
 struct RadixSeq {
     int n;        // stages, -1 if L cannot be split this way
     int r[24];
@@ -323,12 +326,12 @@ struct RadixSeq {
 __host__ __device__ constexpr RadixSeq radix_seq(int L, int R) {
     RadixSeq q{0, {}};
     int m = L;
-    while (m > 1 && m % R == 0 && q.n < 24) {
+    while (R <= kMaxRadix && m > 1 && m % R == 0 && q.n < 24) {
         q.r[q.n++] = R;
         m /= R;
     }
     while (m > 1) {
-        int d = R;
+        int d = R > kMaxRadix ? kMaxRadix : R;
         while (d > 1 && !(R % d == 0 && m % d == 0)) d--;
         if (d <= 1 || q.n >= 24) return RadixSeq{-1, {}};
         q.r[q.n++] = d;

@@ -379,9 +379,13 @@ k_pass_a(BatchArgs a) {
 // zero-padded to L (L = T for power-of-two heights).
 template <int T, int Y>
 struct PassB {
-    static constexpr int V = col_radix(Y);                          // values per thread
+    // values per thread: the column radix.  (32 values -- two radix-16
+    // butterflies per thread and stage, 512 threads -- compiles and passes the
+    // same tests but measured no faster on 4096 x 4096.)
+    static constexpr int V = col_radix(Y);
     static constexpr int P = Y / V;                                 // threads per column
-    static constexpr int W = (16 * P <= 1024) ? 16 : (8 * P <= 1024) ? 8 : (4 * P <= 1024) ? 4 : 2;   // columns per block
+    // columns per block; 32 values per thread need 128 registers: 512 threads
+    static constexpr int W = V == 32 ? 4 : (16 * P <= 1024) ? 16 : (8 * P <= 1024) ? 8 : (4 * P <= 1024) ? 4 : 2;
     static constexpr int NT = W * P;                                // threads per block
     static constexpr int L = prune_len(T, Y, V);                    // pruned forward length
     static constexpr int MY = Y / L, PT = L / V;
@@ -409,7 +413,7 @@ struct PassB {
     static_assert(L > 0 && Y % V == 0 && P % PT == 0, "no pruned plan for this template and height");
     static_assert(NT <= 1024 && SMEM <= 232448, "pass B block exceeds the per-block limits");
     static_assert(TMEM_COLS <= 512, "pass B TMEM layout exceeds 512 columns");
-    static_assert(V == 16 || V == 18, "TMEM load sequence covers 16 or 18 values");
+    static_assert(V == 16 || V == 18 || V == 32, "TMEM load sequence covers 16, 18 or 32 values");
 };
 
 // I' values of one thread (V complex, 2V floats) into its TMEM columns
@@ -418,6 +422,10 @@ __device__ __forceinline__ void tmem_put_values(uint32_t taddr, const float* f) 
     tmptx::tmem_st16(taddr, f);
     tmptx::tmem_st16(taddr + 16, f + 16);
     if constexpr (V == 18) tmptx::tmem_st4(taddr + 32, f + 32);
+    if constexpr (V == 32) {
+        tmptx::tmem_st16(taddr + 32, f + 32);
+        tmptx::tmem_st16(taddr + 48, f + 48);
+    }
 }
 
 template <int T, int Y>
@@ -466,6 +474,7 @@ k_pass_b(BatchArgs a, int n_items) {
         const int group = it / a.nb, o = it % a.nb;
         const int kx0 = group * WG;
         // twiddles of the pruned forward, W_Y^(s * (tp + PT*r)) = w0 * w1^r, loaded early
+        // (with 32 values, from the table again every 8 values)
         const float2 w0 = a.twy.template w<-1>(s * tp, Y);
         const float2 w1 = a.twy.template w<-1>(s * PT, Y);
         // The buffer the next rows go into was last read at the start of the
@@ -512,6 +521,7 @@ k_pass_b(BatchArgs a, int n_items) {
                 float2 w = w0;
 #pragma unroll
                 for (int r = 0; r < V; r++) {
+                    if (V == 32 && r % 8 == 0 && r > 0) w = a.twy.template w<-1>(s * (tp + PT * r), Y);
                     const int n = tp + PT * r;   // rows n >= T of the L-point input are zero
                     v[r] = (L == T || n < T) ? cmul(acur[n * WG + col], w) : make_float2(0.f, 0.f);
                     w = cmul(w, w1);
@@ -530,11 +540,21 @@ k_pass_b(BatchArgs a, int n_items) {
 #pragma unroll
                 for (int r = 0; r < 8; r++) v[r] = cmul_conj(make_float2(iv[2 * r], iv[2 * r + 1]), v[r]);
                 tmptx::tmem_wait_ld();
+                if constexpr (V == 32) tmptx::tmem_ld16(tslot + 32, iv);
 #pragma unroll
                 for (int r = 0; r < 8; r++) v[8 + r] = cmul_conj(make_float2(iw[2 * r], iw[2 * r + 1]), v[8 + r]);
                 if constexpr (V == 18) {
                     v[16] = cmul_conj(make_float2(ix[0], ix[1]), v[16]);
                     v[17] = cmul_conj(make_float2(ix[2], ix[3]), v[17]);
+                }
+                if constexpr (V == 32) {
+                    tmptx::tmem_wait_ld16(iv);
+                    tmptx::tmem_ld16(tslot + 48, iw);
+#pragma unroll
+                    for (int r = 0; r < 8; r++) v[16 + r] = cmul_conj(make_float2(iv[2 * r], iv[2 * r + 1]), v[16 + r]);
+                    tmptx::tmem_wait_ld16(iw);
+#pragma unroll
+                    for (int r = 0; r < 8; r++) v[24 + r] = cmul_conj(make_float2(iw[2 * r], iw[2 * r + 1]), v[24 + r]);
                 }
             } else {
                 const float2* Ic = a.Ip + kx0 + col;

@@ -41,7 +41,8 @@ def test_small_geometry_search_parity(geom):
     _compare_search(case, batch=16, planes=((0.0, 0.0), (200.0, 0.0)))
 
 
-@pytest.mark.parametrize("geom", [(256, 4096, 3888), (256, 4096, 5832), (384, 4096, 5832), (384, 4096, 4096)])
+@pytest.mark.parametrize("geom", [(256, 4096, 3888), (256, 4096, 5832), (384, 4096, 5832), (384, 4096, 4096),
+                                  (256, 4096, 4096), (64, 4096, 4096)])
 def test_full_size_geometry_correlation_maps(geom):
     T, X, Y = geom
     case = make_case(T=T, X=X, Y=Y, pixel_size=1.0, n_particles=4, n_orient=40)

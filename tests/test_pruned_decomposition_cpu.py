@@ -16,13 +16,14 @@ import pytest
 
 
 def _plan(L, R):
-    """radix_seq of tm_fft.cuh: R while it divides, then the largest divisors of R."""
+    """radix_seq of tm_fft.cuh: R while it divides (butterflies of at most radix
+    24), then the largest divisors of R that divide the rest."""
     seq, m = [], L
-    while m > 1 and m % R == 0:
+    while R <= 24 and m > 1 and m % R == 0:
         seq.append(R)
         m //= R
     while m > 1:
-        d = R
+        d = min(R, 24)
         while d > 1 and not (R % d == 0 and m % d == 0):
             d -= 1
         if d <= 1:
@@ -40,7 +41,8 @@ def _prune_len(T, N, V):
 
 
 @pytest.mark.parametrize("T,N,V", [(256, 4096, 16), (384, 4096, 16), (256, 3888, 18), (256, 5832, 18),
-                                   (384, 5832, 18), (32, 288, 18), (48, 288, 18), (48, 256, 16)])
+                                   (384, 5832, 18), (32, 288, 18), (48, 288, 18), (48, 256, 16),
+                                   (256, 4096, 32), (384, 4096, 32), (64, 4096, 32)])
 def test_pruned_forward_equals_full_dft(T, N, V):
     rng = np.random.default_rng(T + N)
     a = rng.normal(size=T) + 1j * rng.normal(size=T)
@@ -66,7 +68,9 @@ def test_pruned_forward_equals_full_dft(T, N, V):
 
 @pytest.mark.parametrize("L,R,expect", [(4096, 16, [16, 16, 16]), (2048, 8, [8, 8, 8, 4]), (5832, 18, [18, 18, 18]),
                                         (3888, 18, [18, 18, 6, 2]), (324, 18, [18, 18]), (486, 18, [18, 9, 3]),
-                                        (384, 24, [24, 8, 2]), (192, 24, [24, 8]), (288, 18, [18, 2, 2, 2, 2])])
+                                        (384, 24, [24, 8, 2]), (192, 24, [24, 8]), (288, 18, [18, 2, 2, 2, 2]),
+                                        (4096, 32, [16, 16, 16]), (256, 32, [16, 16]), (512, 32, [16, 16, 2]),
+                                        (64, 32, [16, 4])])
 def test_radix_plans(L, R, expect):
     seq = _plan(L, R)
     assert seq == expect
@@ -156,7 +160,8 @@ def _kernel_fft(x, R, sign, lmax=None):
 @pytest.mark.parametrize("L,R,lmax", [(36, 18, 288), (288, 18, 288), (324, 18, 3888), (3888, 18, 3888),
                                       (5832, 18, 5832), (486, 18, 5832), (48, 24, 48), (24, 24, 48), (384, 24, 384),
                                       (192, 24, 384), (256, 16, 4096), (4096, 16, 4096), (2048, 8, 4096),
-                                      (64, 16, 256), (512, 16, 4096)])
+                                      (64, 16, 256), (512, 16, 4096), (4096, 32, 4096), (256, 32, 4096),
+                                      (512, 32, 4096), (64, 32, 4096)])
 def test_kernel_fft_addressing(L, R, lmax):
     rng = np.random.default_rng(L + R)
     x = rng.normal(size=L) + 1j * rng.normal(size=L)
