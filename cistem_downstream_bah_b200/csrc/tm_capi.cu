@@ -495,16 +495,16 @@ int template_on_device(cudaStream_t s, int nsm, const TemplateBuffers& b, float 
             }
         TW_CHECK(cudaMemcpyAsync(b.jobs, jobs.data(), sizeof(tmcg::GemmJob) * jobs.size(), cudaMemcpyHostToDevice, s));
         const int TT = T * T;
-        tmcg::k_gemm<<<dim3((T + 63) / 64, (TT + 63) / 64, 2), 256, 0, s>>>(b.jobs, TT, T, T, T, T, T, 0);
+        tmcg::k_gemm<<<dim3((T + 127) / 128, (TT + 127) / 128, 2), 256, 0, s>>>(b.jobs, TT, T, T, T, T, T, 0);
         TW_CHECK(cudaGetLastError());
         for (int pass = 0; pass < 4; pass++) {
-            tmcg::k_gemm<<<dim3((T + 63) / 64, (T + 63) / 64, T), 256, 0, s>>>(b.jobs + 4 + pass * T, T, T, T, T, T, T,
+            tmcg::k_gemm<<<dim3((T + 127) / 128, (T + 127) / 128, T), 256, 0, s>>>(b.jobs + 4 + pass * T, T, T, T, T, T, T,
                                                                               pass % 2);
             TW_CHECK(cudaGetLastError());
         }
-        tmcg::k_gemm<<<dim3((TT + 63) / 64, (T + 63) / 64, 1), 256, 0, s>>>(b.jobs + 2, T, TT, T, T, TT, TT, 0);
+        tmcg::k_gemm<<<dim3((TT + 127) / 128, (T + 127) / 128, 1), 256, 0, s>>>(b.jobs + 2, T, TT, T, T, TT, TT, 0);
         TW_CHECK(cudaGetLastError());
-        tmcg::k_gemm<<<dim3((TT + 63) / 64, (T + 63) / 64, 1), 256, 0, s>>>(b.jobs + 3, T, TT, T, T, TT, TT, 1);
+        tmcg::k_gemm<<<dim3((TT + 127) / 128, (T + 127) / 128, 1), 256, 0, s>>>(b.jobs + 3, T, TT, T, T, TT, TT, 1);
         TW_CHECK(cudaGetLastError());
         rows_src = out;
         add = padding_value;

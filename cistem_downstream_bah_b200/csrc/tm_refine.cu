@@ -427,14 +427,14 @@ int run_batch(tm_refine_ctx* c, int n, int n_jobs) {
                                                               1.0 / (double)c->disc_count);
         TR_LAUNCHED("k_disc_mean");
         // Z = (P - pv) [brt | bit]            (TP x 2T)
-        tmr::k_gemm<<<dim3((2 * T + 63) / 64, (TP + 63) / 64, n_jobs), 256, 0, s>>>(c->gjobs, TP, 2 * T, TP, TP,
+        tmr::k_gemm<<<dim3((2 * T + 127) / 128, (TP + 127) / 128, n_jobs), 256, 0, s>>>(c->gjobs, TP, 2 * T, TP, TP,
                                                                                     2 * T, 2 * T, 0);
         TR_LAUNCHED("k_gemm (1)");
         // Q = Ar Z[:, :T] + (-Ai) Z[:, T:]     (T x T)
-        tmr::k_gemm<<<dim3((T + 63) / 64, (T + 63) / 64, n_jobs), 256, 0, s>>>(c->gjobs + n_jobs, T, T, TP, 2 * TP,
+        tmr::k_gemm<<<dim3((T + 127) / 128, (T + 127) / 128, n_jobs), 256, 0, s>>>(c->gjobs + n_jobs, T, T, TP, 2 * TP,
                                                                               2 * T, T, 0);
         TR_LAUNCHED("k_gemm (2)");
-        tmr::k_gemm<<<dim3((T + 63) / 64, (T + 63) / 64, n_jobs), 256, 0, s>>>(c->gjobs + 2 * n_jobs, T, T, TP,
+        tmr::k_gemm<<<dim3((T + 127) / 128, (T + 127) / 128, n_jobs), 256, 0, s>>>(c->gjobs + 2 * n_jobs, T, T, TP,
                                                                               2 * TP, 2 * T, T, 1);
         TR_LAUNCHED("k_gemm (3)");
     }
