@@ -1,9 +1,11 @@
 // refine_template_main.cpp -- the refine_template program
 // (src/programs/refine_template/refine_template.cpp) on the B200 scoring core.
 //
-//   refine_template ARG0 ... ARG50
+//   refine_template                interactive prompts, as DoInteractiveUserInput
+//                                  (refine_template.cpp:93-258), read from stdin
+//   refine_template ARG0 ... ARG50  the 51 job arguments in the order
+//                                  DoCalculation reads them (:296-346)
 //
-// The 51 job arguments in the order DoCalculation reads them (:296-346).
 // The search maps of one result (argument 46 picks the slice) are read, the
 // micrograph whitened (:612-630), the peaks of the scaled MIP picked
 // (:503-553), and each peak refined by the reference's coordinate descent
@@ -11,8 +13,8 @@
 // (tm_refine_score); the refined MIP, scaled MIP and parameter maps are written
 // to arguments 29-35 with the pixel size set (:1140-1146).  max_threads
 // (argument 47) is the number of peaks refined at once -- the reference's
-// OpenMP threads -- and so the width of the GPU batches.  The interactive
-// prompts and the GUI result (arguments 48-50) are not provided.
+// OpenMP threads -- and so the width of the GPU batches.  The GUI result
+// (arguments 48-50) is not produced.
 #include <chrono>
 #include <cmath>
 #include <complex>
@@ -30,6 +32,7 @@
 #include "prep.hpp"
 #include "refine.hpp"
 #include "tm_b200.h"
+#include "user_input.hpp"
 
 using namespace tmhost;
 
@@ -107,6 +110,67 @@ bool parse(int argc, char** argv, RefineArgs& a) {
     a.threshold_for_result_plotting = F(49);
     a.filename_for_gui_result_image = S(50);
     return true;
+}
+
+// DoInteractiveUserInput (refine_template.cpp:140-258): the prompts, then the
+// job arguments as its ManualSetArguments fills them
+RefineArgs interactive() {
+    UserInput in;
+    RefineArgs a;
+    a.input_search_images = in.filename("Input images to be searched", "The input image stack, containing the images that should be searched", "image_stack.mrc", true);
+    a.input_reconstruction = in.filename("Input template reconstruction", "The 3D reconstruction from which projections are calculated", "reconstruction.mrc", true);
+    a.in_mip = in.filename("Input MIP file", "The file with the maximum intensity projection image", "mip.mrc", false);
+    a.in_scaled_mip = in.filename("Input scaled MIP file", "The file with the scaled MIP (peak search done on this image)", "scaled_mip.mrc", false);
+    a.in_psi = in.filename("Input psi file", "The file with the best psi image", "psi.mrc", true);
+    a.in_theta = in.filename("Input theta file", "The file with the best psi image", "theta.mrc", true);
+    a.in_phi = in.filename("Input phi file", "The file with the best psi image", "phi.mrc", true);
+    a.in_defocus = in.filename("Input defocus file", "The file with the best defocus image", "defocus.mrc", true);
+    a.in_pixel_size = in.filename("Input pixel size file", "The file with the best pixel size image", "pixel_size.mrc", true);
+    a.out_mip = in.filename("Output MIP file", "The file for saving the maximum intensity projection image", "out_mip.mrc", false);
+    a.out_scaled_mip = in.filename("Output Scaled MIP file", "The file for saving the maximum intensity projection image divided by correlation variance", "out_scaled_mip.mrc", false);
+    a.out_psi = in.filename("Output psi file", "The file for saving the best psi image", "out_psi.mrc", false);
+    a.out_theta = in.filename("Output theta file", "The file for saving the best psi image", "out_theta.mrc", false);
+    a.out_phi = in.filename("Output phi file", "The file for saving the best psi image", "out_phi.mrc", false);
+    a.out_defocus = in.filename("Output defocus file", "The file for saving the best defocus image", "out_defocus.mrc", false);
+    a.out_pixel_size = in.filename("Output pixel size file", "The file for saving the best pixel size image", "out_pixel_size.mrc", false);
+    RefineParams& p = a.p;
+    p.wanted_threshold = in.number("Peak threshold", "Peaks over this size will be taken", "7.5", 0.0f);
+    p.min_peak_radius = in.number("Min peak radius (px.)", "Essentially the minimum closeness for peaks", "10.0", 0.0f);
+    p.pixel_size = in.number("Pixel size of images (A)", "Pixel size of input images in Angstroms", "1.0", 0.0f);
+    p.voltage_kV = in.number("Beam energy (keV)", "The energy of the electron beam used to image the sample in kilo electron volts", "300.0", 0.0f);
+    p.spherical_aberration_mm = in.number("Spherical aberration (mm)", "Spherical aberration of the objective lens in millimeters", "2.7");
+    p.amplitude_contrast = in.number("Amplitude contrast", "Assumed amplitude contrast", "0.07", 0.0f, 1.0f);
+    p.defocus1 = in.number("Defocus1 (angstroms)", "Defocus1 for the input image", "10000", 0.0f);
+    p.defocus2 = in.number("Defocus2 (angstroms)", "Defocus2 for the input image", "10000", 0.0f);
+    p.defocus_angle = in.number("Defocus angle (degrees)", "Defocus Angle for the input image", "0.0");
+    p.phase_shift = in.number("Phase shift (degrees)", "Additional phase shift in degrees", "0.0");
+    p.angular_step = in.number("Out of plane angular step", "Angular step size for global grid search", "0.2", 0.01f);
+    p.in_plane_angular_step = in.number("In plane angular step", "Angular step size for in-plane rotations during the search", "0.1", 0.01f);
+    p.defocus_search_range = in.number("Defocus search range (A) (0.0 = no search)", "Search range (-value ... + value) around current defocus", "200.0", 0.0f);
+    p.defocus_search_step = in.number("Desired defocus accuracy (A)", "Accuracy to be achieved in defocus search", "10.0", 0.0f);
+    p.pixel_size_search_range = in.number("Pixel size search range (A) (0.0 = no search)", "Search range (-value ... + value) around current pixel size", "0.1", 0.0f);
+    p.pixel_size_search_step = in.number("Desired pixel size accuracy (A)", "Accuracy to be achieved in pixel size search", "0.01", 0.01f);
+    p.padding = in.number("Padding factor", "Factor determining how much the input volume is padded to improve projections", "2.0", 1.0f);
+    p.mask_radius = in.number("Mask radius (A) (0.0 = no mask)", "Radius of a circular mask to be applied to the input particles during refinement", "0.0", 0.0f);
+    p.xy_change_threshold = in.number("Moved peak warning (A)", "Threshold for displaying warning of peak location changes during refinement", "10.0", 0.0f);
+    p.exclude_above_xy_threshold = in.yes_no("Exclude moving peaks", "Should the peaks that move more than the threshold be excluded from the output MIPs?", "No");
+    a.result_number = (int)in.number("Result number to refine", "If input files contain results from several searches, which one should be refined?", "1", 1.0f);
+    p.max_threads = (int)in.number("Max. threads to use for calculation", "When threading, what is the max threads to run", "1", 1.0f);
+    // the values ManualSetArguments passes besides the answers (:189-258)
+    a.low_resolution_limit = 300.0f;
+    a.high_resolution_limit = 8.0f;
+    a.angular_range = 2.0f;
+    a.best_parameters_to_keep = 20;
+    a.ctf_refinement = false;
+    a.symmetry = "C1";
+    a.first_search_position = -1;
+    a.last_search_position = -1;
+    a.image_number_for_gui = 0;
+    a.number_of_jobs_per_image_in_gui = 0;
+    a.directory_for_results = "/dev/null";
+    a.threshold_for_result_plotting = 0.0f;
+    a.filename_for_gui_result_image = "";
+    return a;
 }
 
 std::vector<float> read_slice(const std::string& path, int slice, int* nx, int* ny) {
@@ -339,8 +403,13 @@ int run(const RefineArgs& a) {
 
 int main(int argc, char** argv) {
     RefineArgs a;
-    if (!parse(argc, argv, a)) {
-        std::fprintf(stderr, "usage: %s ARG0 ... ARG50  (the 51 refine_template job arguments)\n", argv[0]);
+    if (argc == 1) {
+        a = interactive();
+    } else if (!parse(argc, argv, a)) {
+        std::fprintf(stderr,
+                     "usage: %s                  (interactive)\n"
+                     "       %s ARG0 ... ARG50   (the 51 refine_template job arguments)\n",
+                     argv[0], argv[0]);
         return 2;
     }
     try {

@@ -136,5 +136,31 @@ def test_descent_matches_the_reference_loops(pixel_range, defocus_range):
 
 
 def test_refine_program_usage():
-    r = subprocess.run([H.REFINE_CLI_PATH], capture_output=True, text=True, timeout=30)
+    r = subprocess.run([H.REFINE_CLI_PATH, "only-one-argument"], capture_output=True, text=True, timeout=30)
     assert r.returncode == 2 and "ARG50" in r.stderr
+
+
+def test_refine_program_interactive_without_peaks(tmp_path):
+    """The prompts of DoInteractiveUserInput, scripted; no peak above the
+    threshold, so the program only reads, whitens and writes (no GPU)."""
+    rng = np.random.default_rng(9)
+    ny, nx, T = 120, 128, 16
+    H.write_mrc(tmp_path / "img.mrc", rng.normal(size=(ny, nx)).astype(np.float32), 1.5)
+    H.write_mrc(tmp_path / "tpl.mrc", rng.normal(size=(T, T, T)).astype(np.float32), 1.5)
+    maps = {}
+    for k in ("mip", "scaled", "psi", "theta", "phi", "defocus", "pixel"):
+        maps[k] = rng.normal(size=(ny, nx)).astype(np.float32) if k != "scaled" else np.zeros((ny, nx), np.float32)
+        H.write_mrc(tmp_path / f"in_{k}.mrc", maps[k], 1.5)
+    outs = [str(tmp_path / f"out_{k}.mrc") for k in ("mip", "scaled", "psi", "theta", "phi", "defocus", "pixel")]
+    answers = [str(tmp_path / "img.mrc"), str(tmp_path / "tpl.mrc")] + \
+        [str(tmp_path / f"in_{k}.mrc") for k in ("mip", "scaled", "psi", "theta", "phi", "defocus", "pixel")] + \
+        outs + ["7.5", "10", "1.5", "300", "2.7", "0.07", "10000", "10000", "0", "0", "0.2", "0.1", "200", "10",
+                "0.1", "0.01", "1.0", "0", "10", "no", "1", "2"]
+    r = subprocess.run([H.REFINE_CLI_PATH], input="\n".join(answers) + "\n", capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "Peak threshold" in r.stdout and "Refining 0 positions" in r.stdout
+    got = {k: H.read_mrc(o)[0][0] for k, o in zip(("mip", "scaled", "psi", "theta", "phi", "defocus", "pixel"), outs)}
+    assert not got["mip"].any() and not got["scaled"].any()
+    for k in ("psi", "theta", "phi", "defocus", "pixel"):
+        assert np.array_equal(got[k], maps[k]), k
