@@ -251,6 +251,13 @@ const Variant kVariants[] = {
     TM_VARIANT(256, 4096, 5832),
     TM_VARIANT(384, 4096, 4096),
     TM_VARIANT(384, 4096, 5832),
+    // the same camera formats with smaller and larger templates
+    TM_VARIANT(128, 4096, 4096),
+    TM_VARIANT(128, 4096, 3888),
+    TM_VARIANT(128, 4096, 5832),
+    TM_VARIANT(64, 4096, 3888),
+    TM_VARIANT(64, 4096, 5832),
+    TM_VARIANT(384, 4096, 3888),
 };
 
 const Variant* find_variant(int T, int X, int Y) {
