@@ -548,6 +548,96 @@ def run_refine(args, seed=20261215):
         dist.destroy_process_group()
 
 
+PROPOSAL_WEIGHTS = os.path.join(ROOT, "cistem_downstream_bah_b200", "data", "proposal_net.npz")
+
+
+def run_proposal(args):
+    """The learned proposal on the metric's configuration (4096^2, 256^3,
+    fine grid 2.5 / 1.5 deg): coarse search (7.5 / 5 deg) -> network over the
+    64 x 64 tiles -> window search of the proposed tiles over the fine
+    orientations of their 16 angular bins.  The exhaustive fine search runs
+    after it and judges recall of its z >= 7 peaks.  value = the exhaustive
+    search's points / the proposal path's time (host buffers in and out,
+    synchronous calls); the same for the method without the network
+    (thresholded coarse z, bins around the coarse best direction)."""
+    from cistem_downstream_bah_b200 import core, hostprep
+    from cistem_downstream_bah_b200 import proposal as PR
+    world, rank, local = dist_init(args)
+    w = np.load(args.proposal_weights)
+    params = w["params"]
+    net_thr = float(w["network_logit_threshold"])
+    heur_thr = float(w["heuristic_z_threshold"])
+    inp = make_inputs()
+    X, Y, T = inp["X"], inp["Y"], inp["T"]
+    angular = PR.AngularBins(7.5, WORKLOAD["angular_step"], WORKLOAD["psi_step"])
+    coarse_angles = core.orientation_list(hostprep.search_grid(7.5), 0.0, 5.0, 360.0)
+    sc = core.SearchCore(X, Y, T, histogram_min_scaled=inp["hmin"], histogram_step_scaled=inp["hstep"], device=local)
+    sc.set_image(inp["ispec"])
+    sc.set_template(inp["tspec"])
+    net = PR.ProposalNet(PR.FEATURES, PR.TILE, max_batch=256, device=local)
+    net.set_params(params)
+    ws = PR.WindowSearch(inp["ispec"], X, Y, T, inp["tspec"], inp["filt"], angular, inp["hmin"], inp["hstep"],
+                         device=local)
+    # warm-up: kernels of both geometries, the network
+    for _ in range(max(args.warmup, 1)):
+        PR.search_maps(sc, inp["filt"], coarse_angles[:256], X, Y)
+        ws.run(PR.Proposal([0], [angular.nearest([0.0, 0.0, 1.0], 1)], None))
+        net.forward(np.zeros((4, PR.FEATURES, PR.TILE, PR.TILE), np.float32))
+    barrier(world)
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        coarse = PR.search_maps(sc, inp["filt"], coarse_angles, X, Y)
+        t1 = time.perf_counter()
+        feats = PR.tile_features(coarse["z"], coarse["theta"], coarse["phi"])
+        prop = PR.propose_network(net, feats, X // PR.TILE, 1.0 / (1.0 + np.exp(-net_thr)), angular)
+        t2 = time.perf_counter()
+        res = ws.run(prop)
+        t3 = time.perf_counter()
+    t_prop = t3 - t0
+    heur = PR.propose_heuristic(coarse, heur_thr, angular)
+    t4 = time.perf_counter()
+    res_h = ws.run(heur)
+    t_heur = (t1 - t0) + (time.perf_counter() - t4)
+    exh = PR.search_maps(sc, inp["filt"], angular.fine_angles, X, Y)
+    peaks = PR.find_peaks(exh, 7.0, T, WORKLOAD["pixel_size"])
+    z_net = PR.proposal_z(res, coarse, X, Y)
+    z_heur = PR.proposal_z(res_h, coarse, X, Y)
+    rec_net = PR.recall(peaks, exh, res, z_net, 7.0)
+    rec_heur = PR.recall(peaks, exh, res_h, z_heur, 7.0)
+    sel = np.isfinite(res["mip"])
+    mip_err = float(np.max(np.abs(res["mip"][sel] - exh["mip"][sel]) / np.maximum(np.abs(exh["mip"][sel]), 1e-30))) \
+        if sel.any() else None
+    ws.close()
+    net.close()
+    sc.close()
+    pts_exh = exh["points"]
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": pts_exh / t_prop, "unit": UNIT, "n_gpus": world, "steps": 1,
+            "warmup": args.warmup, "ms_per_step": t_prop * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 search, bf16 network weights", "data": "synthetic",
+            "config": {"workload": "learned proposal: " + WORKLOAD["name"] + ", coarse 7.5/5.0 deg, 16 bins per tile",
+                       "flush_l2": "inputs > L2"},
+            "e2e": {"value": pts_exh / t_prop, "unit": UNIT, "h2d_bytes_per_step": int(inp["ispec"].nbytes),
+                    "d2h_bytes_per_step": int(6 * 4 * X * Y)},
+            "proposal": {
+                "exhaustive_points_per_s": pts_exh / exh["seconds"], "exhaustive_s": exh["seconds"],
+                "speedup_vs_exhaustive": exh["seconds"] / t_prop,
+                "coarse_s": t1 - t0, "network_s": t2 - t1, "windows_s": t3 - t2, "windows": res["windows"],
+                "tiles": int(len(prop.tiles)), "tiles_total": int(len(feats)),
+                "fine_points": res["points"], "exhaustive_points": pts_exh,
+                "z7_peaks": int(len(peaks)), "recall_mip": rec_net[0], "recall_z": rec_net[1],
+                "mip_max_rel_err_in_tiles": mip_err,
+                "without_network": {"tiles": int(len(heur.tiles)), "windows": res_h["windows"],
+                                    "s": t_heur, "speedup_vs_exhaustive": exh["seconds"] / t_heur,
+                                    "recall_mip": rec_heur[0], "recall_z": rec_heur[1]},
+                "network_logit_threshold": net_thr, "heuristic_z_threshold": heur_thr},
+            "gpu_launches": None, "clocks": clk.summary()}), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def _cpu_threads():
     """Host threads for the CPU legs (each thread holds ~0.6 GB of 4096^2 buffers)."""
     threads = min(os.cpu_count() or 1, 32)
@@ -602,11 +692,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--accuracy", type=int, default=4,
                     help="orientations compared with the FP64 oracle after timing, in the CPU-baseline leg (0 = skip)")
-    ap.add_argument("--workload", default="full", choices=sorted(WORKLOADS) + ["batched", "refine"],
+    ap.add_argument("--workload", default="full", choices=sorted(WORKLOADS) + ["batched", "refine", "proposal"],
                     help="full = the metric's 4096^2 configuration; the others are the uneven and stress geometries")
     ap.add_argument("--e2e-contexts", type=int, default=2,
                     help="host threads (each with its own search context) sharing the GPU in the e2e leg")
     ap.add_argument("--refine-batch", type=int, default=256, help="candidates per TemplateScore batch (--workload refine)")
+    ap.add_argument("--proposal-weights", default=PROPOSAL_WEIGHTS,
+                    help="trained proposal network (--workload proposal)")
     ap.add_argument("--traffic-b", type=float, default=None, help="ncu DRAM bytes per pass-B launch")
     ap.add_argument("--traffic-c", type=float, default=None, help="ncu DRAM bytes per pass-C launch")
     args = ap.parse_args()
@@ -620,6 +712,8 @@ def main():
         run_batched(args)
     elif args.workload == "refine":
         run_refine(args)
+    elif args.workload == "proposal":
+        run_proposal(args)
     else:
         run_ours(args)
 

@@ -62,7 +62,7 @@ def build_core(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(LIB_DIR, exist_ok=True)
     if force or _stale(CORE_LIB, _sources()):
         cmd = [_nvcc(), *NVCC_FLAGS, "-o", CORE_LIB, os.path.join(CSRC, "tm_capi.cu"), os.path.join(CSRC, "tm_noalloc.cu"),
-               os.path.join(CSRC, "tm_refine.cu")]
+               os.path.join(CSRC, "tm_refine.cu"), os.path.join(CSRC, "tm_proposal.cu")]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd), file=sys.stderr)

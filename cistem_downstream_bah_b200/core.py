@@ -33,7 +33,9 @@ EXPORTED = [
     "tm_last_error", "tm_version", "tm_run_plane_noalloc", "tm_autotune_batch", "tm_orientation_batch",
     "tm_refine_create", "tm_refine_set_particle", "tm_refine_set_filter", "tm_refine_set_operator",
     "tm_refine_score", "tm_refine_last_error", "tm_refine_destroy", "tm_set_micrograph", "tm_whiten_micrograph",
-    "tm_set_template_volume", "tm_template_spectrum",
+    "tm_set_template_volume", "tm_template_spectrum", "tm_set_normalization_pixels", "tm_pnet_create",
+    "tm_pnet_param_count", "tm_pnet_set_params", "tm_pnet_get_params", "tm_pnet_forward", "tm_pnet_gradients",
+    "tm_pnet_train_step", "tm_pnet_last_error", "tm_pnet_destroy",
 ]
 
 
@@ -103,6 +105,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.tm_whiten_micrograph.argtypes = [ip, vp, ip, ip, vp, vp, ip, ctypes.POINTER(ctypes.c_int)]
     L.tm_set_template_volume.argtypes = [vp, vp, ip, fp]
     L.tm_template_spectrum.argtypes = [ip, vp, ip, fp, vp]
+    L.tm_set_normalization_pixels.argtypes = [vp, ctypes.c_longlong]
     _LIB = L
     return L
 

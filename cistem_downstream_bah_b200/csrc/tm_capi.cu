@@ -68,6 +68,7 @@ struct tm_ctx {
     std::vector<std::vector<float>> angle_lists;
     long long next_gidx = 0;
     long long n_ccs = 0;
+    long long norm_pixels = 0;   // projection variance pixel count override (0: X*Y)
     double last_total_ms = 0, last_b_ms = 0, last_c_ms = 0, last_prep_ms = 0;
     std::string err;
 };
@@ -258,6 +259,10 @@ const Variant kVariants[] = {
     TM_VARIANT(64, 4096, 3888),
     TM_VARIANT(64, 4096, 5832),
     TM_VARIANT(384, 4096, 3888),
+    // windows of the learned proposal's fine search (edge max(2T, 256))
+    TM_VARIANT(64, 256, 256),
+    TM_VARIANT(128, 256, 256),
+    TM_VARIANT(256, 512, 512),
 };
 
 const Variant* find_variant(int T, int X, int Y) {
@@ -348,6 +353,7 @@ tmk::BatchArgs make_args(tm_ctx* c) {
     a.hist_inv_step = (float)(1.0 / c->d.histogram_step_scaled);
     a.hist_bins = c->d.histogram_bins;
     a.XP = c->XP;
+    a.norm_pixels = c->norm_pixels;
     a.err = c->err_flag;
     a.tw.tab = c->twx;
     a.tw.lmax = c->X;
@@ -882,6 +888,13 @@ int tm_template_spectrum(int device, const float* volume, int template_size, flo
     if (d_tw) cudaFree(d_tw);
     if (s) cudaStreamDestroy(s);
     return rc;
+}
+
+int tm_set_normalization_pixels(tm_ctx* c, long long n_pixels) {
+    if (!c) return TM_ERR_INVALID;
+    if (n_pixels < 0) return set_err(c, TM_ERR_INVALID, "normalisation pixel count %lld < 0", n_pixels);
+    c->norm_pixels = n_pixels;
+    return TM_OK;
 }
 
 int tm_reset_results(tm_ctx* c) {

@@ -77,6 +77,8 @@ struct BatchArgs {
     float hist_min, hist_inv_step;
     int hist_bins;
     int* err;                     // device error flag (a bounded wait ran out)
+    long long norm_pixels;        // pixel count of the projection variance (0: X*Y, the box;
+                                  // a window of a larger micrograph passes the micrograph's)
     int XP;                       // row pitch (complex values) of A, C and Ip: X/2+1 rounded
                                   // up to a multiple of the pass-B column chunk
     Twiddles tw;                  // x axis (passes A and C): every length divides X
@@ -765,7 +767,7 @@ struct Launch {
     static void prep(BatchArgs& a, cudaStream_t s) {
         k_slice_colfft<T><<<dim3((T / 2 + 1 + SC::CB - 1) / SC::CB, a.nb), SC::NT, 0, s>>>(a);
         k_row_c2r<T><<<dim3(T / RC::ROWS, a.nb), RC::NT, 0, s>>>(a);
-        k_norm<T><<<(a.nb + 7) / 8, 256, 0, s>>>(a, (long long)X * Y);
+        k_norm<T><<<(a.nb + 7) / 8, 256, 0, s>>>(a, a.norm_pixels > 0 ? a.norm_pixels : (long long)X * Y);
         k_pass_a<T, X><<<dim3(T, a.nb), X / 16, 0, s>>>(a);
     }
     static void pass_b(BatchArgs& a, cudaStream_t s, int nsm) {

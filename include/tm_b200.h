@@ -111,6 +111,13 @@ TM_API int tm_set_template_volume(tm_ctx *ctx, const float *volume, int template
 TM_API int tm_template_spectrum(int device, const float *volume, int template_size, float pixel_size_factor,
                                 float *spectrum);
 
+/* Pixel count that the projection variance is formed over (match_template.cpp:1066-1067
+ * use the padded micrograph's). 0, the default, is the context's X*Y. A context that
+ * searches a window cut from a larger whitened micrograph passes that micrograph's
+ * pixel count, so that its correlation values are the larger search's at the
+ * window's interior positions (the window search of the learned proposal). */
+TM_API int tm_set_normalization_pixels(tm_ctx *ctx, long long n_pixels);
+
 /* Clears the running MIP (to -FLT_MAX), best-orientation, sum, sum-of-squares
  * and histogram state, as RunInnerLoop does at entry (TemplateMatchingCore.cu:143-155). */
 TM_API int tm_reset_results(tm_ctx *ctx);
@@ -262,6 +269,38 @@ TM_API int tm_refine_score(tm_refine_ctx *ctx, int n, const float *euler, const 
 
 TM_API const char *tm_refine_last_error(const tm_refine_ctx *ctx);
 TM_API int tm_refine_destroy(tm_refine_ctx *ctx);
+
+/* ---- Learned proposal network (no reference counterpart) ----------------------------
+ * A 5-layer CNN over tile x tile patches of the coarse search's maps
+ * (in_channels planes per tile, [tile][channel][y][x]): three 3x3 conv + ReLU +
+ * 2x2 max-pool layers (32, 64, 128 channels), a 3x3 conv + ReLU (128) with a
+ * global max, and a fully connected layer to 4 outputs per tile: the
+ * objectness logit and a direction (x, y, z) whose nearest angular bins get the
+ * fine search.  FP32 master weights with Adam state; the forward and
+ * backward-data passes use their BF16 copies with FP32 accumulation.
+ * Parameter order: for each conv layer its weights [co][ci][3][3] then its
+ * bias, then the FC weights [4][128] and bias. */
+typedef struct tm_pnet tm_pnet;
+
+/* tile: 16, 32, 64 or 128; max_batch: tiles per call (1..4096). Parameters start at 0. */
+TM_API int tm_pnet_create(int device, int in_channels, int tile, int max_batch, tm_pnet **out);
+TM_API long long tm_pnet_param_count(const tm_pnet *net);
+/* FP32 master values (param_count floats); clears the Adam state */
+TM_API int tm_pnet_set_params(tm_pnet *net, const float *params);
+TM_API int tm_pnet_get_params(tm_pnet *net, float *params);
+/* outputs: 4 floats per tile (objectness logit, direction x, y, z) */
+TM_API int tm_pnet_forward(tm_pnet *net, const float *tiles, int n, float *outputs);
+/* labels: 4 floats per tile (objectness 0/1, unit target direction x, y, z).
+ * Loss L = 1/n sum_i [w_i BCE(o_i, y_i) + dir_weight y_i (1 - cos(d_i, t_i))],
+ * w_i = pos_weight for positives.  grads: param_count floats (dL/d of the BF16
+ * weights the forward used, and of the biases). */
+TM_API int tm_pnet_gradients(tm_pnet *net, const float *tiles, const float *labels, int n, float pos_weight,
+                             float dir_weight, double *loss, float *grads);
+/* One Adam step (beta 0.9, 0.999, eps 1e-8) at learning rate lr; loss may be null. */
+TM_API int tm_pnet_train_step(tm_pnet *net, const float *tiles, const float *labels, int n, float pos_weight,
+                              float dir_weight, float lr, double *loss);
+TM_API const char *tm_pnet_last_error(const tm_pnet *net);
+TM_API int tm_pnet_destroy(tm_pnet *net);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,135 @@
+"""Learned proposal on the CPU: the FP64 network oracle pinned by central
+differences, BF16 rounding, and the host logic (angular bins, tile features
+and labels, window spectra) that needs no GPU."""
+import numpy as np
+import pytest
+
+from cistem_downstream_bah_b200 import proposal as PR
+from oracle import proposal as OP
+
+
+def _params(cin, seed):
+    rng = np.random.default_rng(seed)
+    parts = []
+    for name, shape in OP.layout(cin):
+        n = int(np.prod(shape))
+        scale = np.sqrt(2.0 / np.prod(shape[1:])) if name.startswith("w") else 0.1
+        parts.append(rng.standard_normal(n) * scale)
+    return np.concatenate(parts)
+
+
+def test_layout_matches_host():
+    assert [(n, tuple(s)) for n, s in OP.layout(7)] == [(n, tuple(s)) for n, s in PR.param_layout(7)]
+    assert OP.param_count(7) == len(PR.init_params(7))
+    assert OP.param_count(7) == 242500
+
+
+@pytest.mark.parametrize("pos_weight,dir_weight", [(1.0, 1.0), (3.0, 0.25)])
+def test_oracle_gradients_central_differences(pos_weight, dir_weight):
+    cin = 3
+    p = _params(cin, 1)
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal((3, cin, 16, 16))
+    lab = np.array([[1, 0.6, 0.8, 0.0], [0, 0, 0, 0], [1, 0.0, 0.0, 1.0]])
+    loss, g = OP.gradients(p, x, lab, cin, pos_weight, dir_weight, bf16=False)
+    assert np.isclose(loss, OP.loss_only(p, x, lab, cin, pos_weight, dir_weight))
+    idx = np.concatenate([rng.choice(len(p), 30, replace=False), np.arange(len(p) - 516, len(p))[::37]])
+    h = 1e-6
+    for i in idx:
+        pp, pm = p.copy(), p.copy()
+        pp[i] += h
+        pm[i] -= h
+        fd = (OP.loss_only(pp, x, lab, cin, pos_weight, dir_weight) -
+              OP.loss_only(pm, x, lab, cin, pos_weight, dir_weight)) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 + 1e-5 * abs(fd), (i, fd, g[i])
+
+
+def test_bf16_rounding():
+    v = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -9, 1.0 + 2 ** -9, -2.5, 3.0e-3], np.float32)
+    r = OP.bf16_round(v)
+    assert r[0] == 1.0
+    assert r[1] == 1.0 + 2 ** -7 or r[1] == 1.0    # representable neighbours
+    assert r[3] == 1.0                              # tie to even
+    assert r[2] == 1.0 + 2 ** -7                    # above the tie rounds up
+    assert r[4] == -2.5
+    assert abs(r[5] - 3.0e-3) <= 3.0e-3 * 2 ** -8
+
+
+def test_angular_bins_partition_fine_grid():
+    ab = PR.AngularBins(15.0, 7.5, 10.0)
+    fd = PR.directions(ab.fine_grid[:, 0], ab.fine_grid[:, 1])
+    # every fine position's bin is a nearest coarse centre
+    s = fd @ ab.centers.T
+    assert np.all(s[np.arange(len(fd)), ab.bin_of_position] >= s.max(axis=1) - 1e-12)
+    rows = ab.orientations(range(ab.n_bins))
+    assert np.array_equal(rows, np.arange(len(ab.fine_angles)))
+    b = ab.nearest(ab.centers[5], 4)
+    assert b[0] == 5 and len(set(b)) == 4
+    rows = ab.orientations([b[1], b[0]])
+    assert np.all(np.diff(rows) > 0)
+    pos = np.unique(rows // ab.n_psi)
+    assert set(ab.bin_of_position[pos]) <= {b[0], b[1]}
+
+
+def test_tile_features_and_labels():
+    rng = np.random.default_rng(3)
+    z = rng.standard_normal((128, 192)).astype(np.float32)
+    th = rng.uniform(0, 180, z.shape).astype(np.float32)
+    ph = rng.uniform(0, 360, z.shape).astype(np.float32)
+    z[70, 100] = 9.0
+    f = PR.tile_features(z, th, ph)
+    assert f.shape == (6, PR.FEATURES, 64, 64)
+    t = 1 * 3 + 1   # tile row 1, column 1
+    assert np.isclose(f[t, 0, 70 - 64, 100 - 64], 9.0 / 4.0)
+    d = PR.directions(ph[70, 100], th[70, 100])
+    assert np.allclose(f[t, 4:7, 6, 36], d, atol=1e-6)
+    assert np.allclose(f[t, 1:4, 6, 36], d * 2.0, atol=1e-6)
+    peaks = np.array([[100, 70, 9.0, 30.0, 40.0, 0.0], [101, 71, 8.0, 0.0, 0.0, 0.0], [10, 10, 7.5, 0.0, 90.0, 0.0]])
+    lab = PR.tile_labels(peaks, 192, 128)
+    assert lab[:, 0].tolist() == [1, 0, 0, 0, 1, 0]
+    assert np.allclose(lab[4, 1:], PR.directions(30.0, 40.0))
+    for k in range(8):
+        a = PR.dihedral(f, k)
+        assert a.shape == f.shape
+        assert np.isclose(a[:, 0].max(), f[:, 0].max())
+
+
+def test_window_spectrum_reproduces_correlations():
+    """The window's spectrum gives the full image's circular correlation with
+    a T-support kernel at the window's interior positions (shifted by the
+    window origin), including windows that wrap around the image edge."""
+    rng = np.random.default_rng(4)
+    X = Y = 96
+    T, W = 16, 40
+    img = rng.standard_normal((Y, X))
+    spec = np.fft.rfft2(img) / (X * Y)
+    spec[0, 0] = 0
+    ky = np.arange(Y)[:, None]
+    kx = np.arange(X // 2 + 1)[None, :]
+    spec = spec * np.where(((ky + kx) & 1) == 1, -1.0, 1.0)
+    s = PR.whitened_real(spec.astype(np.complex64), X, Y)
+    assert np.allclose(s, img - img.mean(), atol=1e-4)
+    # round trip on the full box
+    assert np.allclose(PR.window_spectrum(s, 0, 0, X), spec, atol=1e-6)
+    ker = rng.standard_normal((T, T))
+
+    def corr(spec_swapped, n):
+        kyy = np.arange(n)[:, None]
+        kxx = np.arange(n // 2 + 1)[None, :]
+        unswapped = spec_swapped * np.where(((kyy + kxx) & 1) == 1, -1.0, 1.0)
+        kp = np.zeros((n, n))
+        kp[:T, :T] = ker
+        return np.fft.irfft2(unswapped * np.conj(np.fft.rfft2(kp)), s=(n, n)) * n * n
+
+    full = np.fft.irfft2(np.fft.rfft2(s) * np.conj(np.fft.rfft2(np.pad(ker, ((0, Y - T), (0, X - T))))), s=(Y, X))
+    for x0, y0 in [(10, 20), (-8, -8), (70, 80)]:
+        cw = corr(PR.window_spectrum(s, x0, y0, W), W)
+        for r in [(0, 0), (5, 7), (W - T, W - T)]:
+            ref = full[(y0 + r[0]) % Y, (x0 + r[1]) % X]
+            assert np.isclose(cw[r], ref, atol=1e-6), (x0, y0, r)
+
+
+def test_window_geometry():
+    for T in (64, 128, 256):
+        W = PR.window_size(T)
+        assert (W - T) % PR.TILE == 0 and W - T >= PR.TILE
