@@ -322,22 +322,38 @@ def whitened_real(ispec, X, Y):
     return np.fft.irfft2(ispec.astype(np.complex128) * sign, s=(Y, X)) * (X * Y)
 
 
-def window_spectrum(s, x0, y0, W):
-    """Half spectrum of the W x W window at (x0, y0) of the periodic image s,
-    with the forward 1/N and the quadrant swap of the window size; neither the
-    mean nor the norm is touched, so its correlations are the full image's."""
+def window_spectrum(s, x0, y0, W, n_full, used):
+    """Half spectrum of the W x W window at (x0, y0) of the periodic image s, as
+    the search context takes it for a window cut from a micrograph of n_full
+    pixels.  The context divides its image spectrum by its own pixel count and
+    drops the DC term (tm_set_image); so the forward transform is divided by
+    n_full, and the pixels outside the window's used square [used[0],
+    used[1])^2 -- pixels no interior correlation reads -- are set to the
+    constant that makes the window's mean zero, which leaves nothing for the
+    dropped DC term to remove.  The quadrant swap is that of the window size."""
     Y, X = s.shape
-    win = s[np.ix_((y0 + np.arange(W)) % Y, (x0 + np.arange(W)) % X)]
-    spec = np.fft.rfft2(win) / (W * W)
+    win = s[np.ix_((y0 + np.arange(W)) % Y, (x0 + np.arange(W)) % X)].copy()
+    lo, hi = used
+    inside = np.zeros((W, W), bool)
+    inside[lo:hi, lo:hi] = True
+    n_out = W * W - (hi - lo) ** 2
+    assert n_out > 0, "the window needs pixels outside its used square"
+    win[~inside] = -win[inside].sum() / n_out
+    spec = np.fft.rfft2(win) / n_full
     ky = np.arange(W)[:, None]
     kx = np.arange(W // 2 + 1)[None, :]
     return (spec * np.where(((ky + kx) & 1) == 1, -1.0, 1.0)).astype(np.complex64)
 
 
 def window_size(T):
-    """Window edge for a template box: 2T (at least 256); its interior (W - T)
-    holds whole tiles."""
+    """Window edge for a template box: 2T, at least 256."""
     return max(2 * T, 256)
+
+
+def window_core(T):
+    """Edge of the window's interior (whole tiles): the window less the template
+    box and a band of one tile that no interior correlation reads."""
+    return window_size(T) - T - TILE
 
 
 class WindowSearch:
@@ -346,8 +362,9 @@ class WindowSearch:
     def __init__(self, ispec, X, Y, T, tspec, filt, angular, hmin, hstep, device=0):
         self.X, self.Y, self.T = X, Y, T
         self.W = window_size(T)
-        self.core = self.W - T
-        assert self.core % TILE == 0
+        self.core = window_core(T)
+        assert self.core % TILE == 0 and self.core >= TILE
+        self.margin = (self.W - self.core - T) // 2   # unread pixels on each side of the used square
         self.s = whitened_real(ispec, X, Y)
         self.filt = filt
         self.angular = angular
@@ -376,8 +393,10 @@ class WindowSearch:
                 bins.update(int(v) for v in b)
             rows = self.angular.orientations(sorted(bins))
             angles = self.angular.fine_angles[rows]
-            x0, y0 = cx * C - T // 2, cy * C - T // 2
-            self.sc.set_image(window_spectrum(self.s, x0, y0, W))
+            m = self.margin
+            x0, y0 = cx * C - T // 2 - m, cy * C - T // 2 - m
+            # the used square keeps two pixels beyond the interior's reach on each side
+            self.sc.set_image(window_spectrum(self.s, x0, y0, W, X * Y, (m - 2, W - m + 2)))
             self.sc.reset()
             self.sc.run_plane(self.filt, angles)
             r = self.sc.results()

@@ -95,12 +95,15 @@ def test_tile_features_and_labels():
 
 
 def test_window_spectrum_reproduces_correlations():
-    """The window's spectrum gives the full image's circular correlation with
-    a T-support kernel at the window's interior positions (shifted by the
-    window origin), including windows that wrap around the image edge."""
+    """With the search context's conventions (image spectrum divided by its own
+    pixel count, DC term dropped), the window's spectrum gives the full
+    image's correlation with a T-support kernel at the window's interior
+    positions (shifted by the window origin), also for windows that wrap
+    around the image edge."""
     rng = np.random.default_rng(4)
     X = Y = 96
-    T, W = 16, 40
+    T, W = 16, 48
+    lo, hi = 4, 44
     img = rng.standard_normal((Y, X))
     spec = np.fft.rfft2(img) / (X * Y)
     spec[0, 0] = 0
@@ -109,27 +112,32 @@ def test_window_spectrum_reproduces_correlations():
     spec = spec * np.where(((ky + kx) & 1) == 1, -1.0, 1.0)
     s = PR.whitened_real(spec.astype(np.complex64), X, Y)
     assert np.allclose(s, img - img.mean(), atol=1e-4)
-    # round trip on the full box
-    assert np.allclose(PR.window_spectrum(s, 0, 0, X), spec, atol=1e-6)
     ker = rng.standard_normal((T, T))
 
-    def corr(spec_swapped, n):
+    def context_corr(spec_swapped, n, n_pixels):
         kyy = np.arange(n)[:, None]
         kxx = np.arange(n // 2 + 1)[None, :]
-        unswapped = spec_swapped * np.where(((kyy + kxx) & 1) == 1, -1.0, 1.0)
+        ip = spec_swapped * np.where(((kyy + kxx) & 1) == 1, -1.0, 1.0) / n_pixels
+        ip[0, 0] = 0
         kp = np.zeros((n, n))
         kp[:T, :T] = ker
-        return np.fft.irfft2(unswapped * np.conj(np.fft.rfft2(kp)), s=(n, n)) * n * n
+        return np.fft.irfft2(ip * np.conj(np.fft.rfft2(kp)), s=(n, n)) * n * n
 
-    full = np.fft.irfft2(np.fft.rfft2(s) * np.conj(np.fft.rfft2(np.pad(ker, ((0, Y - T), (0, X - T))))), s=(Y, X))
+    full = context_corr(spec, X, X * Y)
     for x0, y0 in [(10, 20), (-8, -8), (70, 80)]:
-        cw = corr(PR.window_spectrum(s, x0, y0, W), W)
-        for r in [(0, 0), (5, 7), (W - T, W - T)]:
+        ws = PR.window_spectrum(s, x0, y0, W, X * Y, (lo, hi))
+        cw = context_corr(ws, W, W * W)
+        for r in [(lo, lo), (lo + 5, lo + 7), (hi - T, hi - T), (lo, hi - T)]:
             ref = full[(y0 + r[0]) % Y, (x0 + r[1]) % X]
-            assert np.isclose(cw[r], ref, atol=1e-6), (x0, y0, r)
+            assert np.isclose(cw[r], ref, rtol=1e-5, atol=1e-9), (x0, y0, r, cw[r], ref)
+    # a window over the whole image with nothing outside its used square is refused
+    with pytest.raises(AssertionError):
+        PR.window_spectrum(s, 0, 0, X, X * Y, (0, X))
 
 
 def test_window_geometry():
     for T in (64, 128, 256):
-        W = PR.window_size(T)
-        assert (W - T) % PR.TILE == 0 and W - T >= PR.TILE
+        W, C = PR.window_size(T), PR.window_core(T)
+        assert C % PR.TILE == 0 and C >= PR.TILE
+        m = (W - C - T) // 2
+        assert m >= 8 and 2 * m + C + T == W
