@@ -588,25 +588,56 @@ def run_proposal(args):
         t0 = time.perf_counter()
         coarse = PR.search_maps(sc, inp["filt"], coarse_angles, X, Y)
         t1 = time.perf_counter()
-        feats = PR.tile_features(coarse["z"], coarse["theta"], coarse["phi"])
-        prop = PR.propose_network(net, feats, X // PR.TILE, 1.0 / (1.0 + np.exp(-net_thr)), angular)
+        frames = PR.tile_frames(coarse["z"], coarse["theta"], coarse["phi"])
+        feats = PR.tile_features(coarse["z"], coarse["theta"], coarse["phi"], frames=frames)
+        out = net.forward(feats)
+        prop = PR.propose_network(net, feats, frames, net_thr, angular, out=out)
+        if len(prop.tiles) > args.proposal_max_tiles:   # bound the run: keep the best-scored tiles
+            keep = np.sort(np.argsort(-out[prop.tiles, 0], kind="stable")[:args.proposal_max_tiles])
+            prop = PR.Proposal(prop.tiles[keep], [prop.bins[i] for i in keep], prop.scores)
         t2 = time.perf_counter()
         res = ws.run(prop)
         t3 = time.perf_counter()
     t_prop = t3 - t0
-    heur = PR.propose_heuristic(coarse, heur_thr, angular)
+    # the method without the network at the network's tile budget (timed the same way)
     t4 = time.perf_counter()
-    res_h = ws.run(heur)
-    t_heur = (t1 - t0) + (time.perf_counter() - t4)
+    top = PR.propose_top_tiles(coarse, len(prop.tiles), angular)
+    res_t = ws.run(top)
+    t_top = (t1 - t0) + (time.perf_counter() - t4)
+    # ... and with its own threshold (recall from the proposed bins; not searched)
+    heur = PR.propose_heuristic(coarse, heur_thr, angular)
     exh = PR.search_maps(sc, inp["filt"], angular.fine_angles, X, Y)
-    peaks = PR.find_peaks(exh, 7.0, T, WORKLOAD["pixel_size"])
-    z_net = PR.proposal_z(res, coarse, X, Y)
-    z_heur = PR.proposal_z(res_h, coarse, X, Y)
-    rec_net = PR.recall(peaks, exh, res, z_net, 7.0)
-    rec_heur = PR.recall(peaks, exh, res_h, z_heur, 7.0)
-    sel = np.isfinite(res["mip"])
-    mip_err = float(np.max(np.abs(res["mip"][sel] - exh["mip"][sel]) / np.maximum(np.abs(exh["mip"][sel]), 1e-30))) \
-        if sel.any() else None
+    peak_sets = {"min_radius_T8": PR.find_peaks(exh, 7.0, T, WORKLOAD["pixel_size"]),
+                 "min_radius_particle": PR.find_peaks(exh, 7.0, T, WORKLOAD["pixel_size"],
+                                                      min_peak_radius=int(WORKLOAD["radius_A"] / WORKLOAD["pixel_size"]))}
+    recalls, diags = {}, {}
+    for key, pk in peak_sets.items():
+        rn = PR.recall(pk, exh, res, PR.proposal_z(res, coarse, X, Y), 7.0)
+        rt = PR.recall(pk, exh, res_t, PR.proposal_z(res_t, coarse, X, Y), 7.0)
+        allnet = PR.propose_network(net, feats, frames, -np.inf, angular, out=out)
+        alltop = PR.propose_heuristic(coarse, -np.inf, angular)
+        dg = PR.peak_diagnostics(pk, exh, coarse, {"network": prop, "top_tiles": top, "threshold": heur,
+                                                   "network_all": allnet, "coarse_all": alltop}, angular)
+        diags[key] = dg
+        ptiles = [(int(p[1]) // PR.TILE) * (X // PR.TILE) + int(p[0]) // PR.TILE for p in pk]
+        curves = {"network": PR.tiles_for_recall(ptiles, dg["network_all_recovered"],
+                                                 np.argsort(-out[:, 0], kind="stable")),
+                  "coarse_z": PR.tiles_for_recall(ptiles, dg["coarse_all_recovered"],
+                                                  np.argsort(-PR.tile_max(coarse["z"])[0], kind="stable"))}
+        recalls[key] = {"z7_peaks": int(len(pk)), "network_recall_mip": rn[0], "network_recall_z": rn[1],
+                        "top_tiles_recall_mip": rt[0], "top_tiles_recall_z": rt[1],
+                        "threshold_recall_mip_from_bins": float(np.mean(dg["threshold_recovered"])) if len(pk) else 1.0,
+                        "network_missed_tile_not_selected": int(np.sum(~dg["network_selected"])),
+                        "network_missed_bin_not_proposed": int(np.sum(dg["network_selected"] & (dg["network_bin_rank"] < 0))),
+                        "bin_outside_16_nearest_at_peak": int(np.sum(dg["bin_rank_at_peak_coarse_direction"] >= 16)),
+                        "tiles_for_recall": curves}
+    # MIP error where the window search found the exhaustive search's best orientation
+    same = np.isfinite(res["mip"]) & (res["psi"] == exh["psi"]) & (res["theta"] == exh["theta"]) & (res["phi"] == exh["phi"])
+    mip_err = float(np.max(np.abs(res["mip"][same] - exh["mip"][same]) / np.maximum(np.abs(exh["mip"][same]), 1e-30))) \
+        if same.any() else None
+    if args.proposal_diag:
+        flat = {f"{k}:{n}": v for k, d in diags.items() for n, v in d.items()}
+        np.savez(args.proposal_diag, **flat)
     ws.close()
     net.close()
     sc.close()
@@ -625,13 +656,12 @@ def run_proposal(args):
                 "speedup_vs_exhaustive": exh["seconds"] / t_prop,
                 "coarse_s": t1 - t0, "network_s": t2 - t1, "windows_s": t3 - t2, "windows": res["windows"],
                 "tiles": int(len(prop.tiles)), "tiles_total": int(len(feats)),
-                "fine_points": res["points"], "exhaustive_points": pts_exh,
-                "z7_peaks": int(len(peaks)), "recall_mip": rec_net[0], "recall_z": rec_net[1],
-                "mip_max_rel_err_in_tiles": mip_err,
-                "without_network": {"tiles": int(len(heur.tiles)), "windows": res_h["windows"],
-                                    "s": t_heur, "speedup_vs_exhaustive": exh["seconds"] / t_heur,
-                                    "recall_mip": rec_heur[0], "recall_z": rec_heur[1]},
-                "network_logit_threshold": net_thr, "heuristic_z_threshold": heur_thr},
+                "fine_points": res["points"], "exhaustive_points": pts_exh, "recall": recalls,
+                "mip_max_rel_err_same_orientation": mip_err,
+                "without_network_same_tiles": {"tiles": int(len(top.tiles)), "windows": res_t["windows"], "s": t_top,
+                                               "speedup_vs_exhaustive": exh["seconds"] / t_top},
+                "without_network_threshold": {"tiles": int(len(heur.tiles)), "z_threshold": heur_thr},
+                "network_logit_threshold": net_thr},
             "gpu_launches": None, "clocks": clk.summary()}), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -699,6 +729,9 @@ def main():
     ap.add_argument("--refine-batch", type=int, default=256, help="candidates per TemplateScore batch (--workload refine)")
     ap.add_argument("--proposal-weights", default=PROPOSAL_WEIGHTS,
                     help="trained proposal network (--workload proposal)")
+    ap.add_argument("--proposal-max-tiles", type=int, default=512,
+                    help="most tiles the proposal's window search takes (--workload proposal)")
+    ap.add_argument("--proposal-diag", default=None, help="npz of per-peak diagnostics (--workload proposal)")
     ap.add_argument("--traffic-b", type=float, default=None, help="ncu DRAM bytes per pass-B launch")
     ap.add_argument("--traffic-c", type=float, default=None, help="ncu DRAM bytes per pass-C launch")
     args = ap.parse_args()

@@ -213,17 +213,60 @@ def tile_grid(nx, ny, tile=TILE):
     return ny // tile, nx // tile
 
 
-def tile_features(z, theta, phi, tile=TILE):
-    """(n_tiles, FEATURES, tile, tile) float32 from coarse maps: clipped z / 4,
-    the best direction weighted by clip(z - 3, 0, 9) / 3, and the direction."""
+def frame(d):
+    """Rotation taking the unit vector d to +z (Rodrigues' formula; the turn
+    about x for d = -z)."""
+    d = np.asarray(d, np.float64)
+    d = d / np.linalg.norm(d)
+    z = np.array([0.0, 0.0, 1.0])
+    v = np.cross(d, z)
+    c = float(d @ z)
+    if c < -1.0 + 1e-12:
+        return np.diag([1.0, -1.0, -1.0])
+    k = np.array([[0.0, -v[2], v[1]], [v[2], 0.0, -v[0]], [-v[1], v[0], 0.0]])
+    return np.eye(3) + k + k @ k / (1.0 + c)
+
+
+def tile_frames(z, theta, phi, tile=TILE):
+    """(n_tiles, 3, 3): per tile, the rotation taking the coarse best direction
+    at the tile's z-score maximum to +z."""
     ny, nx = z.shape
     gy, gx = tile_grid(nx, ny, tile)
+    _, arg = tile_max(z, tile)
+    out = np.zeros((gy * gx, 3, 3))
+    for i in range(gy * gx):
+        ty, tx = divmod(i, gx)
+        y = ty * tile + arg[i] // tile
+        x = tx * tile + arg[i] % tile
+        out[i] = frame(directions(phi[y, x], theta[y, x]))
+    return out
+
+
+def tile_features(z, theta, phi, tile=TILE, frames=None):
+    """(n_tiles, FEATURES, tile, tile) float32 from coarse maps: clipped z / 4,
+    the best direction weighted by clip(z - 3, 0, 9) / 3, and the direction,
+    both directions in the tile's frame (tile_frames), so that the coarse best
+    direction at the tile's maximum reads (0, 0, 1)."""
+    ny, nx = z.shape
+    gy, gx = tile_grid(nx, ny, tile)
+    if frames is None:
+        frames = tile_frames(z, theta, phi, tile)
     zc = np.clip(z[:gy * tile, :gx * tile], -4.0, 12.0)
     d = directions(phi[:gy * tile, :gx * tile], theta[:gy * tile, :gx * tile])
+    d = d.reshape(gy, tile, gx, tile, 3).transpose(0, 2, 1, 3, 4).reshape(gy * gx, tile * tile, 3)
+    d = np.einsum("nij,npj->npi", frames, d)
     w = np.clip(zc - 3.0, 0.0, 9.0) / 3.0
-    f = np.concatenate([(zc / 4.0)[..., None], d * w[..., None], d], axis=-1).astype(np.float32)   # (H, W, 7)
-    f = f.reshape(gy, tile, gx, tile, FEATURES).transpose(0, 2, 4, 1, 3).reshape(gy * gx, FEATURES, tile, tile)
-    return np.ascontiguousarray(f)
+    w = w.reshape(gy, tile, gx, tile).transpose(0, 2, 1, 3).reshape(gy * gx, tile * tile, 1)
+    zt = (zc / 4.0).reshape(gy, tile, gx, tile).transpose(0, 2, 1, 3).reshape(gy * gx, tile * tile, 1)
+    f = np.concatenate([zt, d * w, d], axis=-1).astype(np.float32)          # (n, tile*tile, 7)
+    return np.ascontiguousarray(f.transpose(0, 2, 1).reshape(gy * gx, FEATURES, tile, tile))
+
+
+def to_frames(labels, frames):
+    """Labels with their target directions in the tiles' frames."""
+    out = np.array(labels, np.float32, copy=True)
+    out[:, 1:4] = np.einsum("nij,nj->ni", frames, labels[:, 1:4])
+    return out
 
 
 def find_peaks(maps, threshold, T, pixel_size=1.0, min_peak_radius=None):
@@ -280,11 +323,36 @@ class Proposal:
         self.scores = scores
 
 
-def propose_network(net, feats, gx, threshold, angular, k=BINS_PER_TILE):
-    out = net.forward(feats)
-    prob = 1.0 / (1.0 + np.exp(-out[:, 0].astype(np.float64)))
-    sel = np.flatnonzero(prob >= threshold)
-    return Proposal(sel, [angular.nearest(out[i, 1:4], k) for i in sel], prob)
+def network_directions(out, frames):
+    """The network's directions rotated back out of the tiles' frames."""
+    return np.einsum("nji,nj->ni", frames, out[:, 1:4].astype(np.float64))
+
+
+def propose_network(net, feats, frames, logit_threshold, angular, k=BINS_PER_TILE, out=None):
+    """Tiles whose objectness logit reaches the threshold, with the k bins
+    nearest to the network's direction."""
+    if out is None:
+        out = net.forward(feats)
+    d = network_directions(out, frames)
+    sel = np.flatnonzero(out[:, 0] >= logit_threshold)
+    return Proposal(sel, [angular.nearest(d[i], k) for i in sel], out[:, 0])
+
+
+def tiles_for_recall(peak_tiles, recoverable, ranking, levels=(0.9, 0.95, 0.99, 1.0)):
+    """Tiles taken in ranking order until a share of the peaks is recovered
+    (a peak counts once its tile is taken, if its bin is among that tile's);
+    None where the share cannot be reached."""
+    pos = np.empty(len(ranking), np.int64)
+    pos[np.asarray(ranking)] = np.arange(len(ranking))
+    need = np.sort(np.where(recoverable, pos[np.asarray(peak_tiles, np.int64)] + 1, np.iinfo(np.int64).max))
+    out = {}
+    for q in levels:
+        if len(need) == 0:
+            out[str(q)] = 0
+            continue
+        k = int(np.ceil(q * len(need))) - 1
+        out[str(q)] = None if need[k] == np.iinfo(np.int64).max else int(need[k])
+    return out
 
 
 def tile_max(z, tile=TILE):
@@ -441,3 +509,59 @@ def recall(peaks, exhaustive, window_result, z_prop, threshold, radius=1, rel_to
         hit_m += got >= ref - rel_tol * abs(ref)
         hit_z += float(np.max(z_prop[ys, xs])) >= threshold
     return hit_m / len(peaks), hit_z / len(peaks)
+
+
+def propose_top_tiles(coarse, n_tiles, angular, k=BINS_PER_TILE, tile=TILE):
+    """The method without the network at a given tile budget: the n_tiles tiles
+    with the highest coarse z-score maximum, bins nearest to the coarse best
+    direction there."""
+    zmax, _ = tile_max(coarse["z"], tile)
+    order = np.argsort(-zmax, kind="stable")[:n_tiles]
+    thr = float(zmax[order[-1]]) if len(order) else np.inf
+    p = propose_heuristic(coarse, thr, angular, k, tile)
+    keep = np.isin(p.tiles, order)
+    return Proposal(p.tiles[keep], [b for b, kk in zip(p.bins, keep) if kk], zmax)
+
+
+def peak_diagnostics(peaks, exhaustive, coarse, proposals, angular, tile=TILE):
+    """Per exhaustive peak: its z, the distance to the nearest higher peak, the
+    angular bin of its best orientation, and for each proposal whether its tile
+    was selected, the rank of that bin among the tile's proposed bins (-1: not
+    proposed) and whether the proposal recovers the peak (tile selected, bin
+    proposed: the window search then evaluates the exhaustive search's own best
+    orientation there).  Also the rank of the bin around the coarse best
+    direction at the peak pixel itself."""
+    Y, X = coarse["z"].shape
+    gx = X // tile
+    n = len(peaks)
+    out = {"z": np.array([p[2] for p in peaks]), "x": np.array([p[0] for p in peaks]),
+           "y": np.array([p[1] for p in peaks])}
+    d_near = np.full(n, np.inf)
+    for i in range(n):
+        for j in range(n):
+            if peaks[j][2] > peaks[i][2]:
+                d_near[i] = min(d_near[i], float(np.hypot(peaks[i][0] - peaks[j][0], peaks[i][1] - peaks[j][1])))
+    out["dist_to_higher_peak"] = d_near
+    bins = np.array([int(np.argmax(angular.centers @ directions(p[3], p[4]))) for p in peaks], np.int64)
+    out["bin"] = bins
+    rank_here = []
+    for p, b in zip(peaks, bins):
+        x, y = int(p[0]), int(p[1])
+        order = angular.nearest(directions(coarse["phi"][y, x], coarse["theta"][y, x]), angular.n_bins)
+        rank_here.append(int(np.flatnonzero(order == b)[0]))
+    out["bin_rank_at_peak_coarse_direction"] = np.array(rank_here)
+    for name, prop in proposals.items():
+        where = {int(t): i for i, t in enumerate(prop.tiles)}
+        sel = np.zeros(n, bool)
+        rank = np.full(n, -1)
+        for i, (p, b) in enumerate(zip(peaks, bins)):
+            t = (int(p[1]) // tile) * gx + int(p[0]) // tile
+            if t in where:
+                sel[i] = True
+                pb = np.asarray(prop.bins[where[t]])
+                hit = np.flatnonzero(pb == b)
+                rank[i] = int(hit[0]) if len(hit) else -1
+        out[name + "_selected"] = sel
+        out[name + "_bin_rank"] = rank
+        out[name + "_recovered"] = sel & (rank >= 0)
+    return out

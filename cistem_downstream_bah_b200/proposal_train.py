@@ -7,12 +7,13 @@ Gaussian-atom template (box 64 or 128, defocus 5,000-25,000 A, per-particle SNR
 0.02-0.08).  Per case the search runs twice on the GPU: the coarse grid
 (7.5 / 5 degrees), whose z-score and best-orientation maps are the network's
 input, and the exhaustive fine grid (2.5 / 1.5 degrees), whose z >= 7 peaks are
-its labels.  Cases are split into training and held-out sets; the network is
+its labels.  Cases are split into training, validation and held-out sets; the network is
 trained with Adam on balanced batches (positives drawn with replacement under
-the 8 rotations/flips of the tile); the objectness threshold is set on the
-training positives, and the held-out cases measure recall and searched points
-against the exhaustive search, beside the method without the network
-(thresholded coarse z, bins around the coarse best direction).
+the 8 rotations/flips of the tile); the objectness threshold keeps a set
+share of the training and validation positives (less a margin), and the held-out cases
+measure recall and searched points against the exhaustive search, beside the
+method without the network (tiles by coarse z -- at its own threshold and at
+the network's tile count -- with bins around the coarse best direction).
 """
 from __future__ import annotations
 
@@ -61,8 +62,10 @@ def search_case(c, angular, coarse_angles, device=0, keep_maps=False):
     finally:
         sc.close()
     peaks = PR.find_peaks(fine, Z_THRESHOLD, T, px)
-    out = dict(case=c, feats=PR.tile_features(coarse["z"], coarse["theta"], coarse["phi"]),
-               labels=PR.tile_labels(peaks, N, N), peaks=peaks,
+    frames = PR.tile_frames(coarse["z"], coarse["theta"], coarse["phi"])
+    labels = PR.tile_labels(peaks, N, N)
+    out = dict(case=c, feats=PR.tile_features(coarse["z"], coarse["theta"], coarse["phi"], frames=frames),
+               frames=frames, labels=labels, labels_local=PR.to_frames(labels, frames), peaks=peaks,
                coarse_tile_max=PR.tile_max(coarse["z"])[0], seconds=(coarse["seconds"], fine["seconds"]))
     if keep_maps:
         out.update(coarse=coarse, fine=fine, ispec=ispec, tspec=tspec, filt=filt, hmin=hmin, hstep=hstep)
@@ -95,10 +98,12 @@ def train(feats, labels, steps=1500, batch=128, lr=1e-3, seed=0, dir_weight=1.0,
     return params, np.array(curve)
 
 
-def threshold_for(scores, labels, margin):
-    """Largest threshold that keeps every positive, lowered by the margin."""
-    pos = scores[labels[:, 0] > 0.5]
-    return float(pos.min() - margin) if len(pos) else float("inf")
+def threshold_for(scores, labels, margin, keep=1.0):
+    """Threshold that keeps the share `keep` of the positives, lowered by the margin."""
+    pos = np.sort(scores[labels[:, 0] > 0.5])
+    if not len(pos):
+        return float("inf")
+    return float(pos[int(np.floor((1.0 - keep) * (len(pos) - 1)))] - margin)
 
 
 def network_scores(params, feats, device=0):
@@ -120,16 +125,25 @@ def bins_hit(angular, bins, label_dir):
 def evaluate(cases, params, net_logit_threshold, heur_threshold, angular, device=0):
     """Recall of labelled tiles (tile selected and the label's bin proposed)
     and the fine-search points each method asks for, over the given cases."""
-    res = {"network": dict(tiles=0, hit=0, points=0.0), "heuristic": dict(tiles=0, hit=0, points=0.0), "positives": 0}
+    res = {k: dict(tiles=0, hit=0, points=0.0, missed_not_selected=0, missed_bin=0)
+           for k in ("network", "heuristic", "top_tiles")}
+    res["positives"] = 0
     per_bin = len(angular.fine_angles) / angular.n_bins
+    rank_net, rank_top, peak_tiles, rec_net, rec_top = [], [], [], [], []
+    offset = 0
     for cs in cases:
         out = network_scores(params, cs["feats"], device)
+        ndir = PR.network_directions(out, cs["frames"])
         lab = cs["labels"]
         posi = np.flatnonzero(lab[:, 0] > 0.5)
         res["positives"] += len(posi)
+        net_mask = out[:, 0] >= net_logit_threshold
+        top_mask = np.zeros(len(lab), bool)
+        top_mask[np.argsort(-cs["coarse_tile_max"], kind="stable")[:int(net_mask.sum())]] = True
         for name, sel_mask, dirs in (
-                ("network", out[:, 0] >= net_logit_threshold, out[:, 1:4]),
-                ("heuristic", cs["coarse_tile_max"] >= heur_threshold, cs.get("coarse_dirs"))):
+                ("network", net_mask, ndir),
+                ("heuristic", cs["coarse_tile_max"] >= heur_threshold, cs.get("coarse_dirs")),
+                ("top_tiles", top_mask, cs.get("coarse_dirs"))):
             sel = np.flatnonzero(sel_mask)
             r = res[name]
             r["tiles"] += len(sel)
@@ -137,9 +151,26 @@ def evaluate(cases, params, net_logit_threshold, heur_threshold, angular, device
             r["points"] += len(sel) * PR.BINS_PER_TILE * per_bin * W * W
             for i in posi:
                 if not sel_mask[i]:
+                    r["missed_not_selected"] += 1
                     continue
-                d = dirs[i] if dirs is not None else out[i, 1:4]
-                r["hit"] += bins_hit(angular, angular.nearest(d), lab[i, 1:4])
+                h = bins_hit(angular, angular.nearest(dirs[i]), lab[i, 1:4])
+                r["hit"] += h
+                r["missed_bin"] += 1 - h
+        # recall against tiles taken in each method's order, all cases pooled
+        rank_net.append(out[:, 0])
+        rank_top.append(cs["coarse_tile_max"])
+        for i in posi:
+            peak_tiles.append(offset + i)
+            rec_net.append(bins_hit(angular, angular.nearest(ndir[i]), lab[i, 1:4]))
+            rec_top.append(bins_hit(angular, angular.nearest(cs["coarse_dirs"][i]), lab[i, 1:4]))
+        offset += len(lab)
+    if peak_tiles:
+        res["tiles_for_recall"] = {
+            "network": PR.tiles_for_recall(peak_tiles, np.array(rec_net, bool),
+                                           np.argsort(-np.concatenate(rank_net), kind="stable")),
+            "coarse_z": PR.tiles_for_recall(peak_tiles, np.array(rec_top, bool),
+                                            np.argsort(-np.concatenate(rank_top), kind="stable")),
+            "tiles": offset}
     return res
 
 
@@ -160,8 +191,11 @@ def coarse_directions(coarse):
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--micrographs", type=int, default=24)
-    ap.add_argument("--held-out", type=int, default=4)
+    ap.add_argument("--validation", type=int, default=6, help="cases that set the objectness threshold")
+    ap.add_argument("--held-out", type=int, default=6, help="cases that only measure")
     ap.add_argument("--steps", type=int, default=1500)
+    ap.add_argument("--keep", type=float, default=0.95,
+                    help="share of training and validation positives the objectness threshold keeps")
     ap.add_argument("--seed", type=int, default=1000)
     ap.add_argument("--out", required=True)
     ap.add_argument("--summary", default=None)
@@ -182,21 +216,28 @@ def main(argv=None):
         log(f"case {i}: T={c['T']} snr={c['snr']:.3f} df={c['defocus']:.0f} peaks={len(cs['peaks'])} "
             f"positive tiles={int(cs['labels'][:, 0].sum())} search s={cs['seconds'][0]:.2f}+{cs['seconds'][1]:.2f}")
     gen_s = time.perf_counter() - t0
-    train_cases, held = cases[:-args.held_out], cases[-args.held_out:]
+    nv, nh = args.validation, args.held_out
+    train_cases, val, held = cases[:-(nv + nh)], cases[-(nv + nh):-nh], cases[-nh:]
     feats = np.concatenate([c["feats"] for c in train_cases])
-    labels = np.concatenate([c["labels"] for c in train_cases])
+    labels = np.concatenate([c["labels_local"] for c in train_cases])
     log(f"training tiles {len(feats)}, positives {int(labels[:, 0].sum())}")
     t0 = time.perf_counter()
     params, curve = train(feats, labels, steps=args.steps, seed=args.seed, device=args.device, log=log)
     train_s = time.perf_counter() - t0
-    out = network_scores(params, feats, args.device)
-    net_thr = threshold_for(out[:, 0], labels, margin=1.0)
-    heur_thr = threshold_for(np.concatenate([c["coarse_tile_max"] for c in train_cases]), labels, margin=0.25)
+    # thresholds: every training and validation positive kept, less a margin
+    fit = train_cases + val
+    fit_labels = np.concatenate([c["labels"] for c in fit])
+    out = np.concatenate([network_scores(params, c["feats"], args.device) for c in fit])
+    net_thr = threshold_for(out[:, 0], fit_labels, margin=0.5, keep=args.keep)
+    heur_thr = threshold_for(np.concatenate([c["coarse_tile_max"] for c in fit]), fit_labels, margin=0.25,
+                             keep=args.keep)
     ev_train = evaluate(train_cases, params, net_thr, heur_thr, angular, args.device)
+    ev_val = evaluate(val, params, net_thr, heur_thr, angular, args.device)
     ev_held = evaluate(held, params, net_thr, heur_thr, angular, args.device)
     summary = dict(cases=[c["case"] for c in cases], generation_s=gen_s, training_s=train_s, steps=args.steps,
                    loss_first=float(np.mean(curve[:50])), loss_last=float(np.mean(curve[-50:])),
-                   network_logit_threshold=net_thr, heuristic_z_threshold=heur_thr, train=ev_train, held_out=ev_held,
+                   network_logit_threshold=net_thr, heuristic_z_threshold=heur_thr, train=ev_train, validation=ev_val,
+                   held_out=ev_held,
                    n_params=int(len(params)))
     np.savez(args.out, params=params, network_logit_threshold=net_thr, heuristic_z_threshold=heur_thr,
              loss_curve=curve.astype(np.float32))

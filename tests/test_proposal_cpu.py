@@ -82,12 +82,21 @@ def test_tile_features_and_labels():
     t = 1 * 3 + 1   # tile row 1, column 1
     assert np.isclose(f[t, 0, 70 - 64, 100 - 64], 9.0 / 4.0)
     d = PR.directions(ph[70, 100], th[70, 100])
-    assert np.allclose(f[t, 4:7, 6, 36], d, atol=1e-6)
-    assert np.allclose(f[t, 1:4, 6, 36], d * 2.0, atol=1e-6)
+    # directions in the tile's frame: the coarse best direction at the maximum reads +z
+    frames = PR.tile_frames(z, th, ph)
+    assert np.allclose(frames[t] @ d, [0.0, 0.0, 1.0], atol=1e-12)
+    assert np.allclose(f[t, 4:7, 6, 36], [0.0, 0.0, 1.0], atol=1e-6)
+    assert np.allclose(f[t, 1:4, 6, 36], [0.0, 0.0, 2.0], atol=1e-6)
+    d2 = PR.directions(ph[70, 101], th[70, 101])
+    assert np.allclose(f[t, 4:7, 6, 37], frames[t] @ d2, atol=1e-6)
     peaks = np.array([[100, 70, 9.0, 30.0, 40.0, 0.0], [101, 71, 8.0, 0.0, 0.0, 0.0], [10, 10, 7.5, 0.0, 90.0, 0.0]])
     lab = PR.tile_labels(peaks, 192, 128)
     assert lab[:, 0].tolist() == [1, 0, 0, 0, 1, 0]
     assert np.allclose(lab[4, 1:], PR.directions(30.0, 40.0))
+    loc = PR.to_frames(lab, frames)
+    assert np.allclose(loc[:, 0], lab[:, 0])
+    out = np.concatenate([np.zeros((6, 1)), loc[:, 1:4] * 3.0], axis=1)
+    assert np.allclose(PR.network_directions(out, frames)[4], 3.0 * lab[4, 1:], atol=1e-9)
     for k in range(8):
         a = PR.dihedral(f, k)
         assert a.shape == f.shape
@@ -141,3 +150,11 @@ def test_window_geometry():
         assert C % PR.TILE == 0 and C >= PR.TILE
         m = (W - C - T) // 2
         assert m >= 8 and 2 * m + C + T == W
+
+
+def test_tiles_for_recall():
+    # peaks in tiles 3, 7, 7, 1; the second one cannot be recovered by its bins
+    ranking = np.array([7, 3, 0, 1, 2, 4, 5, 6])
+    need = PR.tiles_for_recall([3, 7, 7, 1], np.array([True, False, True, True]), ranking, levels=(0.5, 0.75, 1.0))
+    assert need == {"0.5": 2, "0.75": 4, "1.0": None}
+    assert PR.tiles_for_recall([], np.zeros(0, bool), ranking) == {"0.9": 0, "0.95": 0, "0.99": 0, "1.0": 0}
