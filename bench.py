@@ -610,7 +610,10 @@ def run_proposal(args):
     peak_sets = {"min_radius_T8": PR.find_peaks(exh, 7.0, T, WORKLOAD["pixel_size"]),
                  "min_radius_particle": PR.find_peaks(exh, 7.0, T, WORKLOAD["pixel_size"],
                                                       min_peak_radius=int(WORKLOAD["radius_A"] / WORKLOAD["pixel_size"]))}
-    recalls, diags = {}, {}
+    # the reference's expected threshold for this search (one false positive: sqrt(2) erfcinv(2 / N),
+    # match_template.cpp:1282): z >= 7 peaks below it are chance maxima of the exhaustive search
+    thr_ref = float(np.sqrt(2.0) * hostprep.lib().tmh_erfcinv(2.0 / (float(X) * Y * len(angular.fine_angles))))
+    recalls, diags = {"expected_threshold": thr_ref}, {}
     for key, pk in peak_sets.items():
         rn = PR.recall(pk, exh, res, PR.proposal_z(res, coarse, X, Y), 7.0)
         rt = PR.recall(pk, exh, res_t, PR.proposal_z(res_t, coarse, X, Y), 7.0)
@@ -630,6 +633,11 @@ def run_proposal(args):
                         "network_missed_tile_not_selected": int(np.sum(~dg["network_selected"])),
                         "network_missed_bin_not_proposed": int(np.sum(dg["network_selected"] & (dg["network_bin_rank"] < 0))),
                         "bin_outside_16_nearest_at_peak": int(np.sum(dg["bin_rank_at_peak_coarse_direction"] >= 16)),
+                        "peaks_above_expected_threshold": int(np.sum(dg["z"] >= thr_ref)) if len(pk) else 0,
+                        "network_recall_above_expected_threshold":
+                            float(np.mean(dg["network_recovered"][dg["z"] >= thr_ref])) if np.any(dg["z"] >= thr_ref) else 1.0,
+                        "top_tiles_recall_above_expected_threshold":
+                            float(np.mean(dg["top_tiles_recovered"][dg["z"] >= thr_ref])) if np.any(dg["z"] >= thr_ref) else 1.0,
                         "tiles_for_recall": curves}
     # MIP error where the window search found the exhaustive search's best orientation
     same = np.isfinite(res["mip"]) & (res["psi"] == exh["psi"]) & (res["theta"] == exh["theta"]) & (res["phi"] == exh["phi"])
