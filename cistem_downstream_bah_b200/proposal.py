@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import ctypes
 import time
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -251,15 +252,25 @@ def tile_features(z, theta, phi, tile=TILE, frames=None):
     gy, gx = tile_grid(nx, ny, tile)
     if frames is None:
         frames = tile_frames(z, theta, phi, tile)
-    zc = np.clip(z[:gy * tile, :gx * tile], -4.0, 12.0)
-    d = directions(phi[:gy * tile, :gx * tile], theta[:gy * tile, :gx * tile])
-    d = d.reshape(gy, tile, gx, tile, 3).transpose(0, 2, 1, 3, 4).reshape(gy * gx, tile * tile, 3)
-    d = np.einsum("nij,npj->npi", frames, d)
-    w = np.clip(zc - 3.0, 0.0, 9.0) / 3.0
-    w = w.reshape(gy, tile, gx, tile).transpose(0, 2, 1, 3).reshape(gy * gx, tile * tile, 1)
-    zt = (zc / 4.0).reshape(gy, tile, gx, tile).transpose(0, 2, 1, 3).reshape(gy * gx, tile * tile, 1)
-    f = np.concatenate([zt, d * w, d], axis=-1).astype(np.float32)          # (n, tile*tile, 7)
-    return np.ascontiguousarray(f.transpose(0, 2, 1).reshape(gy * gx, FEATURES, tile, tile))
+    n, P = gy * gx, tile * tile
+
+    def tiles(a):   # (gy*tile, gx*tile, ...) -> (n, P, ...)
+        return a.reshape(gy, tile, gx, tile, *a.shape[2:]).swapaxes(1, 2).reshape(n, P, *a.shape[2:])
+
+    zc = np.clip(np.asarray(z[:gy * tile, :gx * tile], np.float32), -4.0, 12.0)
+    th = np.radians(np.asarray(theta[:gy * tile, :gx * tile], np.float32))
+    ph = np.radians(np.asarray(phi[:gy * tile, :gx * tile], np.float32))
+    st = np.sin(th)
+    d = tiles(np.stack([st * np.cos(ph), st * np.sin(ph), np.cos(th)], axis=-1))          # (n, P, 3)
+    d = np.matmul(d, np.asarray(frames, np.float32).transpose(0, 2, 1))                    # rows R d
+    zt = tiles(zc)
+    w = np.clip(zt - 3.0, 0.0, 9.0) / 3.0
+    out = np.empty((n, FEATURES, P), np.float32)
+    out[:, 0] = zt / 4.0
+    dt = d.transpose(0, 2, 1)
+    out[:, 1:4] = dt * w[:, None, :]
+    out[:, 4:7] = dt
+    return out.reshape(n, FEATURES, tile, tile)
 
 
 def to_frames(labels, frames):
@@ -453,31 +464,43 @@ class WindowSearch:
         for t, b in zip(proposal.tiles, proposal.bins):
             ty, tx = divmod(int(t), gx)
             groups.setdefault((ty // per_core, tx // per_core), []).append((ty, tx, b))
-        points = 0.0
-        t0 = time.perf_counter()
-        for (cy, cx), items in sorted(groups.items()):
+        m = self.margin
+
+        def prepare(entry):
+            """Orientations and spectrum of one window (host work, run ahead of the GPU)."""
+            (cy, cx), items = entry
             bins = set()
             for _, _, b in items:
                 bins.update(int(v) for v in b)
-            rows = self.angular.orientations(sorted(bins))
-            angles = self.angular.fine_angles[rows]
-            m = self.margin
+            angles = self.angular.fine_angles[self.angular.orientations(sorted(bins))]
             x0, y0 = cx * C - T // 2 - m, cy * C - T // 2 - m
             # the used square keeps two pixels beyond the interior's reach on each side
-            self.sc.set_image(window_spectrum(self.s, x0, y0, W, X * Y, (m - 2, W - m + 2)))
-            self.sc.reset()
-            self.sc.run_plane(self.filt, angles)
-            r = self.sc.results()
-            points += float(len(angles)) * W * W
-            wm = r["mip"].reshape(W, W)
-            for ty, tx, _ in items:
-                ys = slice(ty * TILE, (ty + 1) * TILE)
-                xs = slice(tx * TILE, (tx + 1) * TILE)
-                wy = slice(ty * TILE - y0, (ty + 1) * TILE - y0)
-                wx = slice(tx * TILE - x0, (tx + 1) * TILE - x0)
-                mip[ys, xs] = wm[wy, wx]
-                for k in ang:
-                    ang[k][ys, xs] = r[k].reshape(W, W)[wy, wx]
+            spec = window_spectrum(self.s, x0, y0, W, X * Y, (m - 2, W - m + 2))
+            return items, angles, spec, x0, y0
+
+        points = 0.0
+        t0 = time.perf_counter()
+        entries = sorted(groups.items())
+        with ThreadPoolExecutor(max_workers=1) as pool:
+            ahead = [pool.submit(prepare, e) for e in entries[:2]]
+            for i in range(len(entries)):
+                items, angles, spec, x0, y0 = ahead.pop(0).result()
+                if i + 2 < len(entries):
+                    ahead.append(pool.submit(prepare, entries[i + 2]))
+                self.sc.set_image(spec)
+                self.sc.reset()
+                self.sc.run_plane(self.filt, angles)   # the GIL is released while the GPU searches
+                r = self.sc.results()
+                points += float(len(angles)) * W * W
+                wm = r["mip"].reshape(W, W)
+                for ty, tx, _ in items:
+                    ys = slice(ty * TILE, (ty + 1) * TILE)
+                    xs = slice(tx * TILE, (tx + 1) * TILE)
+                    wy = slice(ty * TILE - y0, (ty + 1) * TILE - y0)
+                    wx = slice(tx * TILE - x0, (tx + 1) * TILE - x0)
+                    mip[ys, xs] = wm[wy, wx]
+                    for k in ang:
+                        ang[k][ys, xs] = r[k].reshape(W, W)[wy, wx]
         return {"mip": mip, **ang, "points": points, "seconds": time.perf_counter() - t0, "windows": len(groups)}
 
     def close(self):
