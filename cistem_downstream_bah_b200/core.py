@@ -165,6 +165,12 @@ class SearchCore:
         self._check(self.L.tm_set_micrograph(self.h, _ptr(img), self.X, self.Y, _ptr(curve), cap, ctypes.byref(n)))
         return curve[:n.value].copy()
 
+    def set_normalization_pixels(self, n_pixels):
+        """Forms the projection variance over n_pixels instead of the context's
+        X*Y (0 restores that): a window cut from a larger whitened micrograph
+        then reports that micrograph's correlation values."""
+        self._check(self.L.tm_set_normalization_pixels(self.h, ctypes.c_longlong(int(n_pixels))))
+
     def reset(self):
         self._check(self.L.tm_reset_results(self.h))
 

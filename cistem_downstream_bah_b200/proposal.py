@@ -450,7 +450,7 @@ class WindowSearch:
         self.sc = core.SearchCore(self.W, self.W, T, histogram_min_scaled=hmin, histogram_step_scaled=hstep,
                                   device=device)
         self.sc.set_template(tspec)
-        self.sc._check(self.sc.L.tm_set_normalization_pixels(self.sc.h, ctypes.c_longlong(X * Y)))
+        self.sc.set_normalization_pixels(X * Y)
 
     def run(self, proposal):
         """MIP / best angles over the proposed tiles (-inf elsewhere), with the

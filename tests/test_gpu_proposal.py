@@ -175,3 +175,14 @@ def test_trained_network_gains_over_the_method_without_it():
           f"untrained {r_untrained:.3f}, coarse z {r_coarse:.3f}")
     assert r_trained == 1.0
     assert r_untrained < r_trained
+
+
+def test_normalization_pixels_argument():
+    sc = core.SearchCore(256, 256, 64, histogram_min_scaled=-0.05, histogram_step_scaled=0.001)
+    try:
+        with pytest.raises(core.TmError):
+            sc.set_normalization_pixels(-1)
+        sc.set_normalization_pixels(1024 * 1024)
+        sc.set_normalization_pixels(0)
+    finally:
+        sc.close()
