@@ -131,20 +131,20 @@ k_conv3x3_wgrad(const float* __restrict__ in, const float* __restrict__ g, float
     float s[10];
 #pragma unroll
     for (int k = 0; k < 10; k++) s[k] = 0.0f;
-    for (int n = n0; n < n1; n++) {
-        const float* gp = g + ((size_t)n * Co + o) * HWp;
+    // threads run over (image, pixel) pairs of the chunk, so that small maps keep them busy
+    const long long e1 = (long long)(n1 - n0) * HWp;
+    for (long long e = threadIdx.x; e < e1; e += kThreads) {
+        const int n = n0 + (int)(e / HWp), p = (int)(e % HWp);
+        const float gv = g[((size_t)n * Co + o) * HWp + p];
+        if (gv == 0.0f) continue;
         const float* ip = in + ((size_t)n * Ci + i) * HWp;
-        for (int p = threadIdx.x; p < HWp; p += kThreads) {
-            const float gv = gp[p];
-            if (gv == 0.0f) continue;
-            const int y = p / W, x = p % W;
+        const int y = p / W, x = p % W;
 #pragma unroll
-            for (int k = 0; k < 9; k++) {
-                const int yy = y + k / 3 - 1, xx = x + k % 3 - 1;
-                if (yy >= 0 && yy < H && xx >= 0 && xx < W) s[k] = fmaf(gv, ip[yy * W + xx], s[k]);
-            }
-            s[9] += gv;
+        for (int k = 0; k < 9; k++) {
+            const int yy = y + k / 3 - 1, xx = x + k % 3 - 1;
+            if (yy >= 0 && yy < H && xx >= 0 && xx < W) s[k] = fmaf(gv, ip[yy * W + xx], s[k]);
         }
+        s[9] += gv;
     }
     __shared__ float red[kThreads / 32][10];
 #pragma unroll
