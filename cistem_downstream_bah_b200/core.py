@@ -182,7 +182,7 @@ class SearchCore:
         self._check(self.L.tm_run_plane(self.h, _ptr(f), _ptr(a), len(a), defocus_offset, pixel_size_offset, cb, None))
 
     def autotune(self, projection_filter, euler_angles):
-        """Picks the orientations per device pass (16, 32 or 64) by timing the
+        """Picks the orientations per device pass (16, 32, 64 or 128) by timing the
         given orientations (contexts created with orientation_batch=0); clears
         the running results.  Returns the batch."""
         f = np.ascontiguousarray(projection_filter, dtype=np.float32)

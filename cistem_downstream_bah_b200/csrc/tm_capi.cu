@@ -595,7 +595,7 @@ int tm_create(const tm_dims* dims, tm_ctx** out) {
     c->T = dims->template_size;
     c->TP = c->T / 2 + 1;
     c->B = dims->orientation_batch > 0 ? dims->orientation_batch : 32;
-    c->Bcap = dims->orientation_batch > 0 ? dims->orientation_batch : 64;   // 0 = automatic: room to tune up to 64
+    c->Bcap = dims->orientation_batch > 0 ? dims->orientation_batch : 128;   // 0 = automatic: room to tune up to 128
     if (dims->histogram_bins <= 0 || dims->histogram_bins > 1024 || !(dims->histogram_step_scaled > 0)) {
         *out = c;
         return set_err(c, TM_ERR_INVALID, "histogram_bins must be 1..1024 and the step positive");
@@ -631,12 +631,11 @@ int tm_create(const tm_dims* dims, tm_ctx** out) {
         if (e != cudaSuccess) { *out = c; return set_err(c, TM_ERR_CUDA, "stream/event creation: %s", cudaGetErrorString(e)); }
     }
     if (dims->orientation_batch <= 0) {
-        // automatic batch: keep the capacity for 64 orientations only if the
-        // correlation spectra of 64 fit in half of the free device memory
+        // automatic batch: keep the capacity for 128 (else 64, else 32) orientations
+        // only if their correlation spectra fit in a quarter of the free device memory
         size_t free_b = 0, total_b = 0;
-        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
-            (size_t)64 * c->Y * c->XP * sizeof(float2) > free_b / 2)
-            c->Bcap = 32;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess)
+            while (c->Bcap > 32 && (size_t)c->Bcap * c->Y * c->XP * sizeof(float2) > free_b / 4) c->Bcap /= 2;
     }
     const size_t T = c->T, X = c->X, Y = c->Y, XP = c->XP, TP = c->TP, B = c->Bcap;
     TRY(dalloc(c, &c->tmpl, T * T * TP));
@@ -1121,7 +1120,7 @@ int tm_debug_stage_buffers(tm_ctx* c, const float* projection_filter, const floa
 
 int tm_autotune_batch(tm_ctx* c, const float* projection_filter, const float* euler_angles, int n, int* chosen) {
     if (!c || !projection_filter || !euler_angles || n <= 0) return TM_ERR_INVALID;
-    const int cands[3] = {16, 32, 64};
+    const int cands[4] = {16, 32, 64, 128};
     int best_b = c->B;
     double best = 1e30;
     bool warmed = false;

@@ -447,8 +447,9 @@ class WindowSearch:
         self.s = whitened_real(ispec, X, Y)
         self.filt = filt
         self.angular = angular
+        # 256 orientations per device pass: at these small boxes the per-pass costs weigh (1.4x over 32)
         self.sc = core.SearchCore(self.W, self.W, T, histogram_min_scaled=hmin, histogram_step_scaled=hstep,
-                                  device=device)
+                                  orientation_batch=256, device=device)
         self.sc.set_template(tspec)
         self.sc.set_normalization_pixels(X * Y)
 

@@ -53,7 +53,7 @@ typedef struct tm_dims {
     double histogram_min_scaled;   /* histogram_min / sqrt(X*Y) */
     double histogram_step_scaled;  /* histogram_step / sqrt(X*Y) */
     int orientation_batch;         /* orientations per device pass; 0 = automatic (32 until
-                                      tm_autotune_batch picks 16, 32 or 64) */
+                                      tm_autotune_batch picks 16, 32, 64 or 128) */
     int device;                    /* CUDA device ordinal */
 } tm_dims;
 
@@ -201,9 +201,10 @@ TM_API int tm_run_plane_noalloc(int device, const tm_dims *dims, const float *d_
 /* Automatic orientation batch (no counterpart in the reference, whose GPU
  * path processes one orientation per launch).  For a context created with
  * orientation_batch = 0, times tm_run_plane over the given orientations with
- * 16, 32 and 64 orientations per device pass (64 only when its buffers fit in
- * half of the free device memory at tm_create), keeps the fastest and clears
- * the running results.  Use 128 or more orientations of the real search.
+ * 16, 32, 64 and 128 orientations per device pass (the larger ones only when
+ * their correlation spectra fit in a quarter of the free device memory at
+ * tm_create), keeps the fastest and clears the running results.  Use 256 or
+ * more orientations of the real search.
  * chosen (may be NULL) receives the batch.  The template and image must be set. */
 TM_API int tm_autotune_batch(tm_ctx *ctx, const float *projection_filter, const float *euler_angles,
                              int n_orientations, int *chosen);

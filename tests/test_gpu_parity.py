@@ -114,7 +114,7 @@ def test_autotuned_batch_keeps_parity():
     case = make_case(T=32, X=256, Y=256, angular_step=30.0, psi_step=30.0)
     with _core(case, batch=0) as sc:
         b = sc.autotune(case["filt"], case["angles"][:160])
-        assert b in (16, 32, 64) and sc.orientation_batch() == b
+        assert b in (16, 32, 64, 128) and sc.orientation_batch() == b
         assert sc.correlations_computed() == 0   # the tuning runs are cleared
         sc.run_plane(case["filt"], case["angles"])
         r = sc.results()
@@ -122,3 +122,19 @@ def test_autotuned_batch_keeps_parity():
     O.search(st, case["tspec"], case["ispec"], case["filt"], case["angles"], hist_min_scaled=case["hmin"],
              hist_step_scaled=case["hstep"])
     assert np.abs(r["mip"] - st.mip).max() / np.abs(st.mip).max() < 1e-4
+
+
+def test_large_batches_match_small():
+    """256 orientations per device pass (the proposal's window searches) give the
+    same maps as 32."""
+    case = make_case(T=32, X=256, Y=256, angular_step=20.0, psi_step=20.0)
+    out = {}
+    for b in (32, 256):
+        with _core(case, batch=b) as sc:
+            sc.run_plane(case["filt"], case["angles"])
+            out[b] = sc.results()
+    assert len(case["angles"]) > 256
+    for k in ("mip", "psi", "theta", "phi"):
+        assert np.array_equal(out[32][k], out[256][k]), k
+    scale = np.abs(out[32]["sum"]).max()
+    assert np.abs(out[32]["sum"] - out[256]["sum"]).max() <= 1e-5 * scale
