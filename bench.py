@@ -462,13 +462,10 @@ def run_ours(args):
 
 
 # ncu dram__bytes_read.sum + dram__bytes_write.sum per launch at 4096^2 / 256^3, by orientation batch
-# (32 and 64 captured; 128 is the 64-orientation capture scaled by the orientations per launch --
-# from 32 to 64 the bytes grew x1.89 (pass B) and x1.73 (pass C) -- since a multi-pass capture at
-# 128 would hold about 10 GB on the device)
 PROFILED_TRAFFIC = {
     32: {"k_pass_b": 0.869e9 + 2.142e9, "k_pass_c": 2.555e9 + 0.382e9},
     64: {"k_pass_b": 1.408e9 + 4.292e9, "k_pass_c": 4.707e9 + 0.388e9},
-    128: {"k_pass_b": 2.0 * (1.408e9 + 4.292e9), "k_pass_c": 2.0 * (4.707e9 + 0.388e9)},
+    128: {"k_pass_b": 2.485e9 + 8.595e9, "k_pass_c": 9.011e9 + 0.392e9},
 }
 
 
