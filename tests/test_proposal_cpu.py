@@ -158,3 +158,43 @@ def test_tiles_for_recall():
     need = PR.tiles_for_recall([3, 7, 7, 1], np.array([True, False, True, True]), ranking, levels=(0.5, 0.75, 1.0))
     assert need == {"0.5": 2, "0.75": 4, "1.0": None}
     assert PR.tiles_for_recall([], np.zeros(0, bool), ranking) == {"0.9": 0, "0.95": 0, "0.99": 0, "1.0": 0}
+
+
+def test_window_variants_are_compiled():
+    """Every template box the proposal trains and evaluates on (64, 128, 256) has a
+    search kernel for its window geometry and for the 1024^2 training micrographs."""
+    import os
+    import re
+    src = open(os.path.join(os.path.dirname(PR.__file__), "csrc", "tm_capi.cu")).read()
+    variants = {tuple(int(v) for v in m) for m in re.findall(r"TM_VARIANT\((\d+),\s*(\d+),\s*(\d+)\)", src)}
+    for T in (64, 128, 256):
+        W = PR.window_size(T)
+        assert (T, W, W) in variants, (T, W)
+    for T in (64, 128):
+        assert (T, 1024, 1024) in variants
+    assert (256, 4096, 4096) in variants
+
+
+def test_threshold_and_bins_helpers():
+    from cistem_downstream_bah_b200 import proposal_train as PT
+    scores = np.array([5.0, -1.0, 3.0, 0.5, 2.0])
+    lab = np.zeros((5, 4))
+    lab[[0, 2, 4], 0] = 1.0
+    assert PT.threshold_for(scores, lab, margin=0.5) == 2.0 - 0.5           # keeps every positive
+    assert PT.threshold_for(scores, lab, margin=0.0, keep=0.5) == 3.0       # keeps the upper half
+    assert PT.threshold_for(scores, np.zeros((5, 4)), margin=0.0) == float("inf")
+    ab = PR.AngularBins(15.0, 7.5, 10.0)
+    d = ab.centers[7]
+    assert PT.bins_hit(ab, ab.nearest(d, 1), d)
+    far = -d
+    assert not PT.bins_hit(ab, ab.nearest(d, 4), far)
+
+
+def test_case_parameters_follow_the_training_distribution():
+    from cistem_downstream_bah_b200 import proposal_train as PT
+    for seed in range(1000, 1100, 7):
+        c = PT.case_params(seed)
+        assert c["T"] in (64, 128)
+        assert 0.02 <= c["snr"] <= 0.08 and 5000.0 <= c["defocus"] <= 25000.0
+        assert c["radius_A"] <= 0.45 * c["T"] * c["pixel_size"]
+        assert c == PT.case_params(seed)    # seeded
