@@ -35,7 +35,8 @@ EXPORTED = [
     "tm_refine_score", "tm_refine_last_error", "tm_refine_destroy", "tm_set_micrograph", "tm_whiten_micrograph",
     "tm_set_template_volume", "tm_template_spectrum", "tm_set_normalization_pixels", "tm_pnet_create",
     "tm_pnet_param_count", "tm_pnet_set_params", "tm_pnet_get_params", "tm_pnet_forward", "tm_pnet_gradients",
-    "tm_pnet_train_step", "tm_pnet_last_error", "tm_pnet_destroy",
+    "tm_pnet_train_step", "tm_pnet_last_error", "tm_pnet_destroy", "tm_set_image_set", "tm_run_plane_images",
+    "tm_get_image_results",
 ]
 
 
@@ -106,6 +107,9 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.tm_set_template_volume.argtypes = [vp, vp, ip, fp]
     L.tm_template_spectrum.argtypes = [ip, vp, ip, fp, vp]
     L.tm_set_normalization_pixels.argtypes = [vp, ctypes.c_longlong]
+    L.tm_set_image_set.argtypes = [vp, ip, vp]
+    L.tm_run_plane_images.argtypes = [vp, vp, vp, ip, vp, ip, fp, fp]
+    L.tm_get_image_results.argtypes = [vp, ip, vp, vp, vp, vp]
     _LIB = L
     return L
 
@@ -170,6 +174,28 @@ class SearchCore:
         X*Y (0 restores that): a window cut from a larger whitened micrograph
         then reports that micrograph's correlation values."""
         self._check(self.L.tm_set_normalization_pixels(self.h, ctypes.c_longlong(int(n_pixels))))
+
+    def set_image_set(self, spectra):
+        """Several micrograph spectra of this context's size, each with its own results."""
+        s = np.ascontiguousarray(spectra, dtype=np.complex64)
+        assert s.ndim == 3 and s.shape[1:] == (self.Y, self.X // 2 + 1), s.shape
+        self._check(self.L.tm_set_image_set(self.h, len(s), _ptr(s)))
+        self.n_images = len(s)
+
+    def run_plane_images(self, projection_filter, euler_angles, images, defocus_offset=0.0, pixel_size_offset=0.0):
+        f = np.ascontiguousarray(projection_filter, dtype=np.float32)
+        assert f.shape == (self.T, self.T // 2 + 1), f.shape
+        a = np.ascontiguousarray(euler_angles, dtype=np.float32).reshape(-1, 3)
+        ids = np.ascontiguousarray(images, dtype=np.int32)
+        self._check(self.L.tm_run_plane_images(self.h, _ptr(f), _ptr(a), len(a), _ptr(ids), len(ids),
+                                               defocus_offset, pixel_size_offset))
+
+    def image_results(self, image):
+        n = self.X * self.Y
+        out = {k: np.zeros(n, np.float32) for k in ("mip", "psi", "theta", "phi")}
+        self._check(self.L.tm_get_image_results(self.h, int(image), _ptr(out["mip"]), _ptr(out["psi"]),
+                                                _ptr(out["theta"]), _ptr(out["phi"])))
+        return out
 
     def reset(self):
         self._check(self.L.tm_reset_results(self.h))

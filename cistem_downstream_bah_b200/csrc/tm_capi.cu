@@ -69,6 +69,15 @@ struct tm_ctx {
     long long next_gidx = 0;
     long long n_ccs = 0;
     long long norm_pixels = 0;   // projection variance pixel count override (0: X*Y)
+    // image set (tm_set_image_set): per image its prepared spectrum and running results
+    struct Slot {
+        float2* Ip = nullptr;
+        float* mip = nullptr;
+        int* best = nullptr;
+        double *sum = nullptr, *sumsq = nullptr;
+        unsigned long long* hist = nullptr;
+    };
+    std::vector<Slot> slots;
     double last_total_ms = 0, last_b_ms = 0, last_c_ms = 0, last_prep_ms = 0;
     std::string err;
 };
@@ -115,6 +124,7 @@ struct Variant {
     int (*configure)(tm_ctx*);
     int (*run_stages)(tm_ctx*, tmk::BatchArgs&);   // every kernel before the MIP epilogue
     WhitenFn whiten;
+    int (*run_batch_images)(tm_ctx*, tmk::BatchArgs&, const int* ids, int n_ids);   // image-set batch
 };
 
 // number of points of the whitening curve (match_template.cpp:702)
@@ -207,6 +217,28 @@ struct Impl {
         return TM_OK;
     }
 
+    // one orientation batch over several images of the image set: the slice,
+    // projection, normalisation and row transforms once, then passes B and C
+    // per image (they reuse the correlation buffer in stream order)
+    static int run_batch_images(tm_ctx* c, tmk::BatchArgs& a, const int* ids, int n_ids) {
+        cudaStream_t s = c->stream;
+        LN::prep(a, s);
+        for (int k = 0; k < n_ids; k++) {
+            const tm_ctx::Slot& sl = c->slots[ids[k]];
+            a.Ip = sl.Ip;
+            a.mip = sl.mip;
+            a.best = sl.best;
+            a.sum = sl.sum;
+            a.sumsq = sl.sumsq;
+            a.hist = sl.hist;
+            LN::pass_b(a, s, c->nsm);
+            LN::pass_c(a, s);
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return set_err(c, TM_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+        return TM_OK;
+    }
+
     static int run_batch(tm_ctx* c, tmk::BatchArgs& a, cudaEvent_t* ev) {
         cudaStream_t s = c->stream;
         if (ev) cudaEventRecord(ev[0], s);
@@ -224,7 +256,7 @@ struct Impl {
 
 #define TM_VARIANT(T, X, Y)                                                                                 \
     {T, X, Y, tmk::Launch<T, X, Y>::pass_b_width, &Impl<T, X, Y>::run_batch, &Impl<T, X, Y>::configure,          \
-     &Impl<T, X, Y>::run_stages, &whiten_on_device<X, Y>}
+     &Impl<T, X, Y>::run_stages, &whiten_on_device<X, Y>, &Impl<T, X, Y>::run_batch_images}
 
 // Geometries with compiled kernels: template box T on a padded X x Y
 // micrograph.  X is a power of two (the reference turns a micrograph whose
@@ -302,6 +334,12 @@ void free_all(tm_ctx* c) {
                     c->rowstat, c->mip, c->best, c->sum, c->sumsq, c->hist, c->err_flag};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    for (tm_ctx::Slot& sl : c->slots) {
+        void* sp[] = {sl.Ip, sl.mip, sl.best, sl.sum, sl.sumsq, sl.hist};
+        for (void* p : sp)
+            if (p) cudaFree(p);
+    }
+    c->slots.clear();
     if (c->best_host) cudaFreeHost(c->best_host);
     if (c->stream) cudaStreamDestroy(c->stream);
     cudaEvent_t evs[] = {c->ev_start, c->ev_prep, c->ev_b, c->ev_c, c->ev_end};
@@ -903,6 +941,11 @@ int tm_reset_results(tm_ctx* c) {
     tmk::k_reset_state<<<c->nsm * 4, 256, 0, c->stream>>>(c->mip, c->best, c->sum, c->sumsq, n);
     TM_CUDA(c, cudaGetLastError());
     TM_CUDA(c, cudaMemsetAsync(c->hist, 0, sizeof(unsigned long long) * 1024, c->stream));
+    for (tm_ctx::Slot& sl : c->slots) {   // the image set's results too (their indices refer to the planes)
+        tmk::k_reset_state<<<c->nsm * 4, 256, 0, c->stream>>>(sl.mip, sl.best, sl.sum, sl.sumsq, n);
+        TM_CUDA(c, cudaGetLastError());
+        TM_CUDA(c, cudaMemsetAsync(sl.hist, 0, sizeof(unsigned long long) * 1024, c->stream));
+    }
     int rc = wait_stream(c, 60.0);
     if (rc != TM_OK) return rc;
     c->planes.clear();
@@ -1148,6 +1191,139 @@ int tm_autotune_batch(tm_ctx* c, const float* projection_filter, const float* eu
 }
 
 int tm_orientation_batch(const tm_ctx* c) { return c ? c->B : 0; }
+
+int tm_set_image_set(tm_ctx* c, int n_images, const float* spectra) {
+    if (!c || !spectra || n_images < 1 || n_images > 4096) return TM_ERR_INVALID;
+    TM_CUDA(c, cudaSetDevice(c->device));
+    int rc = tm_reset_results(c);   // a new set starts a new search: planes and main state cleared
+    if (rc != TM_OK) return rc;
+    const size_t X = c->X, Y = c->Y, XP = c->XP, hc = X / 2 + 1, n = X * Y;
+    if ((int)c->slots.size() != n_images) {
+        for (tm_ctx::Slot& sl : c->slots) {
+            void* sp[] = {sl.Ip, sl.mip, sl.best, sl.sum, sl.sumsq, sl.hist};
+            for (void* q : sp)
+                if (q) cudaFree(q);
+        }
+        c->slots.assign((size_t)n_images, tm_ctx::Slot{});
+        for (tm_ctx::Slot& sl : c->slots) {
+            if ((rc = dalloc(c, &sl.Ip, Y * XP)) != TM_OK) return rc;
+            if ((rc = dalloc(c, &sl.mip, n)) != TM_OK) return rc;
+            if ((rc = dalloc(c, &sl.best, n)) != TM_OK) return rc;
+            if ((rc = dalloc(c, &sl.sum, n)) != TM_OK) return rc;
+            if ((rc = dalloc(c, &sl.sumsq, n)) != TM_OK) return rc;
+            if ((rc = dalloc(c, &sl.hist, (size_t)1024)) != TM_OK) return rc;
+            TM_CUDA(c, cudaMemsetAsync(sl.Ip, 0, sizeof(float2) * Y * XP, c->stream));
+        }
+    }
+    // each spectrum is staged in the correlation buffer and prepared as tm_set_image does
+    for (int k = 0; k < n_images; k++) {
+        tm_ctx::Slot& sl = c->slots[k];
+        TM_CUDA(c, cudaMemcpyAsync(c->C, spectra + (size_t)k * Y * hc * 2, sizeof(float2) * Y * hc,
+                                   cudaMemcpyHostToDevice, c->stream));
+        tmk::k_prepare_image<<<dim3((unsigned)((XP + 127) / 128), (unsigned)Y), 128, 0, c->stream>>>(c->C, sl.Ip, c->X, c->Y,
+                                                                                                    c->XP, c->T);
+        tmk::k_reset_state<<<c->nsm * 4, 256, 0, c->stream>>>(sl.mip, sl.best, sl.sum, sl.sumsq, n);
+        TM_CUDA(c, cudaMemsetAsync(sl.hist, 0, sizeof(unsigned long long) * 1024, c->stream));
+        TM_CUDA(c, cudaGetLastError());
+        // the staging buffer is reused by the next image: keep the copies in order
+        if ((rc = wait_stream(c, 600.0)) != TM_OK) return rc;
+    }
+    return TM_OK;
+}
+
+int tm_run_plane_images(tm_ctx* c, const float* projection_filter, const float* euler_angles, int n,
+                        const int* images, int n_images, float defocus_offset, float pixel_size_offset) {
+    if (!c || !projection_filter || (!euler_angles && n > 0) || n < 0 || !images || n_images < 1) return TM_ERR_INVALID;
+    if (!c->has_template) return set_err(c, TM_ERR_INVALID, "template must be set before tm_run_plane_images");
+    if (c->slots.empty()) return set_err(c, TM_ERR_INVALID, "no image set (tm_set_image_set)");
+    for (int k = 0; k < n_images; k++)
+        if (images[k] < 0 || images[k] >= (int)c->slots.size())
+            return set_err(c, TM_ERR_INVALID, "image %d outside the set of %d", images[k], (int)c->slots.size());
+    if (c->next_gidx + n > 2147483647LL) return set_err(c, TM_ERR_INVALID, "more than 2^31 orientations since the last reset");
+    if (n == 0) return TM_OK;
+    TM_CUDA(c, cudaSetDevice(c->device));
+    if (n > c->rot_capacity) {
+        if (c->rot) cudaFree(c->rot);
+        c->rot = nullptr;
+        int rc = dalloc(c, &c->rot, (size_t)6 * n);
+        if (rc != TM_OK) return rc;
+        c->rot_capacity = n;
+    }
+    std::vector<float> rot((size_t)6 * n);
+    euler_rows(euler_angles, n, rot.data());
+    TM_CUDA(c, cudaMemcpyAsync(c->rot, rot.data(), sizeof(float) * rot.size(), cudaMemcpyHostToDevice, c->stream));
+    TM_CUDA(c, cudaMemcpyAsync(c->filter, projection_filter, sizeof(float) * (size_t)c->T * c->TP, cudaMemcpyHostToDevice, c->stream));
+    Plane pl;
+    pl.base = c->next_gidx;
+    pl.n = n;
+    pl.defocus = defocus_offset;
+    pl.pixel = pixel_size_offset;
+    c->angle_lists.emplace_back(euler_angles, euler_angles + 3 * (size_t)n);
+    pl.angles_id = (int)c->angle_lists.size() - 1;
+    c->planes.push_back(pl);
+    tmk::BatchArgs a = make_args(c);
+    a.rot = c->rot;
+    TM_CUDA(c, cudaEventRecord(c->ev_start, c->stream));
+    for (int o0 = 0; o0 < n; o0 += c->B) {
+        a.orient0 = o0;
+        a.nb = n - o0 < c->B ? n - o0 : c->B;
+        a.gidx0 = pl.base + o0;
+        int rc = c->var->run_batch_images(c, a, images, n_images);
+        if (rc != TM_OK) return rc;
+    }
+    TM_CUDA(c, cudaEventRecord(c->ev_c, c->stream));
+    int w = wait_stream(c, 3600.0);
+    if (w != TM_OK) return w;
+    int flag = 0;
+    TM_CUDA(c, cudaMemcpy(&flag, c->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        cudaMemset(c->err_flag, 0, sizeof(int));
+        return set_err(c, TM_ERR_TIMEOUT, "a bulk copy did not complete within its wait limit; results of this plane are invalid");
+    }
+    float tot = 0;
+    cudaEventElapsedTime(&tot, c->ev_start, c->ev_c);
+    c->last_total_ms = tot;
+    c->last_prep_ms = c->last_b_ms = c->last_c_ms = 0;
+    c->next_gidx += n;
+    c->n_ccs += (long long)n * n_images;
+    return TM_OK;
+}
+
+int tm_get_image_results(tm_ctx* c, int image, float* mip, float* best_psi, float* best_theta, float* best_phi) {
+    if (!c || image < 0 || image >= (int)c->slots.size()) return TM_ERR_INVALID;
+    TM_CUDA(c, cudaSetDevice(c->device));
+    int rc = wait_stream(c, 3600.0);
+    if (rc != TM_OK) return rc;
+    const size_t n = (size_t)c->X * c->Y;
+    const tm_ctx::Slot& sl = c->slots[image];
+    if (mip) TM_CUDA(c, cudaMemcpy(mip, sl.mip, sizeof(float) * n, cudaMemcpyDeviceToHost));
+    if (best_psi || best_theta || best_phi) {
+        std::vector<int> best(n);
+        TM_CUDA(c, cudaMemcpy(best.data(), sl.best, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        // planes are in increasing base order: binary search for the plane of each index
+        std::vector<long long> bases(c->planes.size());
+        for (size_t k = 0; k < bases.size(); k++) bases[k] = c->planes[k].base;
+        for (size_t i = 0; i < n; i++) {
+            const int g = best[i];
+            float psi = 0, th = 0, ph = 0;
+            const auto it = std::upper_bound(bases.begin(), bases.end(), (long long)g);
+            if (g >= 0 && it != bases.begin()) {
+                const Plane& p = c->planes[(size_t)(it - bases.begin()) - 1];
+                const long long o = g - p.base;
+                if (o >= 0 && o < p.n) {
+                    const float* e = c->angle_lists[p.angles_id].data() + 3 * o;
+                    ph = e[0];
+                    th = e[1];
+                    psi = e[2];
+                }
+            }
+            if (best_psi) best_psi[i] = psi;
+            if (best_theta) best_theta[i] = th;
+            if (best_phi) best_phi[i] = ph;
+        }
+    }
+    return TM_OK;
+}
 
 int tm_destroy(tm_ctx* c) {
     if (!c) return TM_ERR_INVALID;

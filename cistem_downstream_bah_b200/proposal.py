@@ -436,7 +436,12 @@ def window_core(T):
 
 
 class WindowSearch:
-    """Fine search of proposed tiles on windows of the whitened micrograph."""
+    """Fine search of proposed tiles on windows of the whitened micrograph.
+    The windows form an image set of one search context; the fine orientations
+    are run one angular bin at a time over the windows that need that bin, so
+    the per-orientation slice and projection work is shared between them.
+    Within a window the bins go in increasing order (a tie between
+    orientations of different bins keeps the lower bin's)."""
 
     def __init__(self, ispec, X, Y, T, tspec, filt, angular, hmin, hstep, device=0):
         self.X, self.Y, self.T = X, Y, T
@@ -447,6 +452,7 @@ class WindowSearch:
         self.s = whitened_real(ispec, X, Y)
         self.filt = filt
         self.angular = angular
+        self.max_set = 128   # windows per image set (about 8 MB of device state each at 512^2)
         # 256 orientations per device pass: at these small boxes the per-pass costs weigh (1.4x over 32)
         self.sc = core.SearchCore(self.W, self.W, T, histogram_min_scaled=hmin, histogram_step_scaled=hstep,
                                   orientation_batch=256, device=device)
@@ -468,40 +474,44 @@ class WindowSearch:
         m = self.margin
 
         def prepare(entry):
-            """Orientations and spectrum of one window (host work, run ahead of the GPU)."""
+            """Bins and spectrum of one window (host work)."""
             (cy, cx), items = entry
             bins = set()
             for _, _, b in items:
                 bins.update(int(v) for v in b)
-            angles = self.angular.fine_angles[self.angular.orientations(sorted(bins))]
             x0, y0 = cx * C - T // 2 - m, cy * C - T // 2 - m
             # the used square keeps two pixels beyond the interior's reach on each side
             spec = window_spectrum(self.s, x0, y0, W, X * Y, (m - 2, W - m + 2))
-            return items, angles, spec, x0, y0
+            return items, bins, spec, x0, y0
 
         points = 0.0
         t0 = time.perf_counter()
         entries = sorted(groups.items())
-        with ThreadPoolExecutor(max_workers=1) as pool:
-            ahead = [pool.submit(prepare, e) for e in entries[:2]]
-            for i in range(len(entries)):
-                items, angles, spec, x0, y0 = ahead.pop(0).result()
-                if i + 2 < len(entries):
-                    ahead.append(pool.submit(prepare, entries[i + 2]))
-                self.sc.set_image(spec)
-                self.sc.reset()
-                self.sc.run_plane(self.filt, angles)   # the GIL is released while the GPU searches
-                r = self.sc.results()
-                points += float(len(angles)) * W * W
-                wm = r["mip"].reshape(W, W)
-                for ty, tx, _ in items:
-                    ys = slice(ty * TILE, (ty + 1) * TILE)
-                    xs = slice(tx * TILE, (tx + 1) * TILE)
-                    wy = slice(ty * TILE - y0, (ty + 1) * TILE - y0)
-                    wx = slice(tx * TILE - x0, (tx + 1) * TILE - x0)
-                    mip[ys, xs] = wm[wy, wx]
-                    for k in ang:
-                        ang[k][ys, xs] = r[k].reshape(W, W)[wy, wx]
+        with ThreadPoolExecutor(max_workers=4) as pool:
+            for c0 in range(0, len(entries), self.max_set):
+                chunk = list(pool.map(prepare, entries[c0:c0 + self.max_set]))
+                # one image set per chunk of windows; each angular bin's orientations are
+                # sliced and projected once and correlated with every window that needs the bin
+                self.sc.set_image_set(np.stack([e[2] for e in chunk]))
+                by_bin = {}
+                for wi, (_, bins, _, _, _) in enumerate(chunk):
+                    for b in bins:
+                        by_bin.setdefault(b, []).append(wi)
+                for b in sorted(by_bin):
+                    angles = self.angular.fine_angles[self.angular.orientations([b])]
+                    self.sc.run_plane_images(self.filt, angles, by_bin[b])
+                    points += float(len(angles)) * W * W * len(by_bin[b])
+                for wi, (items, _, _, x0, y0) in enumerate(chunk):
+                    r = self.sc.image_results(wi)
+                    wm = r["mip"].reshape(W, W)
+                    for ty, tx, _ in items:
+                        ys = slice(ty * TILE, (ty + 1) * TILE)
+                        xs = slice(tx * TILE, (tx + 1) * TILE)
+                        wy = slice(ty * TILE - y0, (ty + 1) * TILE - y0)
+                        wx = slice(tx * TILE - x0, (tx + 1) * TILE - x0)
+                        mip[ys, xs] = wm[wy, wx]
+                        for k in ang:
+                            ang[k][ys, xs] = r[k].reshape(W, W)[wy, wx]
         return {"mip": mip, **ang, "points": points, "seconds": time.perf_counter() - t0, "windows": len(groups)}
 
     def close(self):

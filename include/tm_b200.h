@@ -119,8 +119,27 @@ TM_API int tm_template_spectrum(int device, const float *volume, int template_si
 TM_API int tm_set_normalization_pixels(tm_ctx *ctx, long long n_pixels);
 
 /* Clears the running MIP (to -FLT_MAX), best-orientation, sum, sum-of-squares
- * and histogram state, as RunInnerLoop does at entry (TemplateMatchingCore.cu:143-155). */
+ * and histogram state, as RunInnerLoop does at entry (TemplateMatchingCore.cu:143-155);
+ * also the results of the image set, if the context has one. */
 TM_API int tm_reset_results(tm_ctx *ctx);
+
+/* Image set (no counterpart in the reference): n_images micrograph spectra of
+ * the context's size (each laid out as for tm_set_image, one after another),
+ * each with its own running MIP / best orientation / sums / histogram.  Starts
+ * a new search (as tm_reset_results).  For many small searches that share
+ * orientations, e.g. the windows of the learned proposal. */
+TM_API int tm_set_image_set(tm_ctx *ctx, int n_images, const float *spectra);
+
+/* tm_run_plane over the images of the set listed in `images`: each orientation
+ * batch is sliced, projected and normalised once and correlated with every
+ * listed image.  Every call registers its orientations as one plane. */
+TM_API int tm_run_plane_images(tm_ctx *ctx, const float *projection_filter, const float *euler_angles,
+                               int n_orientations, const int *images, int n_images, float defocus_offset,
+                               float pixel_size_offset);
+
+/* MIP and best angles of one image of the set ([y][x], any pointer may be NULL). */
+TM_API int tm_get_image_results(tm_ctx *ctx, int image, float *mip, float *best_psi, float *best_theta,
+                                float *best_phi);
 
 /* Replaces TemplateMatchingCore::RunInnerLoop (TemplateMatchingCore.cu:140-368)
  * for one (pixel size, defocus) plane: for every orientation in order,

@@ -186,3 +186,43 @@ def test_normalization_pixels_argument():
         sc.set_normalization_pixels(0)
     finally:
         sc.close()
+
+
+def test_image_set_matches_single_images():
+    """Three windows in one image set, bins run over different subsets of them,
+    give the maps of the same windows searched one at a time."""
+    T, N, W = 64, 1024, 256
+    vol = synthetic.template_volume(T, 1.5, 3000, 40.0, seed=9)
+    mic, _ = synthetic.micrograph(N, N, 1.5, 3000, 40.0, 6, 0.05, 12000.0, seed=10, atom_seed=9)
+    ispec, curve = hostprep.whiten(mic)
+    tspec = hostprep.template_spectrum(vol)
+    filt = hostprep.projection_filter(T, curve, kv=300.0, cs_mm=2.7, amplitude_contrast=0.07, defocus1=12000.0,
+                                      defocus2=12000.0, pixel_size=1.5)
+    s = PR.whitened_real(ispec, N, N)
+    spectra = np.stack([PR.window_spectrum(s, x0, y0, W, N * N, (30, W - 30)) for x0, y0 in
+                        [(0, 0), (300, 500), (-100, 900)]])
+    ab = PR.AngularBins(7.5, 2.5, 6.0)
+    ba, bb = ab.nearest(PR.directions(10.0, 50.0), 2)
+    ang = {b: ab.fine_angles[ab.orientations([b])] for b in (ba, bb)}
+    plan = [[ba], [ba, bb], [bb]]
+    hmin, hstep = prep.histogram_scaled(N, N)
+    sc = core.SearchCore(W, W, T, histogram_min_scaled=hmin, histogram_step_scaled=hstep, orientation_batch=64)
+    try:
+        sc.set_template(tspec)
+        sc.set_normalization_pixels(N * N)
+        sc.set_image_set(spectra)
+        sc.run_plane_images(filt, ang[ba], [0, 1])
+        sc.run_plane_images(filt, ang[bb], [1, 2])
+        got = [sc.image_results(k) for k in range(3)]
+        for k, bins in enumerate(plan):
+            sc.set_image(spectra[k])
+            sc.reset()
+            for b in bins:
+                sc.run_plane(filt, ang[b])
+            ref = sc.results()
+            for key in ("mip", "psi", "theta", "phi"):
+                assert np.array_equal(got[k][key], ref[key]), (k, key)
+        with pytest.raises(core.TmError):
+            sc.run_plane_images(filt, ang[ba], [3])
+    finally:
+        sc.close()
