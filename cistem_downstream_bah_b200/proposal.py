@@ -443,7 +443,8 @@ class WindowSearch:
     Within a window the bins go in increasing order (a tie between
     orientations of different bins keeps the lower bin's)."""
 
-    def __init__(self, ispec, X, Y, T, tspec, filt, angular, hmin, hstep, device=0):
+    def __init__(self, ispec, X, Y, T, tspec, filt, angular, hmin, hstep, device=0, context=None):
+        """context: a search context of the window geometry to use instead of a new one."""
         self.X, self.Y, self.T = X, Y, T
         self.W = window_size(T)
         self.core = window_core(T)
@@ -454,8 +455,9 @@ class WindowSearch:
         self.angular = angular
         self.max_set = 128   # windows per image set (about 8 MB of device state each at 512^2)
         # 256 orientations per device pass: at these small boxes the per-pass costs weigh (1.4x over 32)
-        self.sc = core.SearchCore(self.W, self.W, T, histogram_min_scaled=hmin, histogram_step_scaled=hstep,
-                                  orientation_batch=256, device=device)
+        self.sc = context if context is not None else core.SearchCore(
+            self.W, self.W, T, histogram_min_scaled=hmin, histogram_step_scaled=hstep, orientation_batch=256,
+            device=device)
         self.sc.set_template(tspec)
         self.sc.set_normalization_pixels(X * Y)
 

@@ -198,3 +198,76 @@ def test_case_parameters_follow_the_training_distribution():
         assert 0.02 <= c["snr"] <= 0.08 and 5000.0 <= c["defocus"] <= 25000.0
         assert c["radius_A"] <= 0.45 * c["T"] * c["pixel_size"]
         assert c == PT.case_params(seed)    # seeded
+
+
+class _RecordingContext:
+    """Stands in for the window-geometry search context: records the calls and
+    returns, per window, a MIP that encodes (window, pixel) and angles that
+    encode the number of bins the window was searched with."""
+
+    def __init__(self, W):
+        self.W = W
+        self.calls = []
+
+    def set_template(self, tspec):
+        pass
+
+    def set_normalization_pixels(self, n):
+        self.norm = n
+
+    def set_image_set(self, spectra):
+        self.n = len(spectra)
+        self.runs = [0] * self.n
+        self.orient = [0] * self.n
+
+    def run_plane_images(self, filt, angles, images):
+        self.calls.append((len(angles), list(images)))
+        for k in images:
+            self.runs[k] += 1
+            self.orient[k] += len(angles)
+
+    def image_results(self, k):
+        W = self.W
+        mip = (1000.0 * k + np.arange(W * W)).astype(np.float32)
+        return {"mip": mip, "psi": np.full(W * W, self.runs[k], np.float32),
+                "theta": np.full(W * W, self.orient[k], np.float32), "phi": np.zeros(W * W, np.float32)}
+
+
+def test_window_search_host_logic():
+    X = Y = 1024
+    T = 64
+    spec = np.zeros((Y, X // 2 + 1), np.complex64)
+    ab = PR.AngularBins(15.0, 7.5, 30.0)
+    ctx = _RecordingContext(PR.window_size(T))
+    ws = PR.WindowSearch(spec, X, Y, T, None, np.zeros((T, T // 2 + 1), np.float32), ab, 0.0, 1.0, context=ctx)
+    assert ctx.norm == X * Y
+    gx = X // PR.TILE
+    C = PR.window_core(T)
+    tiles = [0, 1, 5, gx + 1, gx * gx - 1]
+    bins = [[0, 1], [1, 2], [3], [2], [4, 0]]
+    res = ws.run(PR.Proposal(tiles, bins, None))
+    # tiles 0, 1 and gx+1 share the first window (core C = 128 px = 2 tiles)
+    assert res["windows"] == 3
+    per_bin = {b: len(ab.orientations([b])) for b in range(5)}
+    # windows in (core row, core column) order: 0 = tiles 0, 1, gx+1; 1 = tile 5; 2 = the last tile;
+    # one call per bin, over the windows that need it, bins in increasing order
+    assert ctx.calls == [(per_bin[0], [0, 2]), (per_bin[1], [0]), (per_bin[2], [0]), (per_bin[3], [1]),
+                         (per_bin[4], [2])]
+    # each window's orientations: the union of its tiles' bins, each bin once
+    want = [sum(per_bin[b] for b in {0, 1, 2}), sum(per_bin[b] for b in {3}), sum(per_bin[b] for b in {0, 4})]
+    assert ctx.orient == want
+    assert res["points"] == float(sum(want)) * ctx.W * ctx.W
+    # placement: tile (ty, tx) of window k holds that window's pixels at (y - y0, x - x0)
+    m = PR.window_size(T) - C - T
+    for t, k in zip(tiles, [0, 0, 1, 0, 2]):
+        ty, tx = divmod(t, gx)
+        cy, cx = ty // (C // PR.TILE), tx // (C // PR.TILE)
+        x0, y0 = cx * C - T // 2 - m // 2, cy * C - T // 2 - m // 2
+        y, x = ty * PR.TILE + 5, tx * PR.TILE + 7
+        assert res["mip"][y, x] == 1000.0 * k + (y - y0) * ctx.W + (x - x0)
+        assert res["theta"][y, x] == want[k]
+    untouched = np.ones((Y, X), bool)
+    for t in tiles:
+        ty, tx = divmod(t, gx)
+        untouched[ty * 64:ty * 64 + 64, tx * 64:tx * 64 + 64] = False
+    assert np.all(np.isneginf(res["mip"][untouched]))
