@@ -575,7 +575,7 @@ def run_proposal(args):
     fine grid 2.5 / 1.5 deg): coarse search (7.5 / 5 deg) -> network over the
     64 x 64 tiles -> window search of the proposed tiles over the fine
     orientations of their 16 angular bins.  The exhaustive fine search runs
-    after it and judges recall of its z >= 7 peaks.  value = the exhaustive
+    after it; recall is measured on its z >= 7 peaks.  value = the exhaustive
     search's points / the proposal path's time (host buffers in and out,
     synchronous calls); the same for the method without the network
     (thresholded coarse z, bins around the coarse best direction)."""
