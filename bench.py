@@ -618,6 +618,10 @@ def run_proposal(args):
         res = ws.run(prop)
         t3 = time.perf_counter()
     t_prop = t3 - t0
+    # this library's kernels in the timed path: 6 per orientation batch of the coarse search (its
+    # results reset: 1), 9 per network forward call, and the window search's own count
+    n_launch_coarse = 1 + 6 * -(-len(coarse_angles) // sc.orientation_batch())
+    n_launch_net = 9 * -(-len(feats) // 256)
     # the method without the network at the network's tile budget (timed the same way)
     t4 = time.perf_counter()
     top = PR.propose_top_tiles(coarse, len(prop.tiles), angular)
@@ -689,7 +693,7 @@ def run_proposal(args):
                                                "speedup_vs_exhaustive": exh["seconds"] / t_top},
                 "without_network_threshold": {"tiles": int(len(heur.tiles)), "z_threshold": heur_thr},
                 "network_logit_threshold": net_thr},
-            "gpu_launches": None, "clocks": clk.summary()}), flush=True)
+            "gpu_launches": n_launch_coarse + n_launch_net + res["launches"], "clocks": clk.summary()}), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -454,6 +454,7 @@ class WindowSearch:
         self.filt = filt
         self.angular = angular
         self.max_set = 128   # windows per image set (about 8 MB of device state each at 512^2)
+        self._slots = 0      # images in the context's current set
         # 256 orientations per device pass: at these small boxes the per-pass costs weigh (1.4x over 32)
         self.sc = context if context is not None else core.SearchCore(
             self.W, self.W, T, histogram_min_scaled=hmin, histogram_step_scaled=hstep, orientation_batch=256,
@@ -487,6 +488,8 @@ class WindowSearch:
             return items, bins, spec, x0, y0
 
         points = 0.0
+        launches = 0
+        B = self.sc.orientation_batch() if hasattr(self.sc, "orientation_batch") else 256
         t0 = time.perf_counter()
         entries = sorted(groups.items())
         with ThreadPoolExecutor(max_workers=4) as pool:
@@ -495,6 +498,9 @@ class WindowSearch:
                 # one image set per chunk of windows; each angular bin's orientations are
                 # sliced and projected once and correlated with every window that needs the bin
                 self.sc.set_image_set(np.stack([e[2] for e in chunk]))
+                # the results reset (main state and the previous set), then per image: prepare, reset
+                launches += 1 + self._slots + 2 * len(chunk)
+                self._slots = len(chunk)
                 by_bin = {}
                 for wi, (_, bins, _, _, _) in enumerate(chunk):
                     for b in bins:
@@ -503,6 +509,8 @@ class WindowSearch:
                     angles = self.angular.fine_angles[self.angular.orientations([b])]
                     self.sc.run_plane_images(self.filt, angles, by_bin[b])
                     points += float(len(angles)) * W * W * len(by_bin[b])
+                    # per orientation batch: slice, rows, normalisation, pass A; passes B and C per window
+                    launches += -(-len(angles) // B) * (4 + 2 * len(by_bin[b]))
                 for wi, (items, _, _, x0, y0) in enumerate(chunk):
                     r = self.sc.image_results(wi)
                     wm = r["mip"].reshape(W, W)
@@ -514,7 +522,8 @@ class WindowSearch:
                         mip[ys, xs] = wm[wy, wx]
                         for k in ang:
                             ang[k][ys, xs] = r[k].reshape(W, W)[wy, wx]
-        return {"mip": mip, **ang, "points": points, "seconds": time.perf_counter() - t0, "windows": len(groups)}
+        return {"mip": mip, **ang, "points": points, "seconds": time.perf_counter() - t0, "windows": len(groups),
+                "launches": launches}
 
     def close(self):
         self.sc.close()
