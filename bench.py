@@ -645,7 +645,7 @@ def run_proposal(args):
         dg = PR.peak_diagnostics(pk, exh, coarse, {"network": prop, "top_tiles": top, "threshold": heur,
                                                    "network_all": allnet, "coarse_all": alltop}, angular)
         diags[key] = dg
-        ptiles = [(int(p[1]) // PR.TILE) * (X // PR.TILE) + int(p[0]) // PR.TILE for p in pk]
+        ptiles = [(int(p[1]) // PR.TILE) * PR.tile_grid(X, Y)[1] + int(p[0]) // PR.TILE for p in pk]
         curves = {"network": PR.tiles_for_recall(ptiles, dg["network_all_recovered"],
                                                  np.argsort(-out[:, 0], kind="stable")),
                   "coarse_z": PR.tiles_for_recall(ptiles, dg["coarse_all_recovered"],

@@ -211,7 +211,16 @@ def search_maps(sc, filt, angles, X, Y):
 
 
 def tile_grid(nx, ny, tile=TILE):
-    return ny // tile, nx // tile
+    """Tile rows and columns; the last ones may be partial."""
+    return -(-ny // tile), -(-nx // tile)
+
+
+def pad_to_tiles(a, fill, tile=TILE):
+    """A map padded (bottom and right, with fill) to whole tiles."""
+    gy, gx = tile_grid(a.shape[1], a.shape[0], tile)
+    out = np.full((gy * tile, gx * tile), fill, np.float32)
+    out[:a.shape[0], :a.shape[1]] = a
+    return out
 
 
 def frame(d):
@@ -257,9 +266,10 @@ def tile_features(z, theta, phi, tile=TILE, frames=None):
     def tiles(a):   # (gy*tile, gx*tile, ...) -> (n, P, ...)
         return a.reshape(gy, tile, gx, tile, *a.shape[2:]).swapaxes(1, 2).reshape(n, P, *a.shape[2:])
 
-    zc = np.clip(np.asarray(z[:gy * tile, :gx * tile], np.float32), -4.0, 12.0)
-    th = np.radians(np.asarray(theta[:gy * tile, :gx * tile], np.float32))
-    ph = np.radians(np.asarray(phi[:gy * tile, :gx * tile], np.float32))
+    # partial tiles: padding reads as z at the clip floor, weight 0, direction +z
+    zc = np.clip(pad_to_tiles(z, -4.0, tile), -4.0, 12.0)
+    th = np.radians(pad_to_tiles(theta, 0.0, tile))
+    ph = np.radians(pad_to_tiles(phi, 0.0, tile))
     st = np.sin(th)
     d = tiles(np.stack([st * np.cos(ph), st * np.sin(ph), np.cos(th)], axis=-1))          # (n, P, 3)
     d = np.matmul(d, np.asarray(frames, np.float32).transpose(0, 2, 1))                    # rows R d
@@ -369,7 +379,7 @@ def tiles_for_recall(peak_tiles, recoverable, ranking, levels=(0.9, 0.95, 0.99, 
 def tile_max(z, tile=TILE):
     ny, nx = z.shape
     gy, gx = tile_grid(nx, ny, tile)
-    zt = z[:gy * tile, :gx * tile].reshape(gy, tile, gx, tile).transpose(0, 2, 1, 3).reshape(gy * gx, tile * tile)
+    zt = pad_to_tiles(z, -np.inf, tile).reshape(gy, tile, gx, tile).transpose(0, 2, 1, 3).reshape(gy * gx, tile * tile)
     return zt.max(axis=1), zt.argmax(axis=1)
 
 
@@ -466,7 +476,7 @@ class WindowSearch:
         """MIP / best angles over the proposed tiles (-inf elsewhere), with the
         number of correlation points and the device-side wall time."""
         X, Y, T, W, C = self.X, self.Y, self.T, self.W, self.core
-        gx = X // TILE
+        gx = tile_grid(X, Y)[1]
         per_core = C // TILE
         mip = np.full((Y, X), -np.inf, np.float32)
         ang = {k: np.zeros((Y, X), np.float32) for k in ("phi", "theta", "psi")}
@@ -515,10 +525,13 @@ class WindowSearch:
                     r = self.sc.image_results(wi)
                     wm = r["mip"].reshape(W, W)
                     for ty, tx, _ in items:
-                        ys = slice(ty * TILE, (ty + 1) * TILE)
-                        xs = slice(tx * TILE, (tx + 1) * TILE)
-                        wy = slice(ty * TILE - y0, (ty + 1) * TILE - y0)
-                        wx = slice(tx * TILE - x0, (tx + 1) * TILE - x0)
+                        # a partial last tile keeps its pixels inside the micrograph
+                        h = min(TILE, Y - ty * TILE)
+                        w = min(TILE, X - tx * TILE)
+                        ys = slice(ty * TILE, ty * TILE + h)
+                        xs = slice(tx * TILE, tx * TILE + w)
+                        wy = slice(ty * TILE - y0, ty * TILE - y0 + h)
+                        wx = slice(tx * TILE - x0, tx * TILE - x0 + w)
                         mip[ys, xs] = wm[wy, wx]
                         for k in ang:
                             ang[k][ys, xs] = r[k].reshape(W, W)[wy, wx]
@@ -577,7 +590,7 @@ def peak_diagnostics(peaks, exhaustive, coarse, proposals, angular, tile=TILE):
     orientation there).  Also the rank of the bin around the coarse best
     direction at the peak pixel itself."""
     Y, X = coarse["z"].shape
-    gx = X // tile
+    gx = tile_grid(X, Y, tile)[1]
     n = len(peaks)
     out = {"z": np.array([p[2] for p in peaks]), "x": np.array([p[0] for p in peaks]),
            "y": np.array([p[1] for p in peaks])}

@@ -271,3 +271,44 @@ def test_window_search_host_logic():
         ty, tx = divmod(t, gx)
         untouched[ty * 64:ty * 64 + 64, tx * 64:tx * 64 + 64] = False
     assert np.all(np.isneginf(res["mip"][untouched]))
+
+
+def test_partial_tiles_are_covered():
+    """Micrographs whose sides are not multiples of the tile (4096 x 3888, 5832 x 4096
+    in the uneven configurations) keep their last, partial tile row and column."""
+    rng = np.random.default_rng(6)
+    ny, nx = 100, 150
+    z = rng.standard_normal((ny, nx)).astype(np.float32)
+    th = rng.uniform(0, 180, z.shape).astype(np.float32)
+    ph = rng.uniform(0, 360, z.shape).astype(np.float32)
+    z[90, 140] = 11.0                                   # in the partial tile (1, 2)
+    assert PR.tile_grid(nx, ny) == (2, 3)
+    f = PR.tile_features(z, th, ph)
+    assert f.shape == (6, PR.FEATURES, 64, 64)
+    zmax, arg = PR.tile_max(z)
+    assert zmax[5] == 11.0 and divmod(int(arg[5]), 64) == (90 - 64, 140 - 128)
+    assert zmax[3] == z[64:, :64].max()
+    assert np.isclose(f[5, 0, 26, 12], 11.0 / 4.0)
+    assert np.all(f[5, 0, 36:, :] == -1.0) and np.all(f[5, 1:4, 36:, :] == 0.0)   # padding
+    lab = PR.tile_labels(np.array([[140, 90, 11.0, 20.0, 30.0, 0.0]]), nx, ny)
+    assert lab[5, 0] == 1.0
+    frames = PR.tile_frames(z, th, ph)
+    assert np.allclose(frames[5] @ PR.directions(ph[90, 140], th[90, 140]), [0, 0, 1], atol=1e-12)
+
+
+def test_window_search_partial_tiles():
+    X, Y = 1000, 900
+    T = 64
+    spec = np.zeros((Y, X // 2 + 1), np.complex64)
+    ab = PR.AngularBins(15.0, 7.5, 30.0)
+    ctx = _RecordingContext(PR.window_size(T))
+    ws = PR.WindowSearch(spec, X, Y, T, None, np.zeros((T, T // 2 + 1), np.float32), ab, 0.0, 1.0, context=ctx)
+    gy, gx = PR.tile_grid(X, Y)
+    last = gy * gx - 1                                   # the bottom-right partial tile
+    res = ws.run(PR.Proposal([last], [[0]], None))
+    ty, tx = divmod(last, gx)
+    h, w = Y - ty * 64, X - tx * 64
+    assert 0 < h < 64 and 0 < w < 64
+    assert np.all(np.isfinite(res["mip"][ty * 64:, tx * 64:]))
+    assert res["mip"].shape == (Y, X)
+    assert np.isneginf(res["mip"][:ty * 64, :]).all()
