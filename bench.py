@@ -410,9 +410,8 @@ def run_ours(args):
     dominant = "k_pass_b" if b_ms >= c_ms else "k_pass_c"
     alg_b = 8.0 * N * nb
     alg_c = 4.0 * N * nb
-    # DRAM bytes per launch from the committed ncu captures of this workload
-    # (profiles/k_pass_b_4096x4096_t256.md, profiles/k_pass_c_4096x4096_t256.md);
-    # they apply to the default workload and its batches only
+    # DRAM bytes per launch measured by ncu on this workload (dram__bytes_read.sum +
+    # dram__bytes_write.sum); they apply to the default workload and its batches only
     prof = PROFILED_TRAFFIC.get(nb) if (X, Y, T) == (4096, 4096, 256) else None
     if dominant == "k_pass_b":
         ach = alg_b / (b_launch_ms * 1e-3) / 1e9

@@ -594,13 +594,19 @@ k_pass_b(BatchArgs a, int n_items) {
 // --------------------------------------------------------------------------------------
 // k_pass_c: one block per row y; X/16 threads each own 16 pixels
 // (x = 2*(t + P*r) + h); loops over the batch keeping the per-pixel state in
-// registers.
+// registers.  The per-pixel sum and sum of squares are compensated (Kahan)
+// FP32 sums over the batch, added to the FP64 running sums once per batch; at
+// X = 4096 (256 threads, two blocks per SM, 128 registers) a thread parks the
+// compensation terms of both sums and its sums of squares in its TMEM lane
+// between orientations (columns 0-15, 16-31 and 32-47 of its 64).
 template <int X>
 struct PassC {
     static constexpr int H = X / 2;
     static constexpr int R = 8;
     static constexpr int P = H / R;                 // X/16 threads
     static constexpr int RSF = tmfft::padded_len(H);
+    static constexpr bool COMP_IN_TMEM = X >= 4096 && P % 32 == 0;
+    static constexpr uint32_t TMEM_COLS = 64 * ((P / 32 + 3) / 4);   // warps of a lane quadrant side by side
     // dynamic shared memory for a row pitch XP and `bins` histogram bins
     static size_t smem_bytes(int XP, int bins) { return 128 + sizeof(float2) * (2 * (size_t)XP + RSF) + 4 * (size_t)bins; }
 };
@@ -610,6 +616,8 @@ __global__ void __launch_bounds__(X / 16, 2)
 k_pass_c(BatchArgs a, int Y) {
     using PC = PassC<X>;
     constexpr int H = PC::H, P = PC::P;
+    constexpr bool kTm = PC::COMP_IN_TMEM;
+    static_assert(!kTm || PC::TMEM_COLS <= 256, "pass C TMEM columns");
     constexpr uint32_t kWaitLimit = 1u << 24;
     const int XP = a.XP;
     // rows of C stream in through 1-D bulk copies, double buffered: the copy
@@ -623,19 +631,36 @@ k_pass_c(BatchArgs a, int Y) {
     const int t = threadIdx.x;
     const int y = blockIdx.x;
     const uint32_t row_bytes = (uint32_t)XP * (uint32_t)sizeof(float2);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem_c + 64);
+    const int warp = t >> 5;
     if (t == 0) {
         tmptx::mbar_init(&mbar[0], 1);
         tmptx::mbar_init(&mbar[1], 1);
     }
+    if constexpr (kTm) {
+        if (warp == 0) {
+            tmptx::tmem_alloc(tmem_slot, PC::TMEM_COLS);
+            tmptx::tmem_relinquish();
+        }
+    }
     for (int b = t; b < a.hist_bins; b += P) shist[b] = 0u;
+    if constexpr (kTm) tmptx::tmem_fence_before_sync();
     __syncthreads();
+    if constexpr (kTm) tmptx::tmem_fence_after_sync();
+    // this thread's 64 TMEM columns (lane quadrant warp % 4)
+    const uint32_t tcomp = kTm ? *tmem_slot + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(64 * (warp >> 2)) : 0u;
     if (t == 0 && a.nb > 0) {
         tmptx::mbar_arrive_expect_tx(&mbar[0], row_bytes);
         tmptx::bulk_g2s(rows, a.C + (size_t)y * XP, row_bytes, &mbar[0]);
     }
     float mip[16];
     int best[16];
-    float fs[16], fq[16];
+    // per-pixel sum and sum of squares over the batch: compensated (Kahan) FP32,
+    // added to the FP64 running sums once per batch.  comp_regs[0..15] and
+    // comp_regs[16..31] are the compensation terms of the two sums (registers
+    // only when they are not parked in TMEM, as is fq_regs).
+    float fs[16];
+    float fq_regs[kTm ? 1 : 16];
     const size_t rowoff = (size_t)y * X;
 #pragma unroll
     for (int r = 0; r < 8; r++) {
@@ -645,13 +670,38 @@ k_pass_c(BatchArgs a, int Y) {
         mip[2 * r] = mv.x; mip[2 * r + 1] = mv.y;
         best[2 * r] = bv.x; best[2 * r + 1] = bv.y;
         fs[2 * r] = 0.f; fs[2 * r + 1] = 0.f;
-        fq[2 * r] = 0.f; fq[2 * r + 1] = 0.f;
+    }
+    // the compensation terms: in registers, or parked in TMEM between orientations
+    float comp_regs[kTm ? 1 : 32];
+    if constexpr (kTm) {
+        float z[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) z[i] = 0.f;
+        tmptx::tmem_st16(tcomp, z);
+        tmptx::tmem_st16(tcomp + 16, z);
+        tmptx::tmem_st16(tcomp + 32, z);
+        tmptx::tmem_wait_st();
+    } else {
+#pragma unroll
+        for (int i = 0; i < (kTm ? 1 : 32); i++) comp_regs[i] = 0.f;
+#pragma unroll
+        for (int i = 0; i < (kTm ? 1 : 16); i++) fq_regs[i] = 0.f;
     }
     auto sync = [] __device__() { __syncthreads(); };
+    // Copy o goes to buffer o & 1 and completes phase o >> 1 of that buffer's
+    // mbarrier.  After a wait runs out the block stops issuing copies and, before
+    // it exits, waits for the copies still in flight at the parity of the phase
+    // each one completes (bounded again).
+    auto drain = [&](int o) {
+        tmptx::mbar_wait_bounded(&mbar[(o - 1) & 1], ((o - 1) >> 1) & 1, kWaitLimit);   // the wait that ran out
+        if (o < a.nb) tmptx::mbar_wait_bounded(&mbar[o & 1], (o >> 1) & 1, kWaitLimit);   // issued at o - 1
+    };
     bool timed_out = false;
-    for (int o = 0; o < a.nb; o++) {
+    int o = 0;
+    for (; o < a.nb; o++) {
         const int buf = o & 1;
-        __syncthreads();  // iteration o-1 is done with row buffer buf ^ 1
+        // iteration o-1 is done with row buffer buf ^ 1; every thread learns whether a wait ran out
+        if (__syncthreads_or(timed_out)) break;
         if (t == 0 && o + 1 < a.nb) {
             tmptx::mbar_arrive_expect_tx(&mbar[buf ^ 1], row_bytes);
             tmptx::bulk_g2s(rows + (buf ^ 1) * XP, a.C + ((size_t)(o + 1) * Y + y) * XP, row_bytes, &mbar[buf ^ 1]);
@@ -676,24 +726,75 @@ k_pass_c(BatchArgs a, int Y) {
         // the barrier at the top of the iteration follows the last reads of fbuf
         tmfft::fft<H, 8, +1, false>(v, t, fbuf, a.tw, sync);
         const int g = (int)(a.gidx0 + o);
+        // epilogue in two sweeps over the 16 values, so that only one sum's 16
+        // compensation terms are live at a time: (1) MIP / argmax, histogram and
+        // the sum, (2) the sum of squares
+        float comp_tm[kTm ? 32 : 1];
 #pragma unroll
-        for (int r = 0; r < 8; r++) {
+        for (int sweep = 0; sweep < 2; sweep++) {
+            float* comp = comp_regs + (kTm ? 0 : 16 * sweep);
+            float* fq = fq_regs;
+            if constexpr (kTm) {
+                // sweep 0: the sum's compensation; sweep 1: the sum of squares and its compensation
+                tmptx::tmem_ld16(tcomp + 16 * sweep, comp_tm);
+                if (sweep == 1) tmptx::tmem_ld16(tcomp + 32, comp_tm + 16);
+                tmptx::tmem_wait_ld32(comp_tm);
+                comp = comp_tm;
+                fq = comp_tm + 16;
+            }
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const float val = h ? v[r].y : v[r].x;
-                const int pi = 2 * r + h;
-                if (val > mip[pi]) { mip[pi] = val; best[pi] = g; }
-                fs[pi] += val;
-                fq[pi] = fmaf(val, val, fq[pi]);
-                const int bin = __float2int_rz((val - a.hist_min) * a.hist_inv_step);
-                if (bin >= 0 && bin < a.hist_bins) atomicAdd(&shist[bin], 1u);
+            for (int r = 0; r < 8; r++) {
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const float val = h ? v[r].y : v[r].x;
+                    const int pi = 2 * r + h;
+                    // Kahan: the compensation holds what the last addition added beyond its input
+                    if (sweep == 0) {
+                        if (val > mip[pi]) { mip[pi] = val; best[pi] = g; }
+                        const float ys = val - comp[pi];
+                        const float ts = fs[pi] + ys;
+                        comp[pi] = (ts - fs[pi]) - ys;
+                        fs[pi] = ts;
+                        const int bin = __float2int_rz((val - a.hist_min) * a.hist_inv_step);
+                        if (bin >= 0 && bin < a.hist_bins) atomicAdd(&shist[bin], 1u);
+                    } else {
+                        const float yq = fmaf(val, val, -comp[pi]);
+                        const float tq = fq[pi] + yq;
+                        comp[pi] = (tq - fq[pi]) - yq;
+                        fq[pi] = tq;
+                    }
+                }
+            }
+            if constexpr (kTm) {
+                tmptx::tmem_st16(tcomp + 16 * sweep, comp_tm);
+                if (sweep == 1) tmptx::tmem_st16(tcomp + 32, comp_tm + 16);
+                tmptx::tmem_wait_st();
             }
         }
     }
-    if (timed_out) {
-        // leave no bulk copy in flight into this block's shared memory
-        tmptx::mbar_wait_bounded(&mbar[0], 0, kWaitLimit);
-        tmptx::mbar_wait_bounded(&mbar[1], 0, kWaitLimit);
+    // the compensation terms (and sums of squares) for the FP64 flush
+    float comp_end[kTm ? 48 : 1];
+    const float* cend = comp_regs;
+    const float* fqend = fq_regs;
+    if constexpr (kTm) {
+        tmptx::tmem_ld16(tcomp, comp_end);
+        tmptx::tmem_ld16(tcomp + 16, comp_end + 16);
+        tmptx::tmem_wait_ld32(comp_end);
+        tmptx::tmem_ld16(tcomp + 32, comp_end + 32);
+        tmptx::tmem_wait_ld16(comp_end + 32);
+        cend = comp_end;
+        fqend = comp_end + 32;
+        tmptx::tmem_fence_before_sync();
+    }
+    const bool failed = __syncthreads_or(timed_out);
+    if constexpr (kTm) {
+        // every warp has finished with its TMEM columns (the barrier above)
+        tmptx::tmem_fence_after_sync();
+        if (warp == 0) tmptx::tmem_dealloc(*tmem_slot, PC::TMEM_COLS);
+    }
+    if (failed) {
+        // results of this block are discarded (the host reports the timeout)
+        drain(o);
         return;
     }
 #pragma unroll
@@ -703,8 +804,10 @@ k_pass_c(BatchArgs a, int Y) {
         *reinterpret_cast<int2*>(a.best + rowoff + x) = make_int2(best[2 * r], best[2 * r + 1]);
         double2 sv = *reinterpret_cast<const double2*>(a.sum + rowoff + x);
         double2 qv = *reinterpret_cast<const double2*>(a.sumsq + rowoff + x);
-        sv.x += (double)fs[2 * r]; sv.y += (double)fs[2 * r + 1];
-        qv.x += (double)fq[2 * r]; qv.y += (double)fq[2 * r + 1];
+        sv.x += (double)fs[2 * r] - (double)cend[2 * r];
+        sv.y += (double)fs[2 * r + 1] - (double)cend[2 * r + 1];
+        qv.x += (double)fqend[2 * r] - (double)cend[16 + 2 * r];
+        qv.y += (double)fqend[2 * r + 1] - (double)cend[16 + 2 * r + 1];
         *reinterpret_cast<double2*>(a.sum + rowoff + x) = sv;
         *reinterpret_cast<double2*>(a.sumsq + rowoff + x) = qv;
     }

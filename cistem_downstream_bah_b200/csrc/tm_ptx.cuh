@@ -95,6 +95,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
         : "r"(taddr)
         : "memory");
 }
+// 32 consecutive 32-bit columns of this thread's lane (as two x16 accesses)
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float* v) {
+    tmem_st16(taddr, v);
+    tmem_st16(taddr + 16, v + 16);
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+    tmem_ld16(taddr, v);
+    tmem_ld16(taddr + 16, v + 16);
+}
 // 4 consecutive 32-bit columns of this thread's lane
 __device__ __forceinline__ void tmem_st4(uint32_t taddr, const float* v) {
     asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "f"(v[0]), "f"(v[1]),
@@ -115,6 +124,16 @@ __device__ __forceinline__ void tmem_wait_ld16(float* v) {
     asm volatile("tcgen05.wait::ld.sync.aligned;"
                  : "+f"(v[0]), "+f"(v[1]), "+f"(v[2]), "+f"(v[3]), "+f"(v[4]), "+f"(v[5]), "+f"(v[6]), "+f"(v[7]),
                    "+f"(v[8]), "+f"(v[9]), "+f"(v[10]), "+f"(v[11]), "+f"(v[12]), "+f"(v[13]), "+f"(v[14]), "+f"(v[15])
+                 :
+                 : "memory");
+}
+// the wait with the 32 destination registers of an earlier tmem_ld32 tied to it
+__device__ __forceinline__ void tmem_wait_ld32(float* v) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+f"(v[0]), "+f"(v[1]), "+f"(v[2]), "+f"(v[3]), "+f"(v[4]), "+f"(v[5]), "+f"(v[6]), "+f"(v[7]),
+                   "+f"(v[8]), "+f"(v[9]), "+f"(v[10]), "+f"(v[11]), "+f"(v[12]), "+f"(v[13]), "+f"(v[14]), "+f"(v[15]),
+                   "+f"(v[16]), "+f"(v[17]), "+f"(v[18]), "+f"(v[19]), "+f"(v[20]), "+f"(v[21]), "+f"(v[22]), "+f"(v[23]),
+                   "+f"(v[24]), "+f"(v[25]), "+f"(v[26]), "+f"(v[27]), "+f"(v[28]), "+f"(v[29]), "+f"(v[30]), "+f"(v[31])
                  :
                  : "memory");
 }

@@ -188,9 +188,8 @@ TM_API int tm_debug_stage_buffers(tm_ctx *ctx, const float *projection_filter, c
 
 /* Plane search that allocates no device memory, for callers that cannot call
  * cudaMalloc: code inside a host framework that owns every device allocation
- * through its own pool, plugins that are only handed pre-allocated buffers,
- * and code that must not allocate while a stream is being captured.  It has no
- * counterpart in the reference.
+ * through its own pool, and plugins that are only handed pre-allocated
+ * buffers.  It has no counterpart in the reference.
  *
  * Same search as tm_run_plane, on the caller's device buffers: the template
  * spectrum (as tm_set_template), the whitened micrograph spectrum (as
@@ -201,16 +200,16 @@ TM_API int tm_debug_stage_buffers(tm_ctx *ctx, const float *projection_filter, c
  * image_y*image_x ([y][x]) or histogram_bins long.  euler_angles is host
  * memory, n_orientations (phi, theta, psi) triples.  The work is ordered on
  * `stream` (a cudaStream_t; NULL = the default stream) and the call returns
- * when it is done.
+ * when it is done.  The caller's current device is restored before return.
  *
  * All intermediates live in one fixed device array of 16 MiB, which every GPU
- * that loads this library holds until the process exits; geometries whose
- * intermediates exceed it, and geometries without a compiled variant (template
- * 32 on 256x256 or 512x512, template 64 on 512x512), return TM_ERR_UNSUPPORTED.
- * The first call on a device looks up that array's device address and sets
- * kernel attributes, so make it before any stream capture.  Every call reuses
- * the same array: calls that overlap on the GPU (other streams, other host
- * threads) race and corrupt each other's results. */
+ * that loads this library holds until the process exits.  The compiled
+ * geometries (template 32 on 256x256 or 512x512, template 64 on 512x512) all
+ * fit it; any other geometry returns TM_ERR_UNSUPPORTED.  The first call on a
+ * device looks up that array's device address and sets kernel attributes, so
+ * make it before any stream capture.  Every call reuses the same array: calls
+ * that overlap on the GPU (other streams, other host threads) race and corrupt
+ * each other's results. */
 TM_API int tm_run_plane_noalloc(int device, const tm_dims *dims, const float *d_template_spectrum,
                                 const float *d_image_spectrum, const float *d_projection_filter,
                                 const float *euler_angles, int n_orientations, int first_orientation_index,

@@ -8,7 +8,7 @@ parses those arrays out of the reference sources and writes the same bytes to
 tests/golden/*.mrc.  It needs the reference tree, so it runs only where the
 reference is mounted; the .mrc outputs are committed.
 
-Usage: python tests/golden/make_console_fixtures.py [/path/to/reference]
+Usage: python tests/golden/make_console_fixtures.py <path of the cisTEM source tree>
 """
 import os
 import re
@@ -23,7 +23,9 @@ FILES = {
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_console_fixtures.py <path of the cisTEM source tree>")
+    ref = sys.argv[1]
     src_dir = os.path.join(ref, "src", "programs", "console_test")
     for out_name, src_name in FILES.items():
         text = open(os.path.join(src_dir, src_name)).read()

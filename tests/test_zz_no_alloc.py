@@ -1,11 +1,11 @@
 """tm_run_plane_noalloc against the context entry points (needs a B200).
 
 The allocation-free entry point is for callers that cannot call cudaMalloc
-(framework-owned memory pools, plugins given pre-allocated buffers, code
-that must not allocate during stream capture).  Here the caller's device
-buffers come from torch, which stands in for such a host allocator; the test
-runs two planes in a row through both entry points on the same inputs and
-compares every running result.  Tolerances are those of the parity tests:
+(framework-owned memory pools, plugins given pre-allocated buffers).  Here
+the caller's device buffers come from torch, which stands in for such a host
+allocator; the test runs two planes in a row through both entry points on
+the same inputs, for each compiled geometry, and compares every running
+result.  Tolerances are those of the parity tests:
 MIP within 1e-4 relative, sums within 1e-5 of their scale, histogram within
 0.1% (+2); best orientation and defocus identical on all but 0.1% of pixels
 (near-ties can resolve differently because the prepared micrograph spectrum
@@ -27,9 +27,10 @@ def _dev(torch, arr, dtype):
     return torch.from_numpy(np.ascontiguousarray(arr).view(dtype)).cuda()
 
 
-def test_noalloc_matches_context_entry_points_two_calls():
+@pytest.mark.parametrize("T,X,Y,step", [(32, 256, 256, 45.0), (32, 512, 512, 60.0), (64, 512, 512, 60.0)])
+def test_noalloc_matches_context_entry_points_two_calls(T, X, Y, step):
     torch = pytest.importorskip("torch")
-    case = make_case(T=32, X=256, Y=256, angular_step=45.0, psi_step=45.0)
+    case = make_case(T=T, X=X, Y=Y, angular_step=step, psi_step=step)
     X, Y, T = case["X"], case["Y"], case["T"]
     ang = case["angles"]
     half = len(ang) // 2
@@ -66,6 +67,7 @@ def test_noalloc_matches_context_entry_points_two_calls():
         rc = L.tm_run_plane_noalloc(0, ctypes.byref(dims), p(d_t), p(d_i), p(f), a.ctypes.data_as(ctypes.c_void_p),
                                     len(a), first, p(d_mip), p(d_best), p(d_sum), p(d_sq), p(d_hist), None)
         assert rc == core.TM_OK, rc
+        assert torch.cuda.current_device() == 0
         first += len(a)
     mip = d_mip.cpu().numpy()
     best = d_best.cpu().numpy()
@@ -92,7 +94,8 @@ def test_noalloc_matches_context_entry_points_two_calls():
 def test_noalloc_rejects_unsupported_geometry():
     torch = pytest.importorskip("torch")
     L = core.load()
-    dims = core.TmDims(4096, 4096, 256, 512, -0.003, 1e-5, 0, 0)   # intermediates exceed the fixed scratch
+    # no compiled no-alloc variant (its intermediates would not fit the fixed array)
+    dims = core.TmDims(4096, 4096, 256, 512, -0.003, 1e-5, 0, 0)
     buf = torch.zeros(16, dtype=torch.float64, device="cuda")
     p = ctypes.c_void_p(buf.data_ptr())
     a = np.zeros(3, np.float32)
