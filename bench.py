@@ -312,6 +312,8 @@ def run_ours(args):
     npix_orig = WORKLOAD["nx"] * WORKLOAD["ny"]
     sc = core.SearchCore(X, Y, T, histogram_min_scaled=inp["hmin"], histogram_step_scaled=inp["hstep"],
                          orientation_batch=args.batch, device=local)
+    precision = core.PRECISION_FP16_TENSOR if args.precision == "fp16" else core.PRECISION_FP32
+    sc.set_precision(precision)
     sc.set_template(inp["tspec"])
     sc.set_image(inp["ispec"])
     if args.batch == 0:
@@ -358,6 +360,8 @@ def run_ours(args):
     n_ctx = max(1, min(args.e2e_contexts, args.steps))
     ctxs = [sc] + [core.SearchCore(X, Y, T, histogram_min_scaled=inp["hmin"], histogram_step_scaled=inp["hstep"],
                                    orientation_batch=batch, device=local) for _ in range(n_ctx - 1)]
+    for c in ctxs[1:]:
+        c.set_precision(precision)
     bufs = []
     for _ in ctxs:
         outs = {k: pinned_copy(np.zeros(n, np.float32)) for k in ("mip", "psi", "theta", "phi", "defocus", "pixel")}
@@ -748,6 +752,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--orientations-per-step", type=int, default=1024)
     ap.add_argument("--batch", type=int, default=0, help="orientations per device pass; 0 = autotuned")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16"],
+                    help="fp32 = the parity path; fp16 = FP16 correlation spectra with the tensor-core row transform")
     ap.add_argument("--cpu-sample", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--accuracy", type=int, default=4,

@@ -26,6 +26,8 @@ TM_ERR_UNSUPPORTED = -3
 TM_ERR_OOM = -4
 TM_ERR_TIMEOUT = -5
 TM_ERR_CANCELLED = -6
+PRECISION_FP32 = 0
+PRECISION_FP16_TENSOR = 1
 
 EXPORTED = [
     "tm_create", "tm_set_template", "tm_set_image", "tm_reset_results", "tm_run_plane",
@@ -36,7 +38,7 @@ EXPORTED = [
     "tm_set_template_volume", "tm_template_spectrum", "tm_set_normalization_pixels", "tm_pnet_create",
     "tm_pnet_param_count", "tm_pnet_set_params", "tm_pnet_get_params", "tm_pnet_forward", "tm_pnet_gradients",
     "tm_pnet_train_step", "tm_pnet_last_error", "tm_pnet_destroy", "tm_set_image_set", "tm_run_plane_images",
-    "tm_get_image_results",
+    "tm_get_image_results", "tm_set_precision", "tm_get_precision",
 ]
 
 
@@ -110,6 +112,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.tm_set_image_set.argtypes = [vp, ip, vp]
     L.tm_run_plane_images.argtypes = [vp, vp, vp, ip, vp, ip, fp, fp]
     L.tm_get_image_results.argtypes = [vp, ip, vp, vp, vp, vp]
+    L.tm_set_precision.argtypes = [vp, ip]
+    L.tm_get_precision.argtypes = [vp]
     _LIB = L
     return L
 
@@ -151,6 +155,14 @@ class SearchCore:
         s = np.ascontiguousarray(spectrum, dtype=np.complex64)
         assert s.shape == (self.Y, self.X // 2 + 1), s.shape
         self._check(self.L.tm_set_image(self.h, _ptr(s), self.X, self.Y))
+
+    def set_precision(self, precision):
+        """PRECISION_FP32 (the parity path) or PRECISION_FP16_TENSOR (FP16
+        correlation spectra, tensor-core row transform; tm_set_precision)."""
+        self._check(self.L.tm_set_precision(self.h, int(precision)))
+
+    def precision(self):
+        return int(self.L.tm_get_precision(self.h))
 
     def set_template_volume(self, volume, pixel_size_factor=1.0):
         """Prepares the template spectrum on the device from the T^3 volume."""

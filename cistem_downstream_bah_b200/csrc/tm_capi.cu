@@ -61,6 +61,8 @@ struct tm_ctx {
     unsigned long long* hist = nullptr;
     int* err_flag = nullptr;
     int* best_host = nullptr;   // page-locked copy of the best-orientation map (tm_get_results)
+    int precision = TM_PRECISION_FP32;
+    uint4* dft = nullptr;       // DFT operands of the tensor-core row pass (FP16 form)
     long long rot_capacity = 0;
     bool has_template = false, has_image = false;
     // bookkeeping for decoding the argmax
@@ -117,6 +119,14 @@ struct WhitenBuffers {
 };
 using WhitenFn = int (*)(cudaStream_t, int nsm, const WhitenBuffers&, std::vector<double>& curve, std::string& err);
 
+// The FP16 tensor-core form of a geometry (tm_set_precision).
+struct TensorForm {
+    int (*configure)(tm_ctx*);
+    int (*run_batch)(tm_ctx*, tmk::BatchArgs&, cudaEvent_t* ev);
+    size_t dft_bytes;                 // the row pass's DFT operands
+    void (*fill_dft)(uint16_t*);
+};
+
 struct Variant {
     int T, X, Y;
     int W;   // row pitch alignment of the pass-B column chunks (columns)
@@ -125,6 +135,7 @@ struct Variant {
     int (*run_stages)(tm_ctx*, tmk::BatchArgs&);   // every kernel before the MIP epilogue
     WhitenFn whiten;
     int (*run_batch_images)(tm_ctx*, tmk::BatchArgs&, const int* ids, int n_ids);   // image-set batch
+    const TensorForm* tc;   // null where the FP16 tensor-core form has no kernels
 };
 
 // number of points of the whitening curve (match_template.cpp:702)
@@ -254,9 +265,39 @@ struct Impl {
     }
 };
 
+template <int T, int X, int Y>
+struct TcImpl {
+    using LT = tmk::LaunchTc<T, X, Y>;
+    static int configure(tm_ctx* c) {
+        TM_CUDA(c, LT::configure(c->XP, c->d.histogram_bins));
+        return TM_OK;
+    }
+    // the FP16 form of a batch: the same slice and projection kernels, pass B
+    // with FP16 output, the tensor-core row pass
+    static int run_batch(tm_ctx* c, tmk::BatchArgs& a, cudaEvent_t* ev) {
+        using LN = tmk::Launch<T, X, Y>;
+        cudaStream_t s = c->stream;
+        if (ev) cudaEventRecord(ev[0], s);
+        LN::prep(a, s);
+        if (ev) cudaEventRecord(ev[1], s);
+        LT::pass_b(a, s, c->nsm);
+        if (ev) cudaEventRecord(ev[2], s);
+        LT::pass_c(a, s, c->dft);
+        if (ev) cudaEventRecord(ev[3], s);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return set_err(c, TM_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+        return TM_OK;
+    }
+    static constexpr TensorForm form = {&TcImpl::configure, &TcImpl::run_batch, LT::dft_bytes, &LT::fill_dft};
+};
+
 #define TM_VARIANT(T, X, Y)                                                                                 \
     {T, X, Y, tmk::Launch<T, X, Y>::pass_b_width, &Impl<T, X, Y>::run_batch, &Impl<T, X, Y>::configure,          \
-     &Impl<T, X, Y>::run_stages, &whiten_on_device<X, Y>, &Impl<T, X, Y>::run_batch_images}
+     &Impl<T, X, Y>::run_stages, &whiten_on_device<X, Y>, &Impl<T, X, Y>::run_batch_images, nullptr}
+// a geometry that also has the FP16 tensor-core form
+#define TM_VARIANT_TC(T, X, Y)                                                                              \
+    {T, X, Y, tmk::Launch<T, X, Y>::pass_b_width, &Impl<T, X, Y>::run_batch, &Impl<T, X, Y>::configure,          \
+     &Impl<T, X, Y>::run_stages, &whiten_on_device<X, Y>, &Impl<T, X, Y>::run_batch_images, &TcImpl<T, X, Y>::form}
 
 // Geometries with compiled kernels: template box T on a padded X x Y
 // micrograph.  X is a power of two (the reference turns a micrograph whose
@@ -271,26 +312,26 @@ const Variant kVariants[] = {
     TM_VARIANT(32, 256, 512),
     TM_VARIANT(32, 512, 512),
     TM_VARIANT(64, 512, 512),
-    TM_VARIANT(64, 1024, 1024),
-    TM_VARIANT(128, 1024, 1024),
-    TM_VARIANT(128, 2048, 2048),
-    TM_VARIANT(256, 2048, 2048),
-    TM_VARIANT(256, 4096, 4096),
-    TM_VARIANT(64, 4096, 4096),
+    TM_VARIANT_TC(64, 1024, 1024),
+    TM_VARIANT_TC(128, 1024, 1024),
+    TM_VARIANT_TC(128, 2048, 2048),
+    TM_VARIANT_TC(256, 2048, 2048),
+    TM_VARIANT_TC(256, 4096, 4096),
+    TM_VARIANT_TC(64, 4096, 4096),
     TM_VARIANT(32, 256, 288),
     TM_VARIANT(48, 256, 256),
     TM_VARIANT(48, 256, 288),
-    TM_VARIANT(256, 4096, 3888),
+    TM_VARIANT_TC(256, 4096, 3888),
     TM_VARIANT(256, 4096, 5832),
-    TM_VARIANT(384, 4096, 4096),
+    TM_VARIANT_TC(384, 4096, 4096),
     TM_VARIANT(384, 4096, 5832),
     // the same camera formats with smaller and larger templates
-    TM_VARIANT(128, 4096, 4096),
-    TM_VARIANT(128, 4096, 3888),
+    TM_VARIANT_TC(128, 4096, 4096),
+    TM_VARIANT_TC(128, 4096, 3888),
     TM_VARIANT(128, 4096, 5832),
-    TM_VARIANT(64, 4096, 3888),
+    TM_VARIANT_TC(64, 4096, 3888),
     TM_VARIANT(64, 4096, 5832),
-    TM_VARIANT(384, 4096, 3888),
+    TM_VARIANT_TC(384, 4096, 3888),
     // windows of the learned proposal's fine search (edge max(2T, 256))
     TM_VARIANT(64, 256, 256),
     TM_VARIANT(128, 256, 256),
@@ -331,7 +372,7 @@ int wait_stream(tm_ctx* c, double limit_s) {
 
 void free_all(tm_ctx* c) {
     void* ptrs[] = {c->tmpl, c->Ip, c->S, c->A, c->C, c->norm, c->twx, c->twy, c->twt, c->P, c->filter, c->rot,
-                    c->rowstat, c->mip, c->best, c->sum, c->sumsq, c->hist, c->err_flag};
+                    c->rowstat, c->mip, c->best, c->sum, c->sumsq, c->hist, c->err_flag, c->dft};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (tm_ctx::Slot& sl : c->slots) {
@@ -399,6 +440,9 @@ tmk::BatchArgs make_args(tm_ctx* c) {
     a.twy.lmax = c->Y;
     a.twt.tab = c->twt;
     a.twt.lmax = c->T;
+    // FP16 form: correlation spectra times 2^e with 2^e ~ sqrt(X Y), so that the
+    // row outputs (correlation values ~ 1/sqrt(X Y)) are O(1) in FP16
+    a.half_scale_exp = (int)lround(0.5 * log2((double)c->X * (double)c->Y));
     return a;
 }
 
@@ -934,6 +978,32 @@ int tm_set_normalization_pixels(tm_ctx* c, long long n_pixels) {
     return TM_OK;
 }
 
+int tm_set_precision(tm_ctx* c, int precision) {
+    if (!c) return TM_ERR_INVALID;
+    if (precision == TM_PRECISION_FP32) {
+        c->precision = precision;
+        return TM_OK;
+    }
+    if (precision != TM_PRECISION_FP16_TENSOR) return set_err(c, TM_ERR_INVALID, "unknown precision %d", precision);
+    if (!c->var->tc)
+        return set_err(c, TM_ERR_UNSUPPORTED, "no FP16 tensor-core form for template %d and image %d x %d", c->T, c->X, c->Y);
+    TM_CUDA(c, cudaSetDevice(c->device));
+    if (!c->dft) {
+        const size_t bytes = c->var->tc->dft_bytes;
+        std::vector<uint16_t> host(bytes / 2);
+        c->var->tc->fill_dft(host.data());
+        int rc = dalloc(c, &c->dft, bytes / sizeof(uint4));
+        if (rc != TM_OK) return rc;
+        TM_CUDA(c, cudaMemcpy(c->dft, host.data(), bytes, cudaMemcpyHostToDevice));
+        rc = c->var->tc->configure(c);
+        if (rc != TM_OK) return rc;
+    }
+    c->precision = precision;
+    return TM_OK;
+}
+
+int tm_get_precision(const tm_ctx* c) { return c ? c->precision : TM_ERR_INVALID; }
+
 int tm_reset_results(tm_ctx* c) {
     if (!c) return TM_ERR_INVALID;
     TM_CUDA(c, cudaSetDevice(c->device));
@@ -1003,7 +1073,9 @@ int tm_run_plane(tm_ctx* c, const float* projection_filter, const float* euler_a
         // read after the plane, so the stream never stalls for them)
         const int set = bi == 0 ? 0 : (bi == nbatch - 1 ? 1 : -1);
         if (set >= 0) timed_nb[set] = a.nb;
-        int rc = c->var->run_batch(c, a, set >= 0 ? c->ev_batch[set] : nullptr);
+        int rc = c->precision == TM_PRECISION_FP16_TENSOR
+                     ? c->var->tc->run_batch(c, a, set >= 0 ? c->ev_batch[set] : nullptr)
+                     : c->var->run_batch(c, a, set >= 0 ? c->ev_batch[set] : nullptr);
         if (rc != TM_OK) return rc;
         if (progress) {
             if (progress((long long)(a.orient0 + a.nb), (long long)n, user) != 0) {

@@ -28,6 +28,7 @@
 // (ClipIntoLargerRealSpace2D, image.cpp:8398-8465), the forward-FFT scaling
 // 1/N and the zeroed central pixel are folded into I' once per micrograph.
 #pragma once
+#include <cuda_fp16.h>
 #include <float.h>
 #include "tm_fft.cuh"
 #include "tm_ptx.cuh"
@@ -77,6 +78,7 @@ struct BatchArgs {
     float hist_min, hist_inv_step;
     int hist_bins;
     int* err;                     // device error flag (a bounded wait ran out)
+    int half_scale_exp;           // FP16 form: the correlation spectra are stored times 2^half_scale_exp
     long long norm_pixels;        // pixel count of the projection variance (0: X*Y, the box;
                                   // a window of a larger micrograph passes the micrograph's)
     int XP;                       // row pitch (complex values) of A, C and Ip: X/2+1 rounded
@@ -430,7 +432,12 @@ __device__ __forceinline__ void tmem_put_values(uint32_t taddr, const float* f) 
     }
 }
 
-template <int T, int Y>
+// RB = 0: C[o][y][kx] in FP32 complex.  RB > 0 (the FP16 form): C in FP16
+// complex times 2^half_scale_exp, rows interleaved in blocks of RB,
+// C16[o][y / RB][kx][y % RB], so that a warp's stores (8 consecutive rows of 4
+// columns) fill whole 32-byte sectors and the tensor-core row pass reads a
+// block of RB rows with one bulk copy.
+template <int T, int Y, int RB = 0>
 __global__ void __launch_bounds__(PassB<T, Y>::NT, 1)
 k_pass_b(BatchArgs a, int n_items) {
     using PB = PassB<T, Y>;
@@ -564,7 +571,15 @@ k_pass_b(BatchArgs a, int n_items) {
                 for (int r = 0; r < V; r++) v[r] = cmul_conj(__ldg(Ic + (size_t)(j + P * r) * XP), v[r]);
             }
             tmfft::fft<Y, V, +1>(v, j, colbuf, a.twy, sync);
-            if constexpr (G == 1) {
+            if constexpr (RB > 0) {
+                static_assert(G == 1 && Y % RB == 0 && (P % RB == 0), "FP16 output needs whole-column chunks");
+                // row j + P r sits in block j / RB + r P / RB at position j % RB (RB divides P)
+                const float sc = __int_as_float((127 + a.half_scale_exp) << 23);   // 2^e
+                __half2* Co = reinterpret_cast<__half2*>(a.C) + (size_t)o * Y * XP +
+                              ((size_t)(j / RB) * XP + kx0 + col) * RB + (j % RB);
+#pragma unroll
+                for (int r = 0; r < V; r++) Co[(size_t)r * P * XP] = __floats2half2_rn(v[r].x * sc, v[r].y * sc);
+            } else if constexpr (G == 1) {
                 float2* Co = a.C + (size_t)o * Y * XP + kx0 + col;
 #pragma unroll
                 for (int r = 0; r < V; r++) Co[(size_t)(j + P * r) * XP] = v[r];
@@ -880,6 +895,36 @@ struct Launch {
     static void pass_c(BatchArgs& a, cudaStream_t s) {
         k_pass_c<X><<<Y, X / 16, PC::smem_bytes(a.XP, a.hist_bins), s>>>(a, Y);
     }
+};
+
+}  // namespace tmk
+
+#include "tm_tensor.cuh"
+
+namespace tmk {
+
+// Launch shapes of the FP16 tensor-core form of one geometry (row lengths X of
+// 1024, 2048 or 4096): k_pass_b with FP16 output in blocks of R rows, and the
+// tensor-core row pass.
+template <int T, int X, int Y>
+struct LaunchTc {
+    using PB = PassB<T, Y>;
+    using PCT = PassCTc<X>;
+    static constexpr int R = PCT::R;
+    static cudaError_t configure(int XP, int bins) {
+        cudaError_t e = cudaFuncSetAttribute(k_pass_b<T, Y, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB::SMEM);
+        if (e != cudaSuccess) return e;
+        return cudaFuncSetAttribute(k_pass_c_tc<X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PCT::smem_bytes(XP, bins));
+    }
+    static void pass_b(BatchArgs& a, cudaStream_t s, int nsm) {
+        const int n_items = (a.XP / PB::WG) * a.nb;
+        k_pass_b<T, Y, R><<<n_items < nsm ? n_items : nsm, PB::NT, PB::SMEM, s>>>(a, n_items);
+    }
+    static void pass_c(BatchArgs& a, cudaStream_t s, const uint4* dft) {
+        k_pass_c_tc<X><<<Y / R, PCT::NT, PCT::smem_bytes(a.XP, a.hist_bins), s>>>(a, Y, dft);
+    }
+    static constexpr size_t dft_bytes = (size_t)PCT::B1_BYTES + PCT::B2_BYTES;
+    static void fill_dft(uint16_t* host) { fill_tc_dft<X>(host); }
 };
 
 }  // namespace tmk

@@ -8,6 +8,7 @@
 // intermediate of the search lives in one file-scope device array of fixed
 // size (kScratchBytes), which each GPU that loads this library keeps until
 // the process exits.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <float.h>
 #include <math.h>

@@ -1,5 +1,7 @@
-// tm_ptx.cuh -- sm_100a inline-PTX helpers: mbarriers and 1-D bulk (TMA) copies
-// from global to shared memory.  No cluster multicast is used anywhere.
+// tm_ptx.cuh -- sm_100a inline-PTX helpers: mbarriers, 1-D bulk (TMA) copies
+// from global to shared memory, tensor memory, and the 5th-generation tensor
+// core MMA (tcgen05.mma, kind::f16) with its shared-memory matrix descriptors.
+// No cluster multicast is used anywhere.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -136,6 +138,54 @@ __device__ __forceinline__ void tmem_wait_ld32(float* v) {
                    "+f"(v[24]), "+f"(v[25]), "+f"(v[26]), "+f"(v[27]), "+f"(v[28]), "+f"(v[29]), "+f"(v[30]), "+f"(v[31])
                  :
                  : "memory");
+}
+
+// ---- Tensor-core MMA (tcgen05.mma.cta_group::1.kind::f16) -------------------
+// Shared-memory matrix descriptor, no swizzle: the operand tile is made of
+// 8 x 8 "core matrices" of 16-bit elements, each 128 contiguous bytes (8 rows
+// of 16 bytes).  For a K-major operand a core-matrix row holds 8 consecutive K
+// elements of one M (or N) index; for an MN-major operand it holds 8
+// consecutive M (or N) elements of one K index.  lbo = byte distance between
+// core matrices adjacent in K, sbo = between core matrices adjacent in M (N).
+// Bits: start address >> 4 in [0,14), lbo >> 4 in [16,30), sbo >> 4 in
+// [32,46), descriptor version 1 in [46,48), layout type 0 (no swizzle) in
+// [61,64).
+__host__ __device__ constexpr uint64_t smem_desc_noswizzle(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+// Instruction descriptor of kind::f16 with FP16 A and B and an FP32
+// accumulator: D format F32 (bits [4,6) = 1), A and B format F16 (bits [7,10)
+// and [10,13) = 0), A major (bit 15; 1 = MN-major), B major (bit 16), N >> 3 in
+// bits [17,23), M >> 4 in bits [24,29).
+__host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N, bool a_mn_major, bool b_mn_major) {
+    return (1u << 4) | ((a_mn_major ? 1u : 0u) << 15) | ((b_mn_major ? 1u : 0u) << 16) |
+           ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// D[tmem] (+)= A[smem] x B[smem], one instruction of K = 16; issued by one thread.
+__device__ __forceinline__ void mma_f16_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                           bool accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate ? 1u : 0u)
+        : "memory");
+}
+
+// The mbarrier receives one arrival when every MMA this thread issued before
+// has completed.
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Orders this thread's generic-proxy shared-memory writes before later
+// async-proxy reads (the tensor core reads its operands through the async proxy).
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 }  // namespace tmptx

@@ -26,6 +26,7 @@
 //
 // Transforms are unnormalised: the score is invariant to the scale of the
 // projection spectrum, so the reference's 1/N factors cancel.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <float.h>
 #include <math.h>

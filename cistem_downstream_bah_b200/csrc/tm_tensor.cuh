@@ -1,0 +1,427 @@
+// tm_tensor.cuh -- FP16 tensor-core form of the row pass (pass C).
+//
+// The FP16 form of the search keeps the slice, projection and column kernels
+// (k_pass_b stores its correlation spectra as FP16 complex, scaled by 2^e so
+// that the row outputs are O(1), rows interleaved in blocks of R) and replaces
+// k_pass_c by k_pass_c_tc: per block of R rows, for one orientation at a time,
+//
+//   pre-processing   the half-complex row Z[k] (k = 0..X/2) becomes the
+//                    H = X/2-point complex sequence v[k] whose inverse FFT packs
+//                    the real row (pixels 2n, 2n+1 = Re, Im of z[n]) -- the same
+//                    packing as k_pass_c -- and is written, FP16, as the A
+//                    operand of stage 1
+//   stage 1 (MMA)    H = N1 x 64: for every k1 the 64-point inverse DFT over
+//                    k2 of v[k1 + N1 k2], as one 128 x 128 x 64 tcgen05.mma
+//                    (A = data, M = (row, k1, re/im); B = [cos | sin] of the
+//                    64-point DFT, K = k2), FP32 accumulators in TMEM
+//   epilogue 1       TMEM -> registers, re/im parts combined across lane
+//                    pairs, twiddle exp(+2 pi i k1 n2 / H), FP16 A operand of
+//                    stage 2 for each row
+//   stage 2 (MMA)    for every n2 the N1-point inverse DFT over k1, one
+//                    128 x 2N1 x N1 tcgen05.mma per row (K padded to 16)
+//   epilogue 2       TMEM -> registers, re/im combined, z[n2 + 64 n1] scaled
+//                    by 2^-e, and the MIP / argmax / compensated sums /
+//                    histogram update of k_pass_c (match_template.cpp:1102-1149)
+//
+// R = 64 / N1 = 8192 / X rows, so that stage 1 is always M = 128 and every
+// block holds 8192 pixels: 512 threads, 16 pixels each, their MIP, argmax and
+// sum in registers and their sum of squares and the two compensation terms in
+// TMEM.  The operands use the tensor core's no-swizzle layout of 8 x 8 core
+// matrices (tmptx::smem_desc_noswizzle); the A operands are MN-major with their
+// M groups 144 bytes apart, so that the epilogue's 16-byte stores of
+// neighbouring lanes fall in different banks.
+#pragma once
+#include <cuda_fp16.h>
+
+#include "tm_ptx.cuh"
+
+namespace tmk {
+
+template <int X>
+struct PassCTc {
+    static constexpr int H = X / 2;
+    static constexpr int N2 = 64;                    // stage-1 DFT length
+    static constexpr int N1 = H / N2;                // stage-2 DFT length
+    static constexpr int R = N2 / N1;                // rows per block (8192 / X)
+    static constexpr int K2 = N1 < 16 ? 16 : N1;     // stage-2 K, padded to the MMA's K step
+    static constexpr int NT = 512;
+    static constexpr int SBO_A = 144;                // A operands: M groups (16 B rows of 8 elements)
+    static constexpr int LBO_A = 16 * SBO_A;         // K groups (M = 128: 16 M groups)
+    static constexpr int A1_BYTES = (64 / 8) * LBO_A;
+    static constexpr int A2_BYTES = (K2 / 8) * LBO_A;   // per row
+    static constexpr int B1_N = 128, B1_K = 64;      // [cos | sin] of the 64-point DFT
+    static constexpr int B2_N = 2 * N1, B2_K = K2;   // [cos | sin] of the N1-point DFT
+    static constexpr int SBO_B = 128;                // B operands (K-major): N groups
+    static constexpr int LBO_B1 = (B1_N / 8) * 128;  // K groups
+    static constexpr int LBO_B2 = (B2_N / 8) * 128;
+    static constexpr int B1_BYTES = (B1_K / 8) * LBO_B1;
+    static constexpr int B2_BYTES = (B2_K / 8) * LBO_B2;
+    static constexpr int TM_D1 = 0;                  // TMEM columns: stage-1 accumulator
+    static constexpr int TM_D2 = 128;                // stage-2 accumulators, 2 N1 per row
+    static constexpr int TM_STATE = 256;             // 48 per warp of a lane quadrant
+    static constexpr uint32_t TMEM_COLS = 512;
+    static constexpr int OFF_B1 = 128;
+    static constexpr int OFF_B2 = OFF_B1 + B1_BYTES;
+    static constexpr int OFF_A1 = OFF_B2 + B2_BYTES;
+    static constexpr int OFF_A2 = OFF_A1 + A1_BYTES;
+    static constexpr int OFF_ROWS = OFF_A2 + R * A2_BYTES;
+    static_assert(N1 >= 2 && N1 * N2 == H && R * N1 == 64, "row length must be 2 * 64 * N1");
+    static_assert(B2_N % 16 == 0 && B2_N <= 256, "stage-2 N must be a multiple of 16");
+    static_assert(OFF_ROWS % 16 == 0, "operand regions 16-byte aligned");
+    // bytes of one staged row block: R rows x XP FP16 complex values
+    __host__ __device__ static size_t block_bytes(int XP) { return (size_t)XP * R * 4; }
+    static size_t smem_bytes(int XP, int bins) { return OFF_ROWS + 2 * block_bytes(XP) + 4 * (size_t)bins; }
+};
+
+// The DFT matrices of the two stages as FP16 B operands, in the byte layout the
+// kernel copies into shared memory: B1 (K = k2, N = [cos n2 | sin n2]) then B2
+// (K = k1 padded to K2 with zero rows, N = [cos n1 | sin n1]).  Filled on the
+// host; entry (n, k) of a K-major operand with N groups `sbo` and K groups `lbo`
+// apart sits at (n % 8) * 16 + (k % 8) * 2 + (n / 8) * sbo + (k / 8) * lbo.
+template <int X>
+void fill_tc_dft(uint16_t* out) {
+    using PC = PassCTc<X>;
+    auto put = [](uint16_t* base, int n, int k, int sbo, int lbo, double v) {
+        const __half h = __double2half(v);
+        base[((n % 8) * 16 + (k % 8) * 2 + (n / 8) * sbo + (k / 8) * lbo) / 2] = *reinterpret_cast<const uint16_t*>(&h);
+    };
+    uint16_t* b1 = out;
+    uint16_t* b2 = out + PC::B1_BYTES / 2;
+    for (int i = 0; i < (PC::B1_BYTES + PC::B2_BYTES) / 2; i++) out[i] = 0;
+    for (int k = 0; k < 64; k++)
+        for (int n = 0; n < 64; n++) {
+            const double th = 2.0 * M_PI * (double)((k * n) % 64) / 64.0;
+            put(b1, n, k, PC::SBO_B, PC::LBO_B1, cos(th));
+            put(b1, 64 + n, k, PC::SBO_B, PC::LBO_B1, sin(th));
+        }
+    for (int k = 0; k < PC::N1; k++)
+        for (int n = 0; n < PC::N1; n++) {
+            const double th = 2.0 * M_PI * (double)((k * n) % PC::N1) / (double)PC::N1;
+            put(b2, n, k, PC::SBO_B, PC::LBO_B2, cos(th));
+            put(b2, PC::N1 + n, k, PC::SBO_B, PC::LBO_B2, sin(th));
+        }
+}
+
+// byte offset of element (m, k) in an MN-major A operand (M = 128)
+template <int X>
+__device__ __forceinline__ uint32_t a_off(int m, int k) {
+    using PC = PassCTc<X>;
+    return (uint32_t)((m % 8) * 2 + (k % 8) * 16 + (m / 8) * PC::SBO_A + (k / 8) * PC::LBO_A);
+}
+
+__device__ __forceinline__ uint32_t h2_bits(float a, float b) {
+    const __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+template <int X>
+__global__ void __launch_bounds__(512, 1)
+k_pass_c_tc(BatchArgs a, int Y, const uint4* __restrict__ dft) {
+    using PC = PassCTc<X>;
+    constexpr int H = PC::H, N1 = PC::N1, R = PC::R, K2 = PC::K2;
+    constexpr uint32_t kWaitLimit = 1u << 24;
+    const int XP = a.XP;
+    extern __shared__ __align__(128) unsigned char smem_t[];
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_t);   // [0], [1]: row blocks; [2]: MMA completion
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem_t + 64);
+    unsigned char* sB1 = smem_t + PC::OFF_B1;
+    unsigned char* sB2 = smem_t + PC::OFF_B2;
+    unsigned char* sA1 = smem_t + PC::OFF_A1;
+    unsigned char* sA2 = smem_t + PC::OFF_A2;
+    unsigned char* rows = smem_t + PC::OFF_ROWS;
+    const size_t blk = PC::block_bytes(XP);
+    unsigned int* shist = reinterpret_cast<unsigned int*>(rows + 2 * blk);
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int q = warp & 3, sub = warp >> 2;              // TMEM lane quadrant, column share
+    const int m = 32 * q + lane;                          // this thread's TMEM lane (accumulator row)
+    const int y0 = blockIdx.x * R;
+    const uint32_t blk_bytes = (uint32_t)blk;
+    const __half2* C16 = reinterpret_cast<const __half2*>(a.C);
+    const float out_scale = exp2f(-(float)a.half_scale_exp);
+
+    if (t == 0) {
+        tmptx::mbar_init(&mbar[0], 1);
+        tmptx::mbar_init(&mbar[1], 1);
+        tmptx::mbar_init(&mbar[2], 1);
+    }
+    if (warp == 0) {
+        tmptx::tmem_alloc(tmem_slot, PC::TMEM_COLS);
+        tmptx::tmem_relinquish();
+    }
+    // DFT matrices into shared memory; the stage-2 A operands start at zero
+    // (their K rows beyond N1 are never written and multiply zero B rows)
+    for (int i = t; i < (PC::B1_BYTES + PC::B2_BYTES) / 16; i += PC::NT)
+        reinterpret_cast<uint4*>(sB1)[i] = __ldg(dft + i);
+    for (int i = t; i < R * PC::A2_BYTES / 16; i += PC::NT) reinterpret_cast<uint4*>(sA2)[i] = make_uint4(0, 0, 0, 0);
+    for (int b = t; b < a.hist_bins; b += PC::NT) shist[b] = 0u;
+    tmptx::fence_proxy_async_smem();
+    tmptx::tmem_fence_before_sync();
+    __syncthreads();
+    tmptx::tmem_fence_after_sync();
+    const uint32_t tbase = *tmem_slot;
+    const uint32_t tlane = (uint32_t)(32 * q) << 16;
+    const uint32_t tstate = tbase + tlane + (uint32_t)(PC::TM_STATE + 48 * sub);
+    if (t == 0 && a.nb > 0) {
+        tmptx::mbar_arrive_expect_tx(&mbar[0], blk_bytes);
+        tmptx::bulk_g2s(rows, C16 + (size_t)blockIdx.x * XP * R, blk_bytes, &mbar[0]);
+    }
+
+    // ---- this thread's 16 pixels: items u = 8 * (2 sub + p) + i of the lane pair
+    // (n2 = m / 2), item = (row r, n1); pixel x = 2 (n2 + 64 n1) + h
+    const int n2_own = m >> 1, p_own = m & 1;
+    const int item0 = 8 * (2 * sub + p_own);
+    float mip[16], fs[16];
+    int best[16];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int it = item0 + i, r = it / N1, n1 = it % N1;
+        const size_t off = (size_t)(y0 + r) * X + 2 * (n2_own + 64 * n1);
+        const float2 mv = *reinterpret_cast<const float2*>(a.mip + off);
+        const int2 bv = *reinterpret_cast<const int2*>(a.best + off);
+        mip[2 * i] = mv.x; mip[2 * i + 1] = mv.y;
+        best[2 * i] = bv.x; best[2 * i + 1] = bv.y;
+        fs[2 * i] = 0.f; fs[2 * i + 1] = 0.f;
+    }
+    {
+        float z[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) z[i] = 0.f;
+        tmptx::tmem_st16(tstate, z);
+        tmptx::tmem_st16(tstate + 16, z);
+        tmptx::tmem_st16(tstate + 32, z);
+        tmptx::tmem_wait_st();
+    }
+
+    const uint32_t id1 = tmptx::idesc_f16_f32(128, PC::B1_N, true, false);
+    const uint32_t id2 = tmptx::idesc_f16_f32(128, PC::B2_N, true, false);
+    const uint32_t a1_addr = tmptx::smem_u32(sA1), a2_addr = tmptx::smem_u32(sA2);
+    const uint32_t b1_addr = tmptx::smem_u32(sB1), b2_addr = tmptx::smem_u32(sB2);
+    bool timed_out = false;
+    bool mma_pending = false;   // a commit whose wait ran out
+    uint32_t mma_phase = 0;     // commits completed and waited for
+    int o = 0;
+    for (; o < a.nb; o++) {
+        const int buf = o & 1;
+        // iteration o-1 is done with row buffer buf ^ 1, A1 and the accumulators
+        if (__syncthreads_or(timed_out)) break;
+        if (t == 0 && o + 1 < a.nb) {
+            tmptx::mbar_arrive_expect_tx(&mbar[buf ^ 1], blk_bytes);
+            tmptx::bulk_g2s(rows + (buf ^ 1) * blk, C16 + ((size_t)(o + 1) * (Y / R) + blockIdx.x) * XP * R, blk_bytes,
+                            &mbar[buf ^ 1]);
+        }
+        if (!tmptx::mbar_wait_bounded(&mbar[buf], (o >> 1) & 1, kWaitLimit)) {
+            timed_out = true;
+            atomicExch(a.err, 1);
+        }
+        // ---- pre-processing: v[r][k] -> A1[(r, k1, re/im)][k2], k = k1 + N1 k2
+        {
+            const __half2* zb = reinterpret_cast<const __half2*>(rows + buf * blk);
+#pragma unroll
+            for (int i = 0; i < (R * H) / PC::NT; i++) {
+                const int idx = t + PC::NT * i;
+                const int r = idx / H, k = idx % H;
+                float2 hk = __half22float2(zb[k * R + r]);
+                float2 hm = __half22float2(zb[(H - k) * R + r]);
+                if (k == 0) { hk.y = 0.f; hm.y = 0.f; }
+                const float2 e = make_float2(hk.x + hm.x, hk.y - hm.y);
+                const float2 d = make_float2(hk.x - hm.x, hk.y + hm.y);
+                const float2 od = cmul(d, a.tw.template w<+1>(k, X));
+                const int k1 = k % N1, k2 = k / N1;
+                *reinterpret_cast<uint32_t*>(sA1 + a_off<X>(2 * (k1 + N1 * r), k2)) = h2_bits(e.x - od.y, e.y + od.x);
+            }
+        }
+        tmptx::fence_proxy_async_smem();
+        if (__syncthreads_or(timed_out)) break;
+        // ---- stage 1: D1 = A1 (128 x 64) x B1 (64 x 128)
+        if (t == 0) {
+            tmptx::tmem_fence_after_sync();
+#pragma unroll
+            for (int kk = 0; kk < 4; kk++)
+                tmptx::mma_f16_ss(tbase + PC::TM_D1,
+                                  tmptx::smem_desc_noswizzle(a1_addr + kk * 2 * PC::LBO_A, PC::LBO_A, PC::SBO_A),
+                                  tmptx::smem_desc_noswizzle(b1_addr + kk * 2 * PC::LBO_B1, PC::LBO_B1, PC::SBO_B), id1,
+                                  kk > 0);
+            tmptx::mma_commit(&mbar[2]);
+        }
+        mma_pending = true;
+        if (tmptx::mbar_wait_bounded(&mbar[2], mma_phase & 1, kWaitLimit)) {
+            mma_pending = false;
+        } else {
+            timed_out = true;
+            atomicExch(a.err, 1);
+        }
+        mma_phase++;
+        tmptx::tmem_fence_after_sync();
+        // ---- epilogue 1: lane m = (r, k1, p); columns n2 in [16 sub, 16 sub + 16) of the cos and sin halves
+        {
+            const int p = m & 1, k1 = (m >> 1) % N1, r = (m >> 1) / N1;
+            float c[16], sn[16];
+            tmptx::tmem_ld16(tbase + tlane + PC::TM_D1 + 16 * sub, c);
+            tmptx::tmem_ld16(tbase + tlane + PC::TM_D1 + 64 + 16 * sub, sn);
+            tmptx::tmem_wait_ld16(c);
+            tmptx::tmem_wait_ld16(sn);
+            // the pair (p = 0, 1) splits the 16 n2: p = 0 takes the first 8, p = 1 the last 8;
+            // each sends the partner the products it needs
+            float rc[8], rs[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                rc[i] = __shfl_xor_sync(0xffffffffu, p ? c[i] : c[8 + i], 1);
+                rs[i] = __shfl_xor_sync(0xffffffffu, p ? sn[i] : sn[8 + i], 1);
+            }
+            const int n2_0 = 16 * sub + 8 * p;
+            uint32_t packed[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                // Y = (P_re,c - P_im,s) + i (P_re,s + P_im,c)
+                const float yr = p ? rc[i] - sn[8 + i] : c[i] - rs[i];
+                const float yi = p ? rs[i] + c[8 + i] : sn[i] + rc[i];
+                const float2 yv = cmul(make_float2(yr, yi), a.tw.template w<+1>(k1 * (n2_0 + i), H));
+                packed[i] = h2_bits(yv.x, yv.y);
+            }
+            // A2_r[(n2, re/im)][k1]: two 16-byte rows (4 n2 each) of two M groups
+            unsigned char* dst = sA2 + r * PC::A2_BYTES;
+            *reinterpret_cast<uint4*>(dst + a_off<X>(2 * n2_0, k1)) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+            *reinterpret_cast<uint4*>(dst + a_off<X>(2 * n2_0 + 8, k1)) = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+        }
+        tmptx::fence_proxy_async_smem();
+        tmptx::tmem_fence_before_sync();
+        if (__syncthreads_or(timed_out)) break;
+        // ---- stage 2: per row, D2_r = A2_r (128 x K2) x B2 (K2 x 2 N1)
+        if (t == 0) {
+            tmptx::tmem_fence_after_sync();
+#pragma unroll
+            for (int r = 0; r < R; r++)
+#pragma unroll
+                for (int kk = 0; kk < K2 / 16; kk++)
+                    tmptx::mma_f16_ss(tbase + PC::TM_D2 + r * PC::B2_N,
+                                      tmptx::smem_desc_noswizzle(a2_addr + r * PC::A2_BYTES + kk * 2 * PC::LBO_A, PC::LBO_A,
+                                                                 PC::SBO_A),
+                                      tmptx::smem_desc_noswizzle(b2_addr + kk * 2 * PC::LBO_B2, PC::LBO_B2, PC::SBO_B), id2,
+                                      kk > 0);
+            tmptx::mma_commit(&mbar[2]);
+        }
+        mma_pending = true;
+        if (tmptx::mbar_wait_bounded(&mbar[2], mma_phase & 1, kWaitLimit)) {
+            mma_pending = false;
+        } else {
+            timed_out = true;
+            atomicExch(a.err, 1);
+        }
+        mma_phase++;
+        tmptx::tmem_fence_after_sync();
+        // ---- epilogue 2: lane m = (n2, p); the 16 items [16 sub, 16 sub + 16) of the lane pair
+        {
+            const int p = p_own;
+            float c[16], sn[16];
+            const int it0 = 16 * sub;
+            if constexpr (N1 >= 16) {
+                const int r = it0 / N1, n1_0 = it0 % N1;
+                const uint32_t col = tbase + tlane + PC::TM_D2 + r * PC::B2_N + n1_0;
+                tmptx::tmem_ld16(col, c);
+                tmptx::tmem_ld16(col + N1, sn);
+            } else {
+                // N1 = 8: the 16 items are two whole rows, [cos 8 | sin 8] each
+                const uint32_t col = tbase + tlane + PC::TM_D2 + (it0 / N1) * PC::B2_N;
+                float w[32];
+                tmptx::tmem_ld16(col, w);
+                tmptx::tmem_ld16(col + 16, w + 16);
+                tmptx::tmem_wait_ld32(w);
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    c[i] = w[i]; sn[i] = w[8 + i];
+                    c[8 + i] = w[16 + i]; sn[8 + i] = w[24 + i];
+                }
+            }
+            tmptx::tmem_wait_ld16(c);
+            tmptx::tmem_wait_ld16(sn);
+            float rc[8], rs[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                rc[i] = __shfl_xor_sync(0xffffffffu, p ? c[i] : c[8 + i], 1);
+                rs[i] = __shfl_xor_sync(0xffffffffu, p ? sn[i] : sn[8 + i], 1);
+            }
+            // every read of D2 is done before the next stage-2 MMA (the next iteration's barriers)
+            tmptx::tmem_fence_before_sync();
+            const int g = (int)(a.gidx0 + o);
+            float val[16];
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                val[2 * i] = (p ? rc[i] - sn[8 + i] : c[i] - rs[i]) * out_scale;
+                val[2 * i + 1] = (p ? rs[i] + c[8 + i] : sn[i] + rc[i]) * out_scale;
+            }
+            float st[32];
+            // sweep 0: MIP / argmax, histogram and the sum (compensation in TMEM columns 0-15)
+            tmptx::tmem_ld16(tstate, st);
+            tmptx::tmem_wait_ld16(st);
+#pragma unroll
+            for (int pi = 0; pi < 16; pi++) {
+                const float v = val[pi];
+                if (v > mip[pi]) { mip[pi] = v; best[pi] = g; }
+                const float ys = v - st[pi];
+                const float ts = fs[pi] + ys;
+                st[pi] = (ts - fs[pi]) - ys;
+                fs[pi] = ts;
+                const int bin = __float2int_rz((v - a.hist_min) * a.hist_inv_step);
+                if (bin >= 0 && bin < a.hist_bins) atomicAdd(&shist[bin], 1u);
+            }
+            tmptx::tmem_st16(tstate, st);
+            // sweep 1: the sum of squares (columns 32-47) and its compensation (16-31)
+            tmptx::tmem_ld16(tstate + 16, st);
+            tmptx::tmem_ld16(tstate + 32, st + 16);
+            tmptx::tmem_wait_ld32(st);
+#pragma unroll
+            for (int pi = 0; pi < 16; pi++) {
+                const float v = val[pi];
+                const float yq = fmaf(v, v, -st[pi]);
+                const float tq = st[16 + pi] + yq;
+                st[pi] = (tq - st[16 + pi]) - yq;
+                st[16 + pi] = tq;
+            }
+            tmptx::tmem_st16(tstate + 16, st);
+            tmptx::tmem_st16(tstate + 32, st + 16);
+            tmptx::tmem_wait_st();
+        }
+    }
+    // ---- end of the batch: the FP64 flush, or the drain after a wait ran out
+    float st[48];
+    tmptx::tmem_ld16(tstate, st);
+    tmptx::tmem_ld16(tstate + 16, st + 16);
+    tmptx::tmem_wait_ld32(st);
+    tmptx::tmem_ld16(tstate + 32, st + 32);
+    tmptx::tmem_wait_ld16(st + 32);
+    tmptx::tmem_fence_before_sync();
+    const bool failed = __syncthreads_or(timed_out);
+    if (failed) {
+        // no MMA or bulk copy may still be writing TMEM or shared memory when the block exits
+        if (mma_pending) tmptx::mbar_wait_bounded(&mbar[2], (mma_phase - 1) & 1, kWaitLimit);
+        if (o > 0) tmptx::mbar_wait_bounded(&mbar[(o - 1) & 1], ((o - 1) >> 1) & 1, kWaitLimit);
+        if (o < a.nb) tmptx::mbar_wait_bounded(&mbar[o & 1], (o >> 1) & 1, kWaitLimit);
+    }
+    tmptx::tmem_fence_before_sync();
+    __syncthreads();
+    tmptx::tmem_fence_after_sync();
+    if (warp == 0) tmptx::tmem_dealloc(tbase, PC::TMEM_COLS);
+    if (failed) return;   // results of this block are discarded (the host reports the timeout)
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int it = item0 + i, r = it / N1, n1 = it % N1;
+        const size_t off = (size_t)(y0 + r) * X + 2 * (n2_own + 64 * n1);
+        *reinterpret_cast<float2*>(a.mip + off) = make_float2(mip[2 * i], mip[2 * i + 1]);
+        *reinterpret_cast<int2*>(a.best + off) = make_int2(best[2 * i], best[2 * i + 1]);
+        double2 sv = *reinterpret_cast<const double2*>(a.sum + off);
+        double2 qv = *reinterpret_cast<const double2*>(a.sumsq + off);
+        sv.x += (double)fs[2 * i] - (double)st[2 * i];
+        sv.y += (double)fs[2 * i + 1] - (double)st[2 * i + 1];
+        qv.x += (double)st[32 + 2 * i] - (double)st[16 + 2 * i];
+        qv.y += (double)st[32 + 2 * i + 1] - (double)st[16 + 2 * i + 1];
+        *reinterpret_cast<double2*>(a.sum + off) = sv;
+        *reinterpret_cast<double2*>(a.sumsq + off) = qv;
+    }
+    __syncthreads();
+    for (int b = t; b < a.hist_bins; b += PC::NT) {
+        const unsigned int cnt = shist[b];
+        if (cnt) atomicAdd(a.hist + b, (unsigned long long)cnt);
+    }
+}
+
+}  // namespace tmk

@@ -111,6 +111,23 @@ TM_API int tm_set_template_volume(tm_ctx *ctx, const float *volume, int template
 TM_API int tm_template_spectrum(int device, const float *volume, int template_size, float pixel_size_factor,
                                 float *spectrum);
 
+/* Arithmetic of the search's correlation transforms (no counterpart in the
+ * reference's CPU path; its GPU path runs cuFFT with FP16 image and
+ * correlation buffers, src/gpu/GpuImage.cu:2138-2145,
+ * TemplateMatchingCore.cu:388-425).
+ *   TM_PRECISION_FP32 (default): every transform in FP32, the parity path.
+ *   TM_PRECISION_FP16_TENSOR: the column pass stores its correlation spectra
+ *   as FP16 (times a power of two) and the row pass runs its inverse
+ *   transform as two DFT-matrix stages on the tensor cores (FP16 operands,
+ *   FP32 accumulation); the MIP and the compensated sums stay FP32, their
+ *   batch totals FP64.  MIP error about 1e-4 of the MIP scale.
+ * TM_ERR_UNSUPPORTED for geometries without the FP16 kernels (image_x of
+ * 1024, 2048 or 4096 and image_y a power of two or 3888 have them). */
+#define TM_PRECISION_FP32 0
+#define TM_PRECISION_FP16_TENSOR 1
+TM_API int tm_set_precision(tm_ctx *ctx, int precision);
+TM_API int tm_get_precision(const tm_ctx *ctx);
+
 /* Pixel count that the projection variance is formed over (match_template.cpp:1066-1067
  * use the padded micrograph's). 0, the default, is the context's X*Y. A context that
  * searches a window cut from a larger whitened micrograph passes that micrograph's

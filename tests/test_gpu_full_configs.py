@@ -62,6 +62,24 @@ def _check_search_state(got, st, X, Y):
     assert np.all(np.abs(got["hist"] - h) <= 1e-3 * h + 2)
 
 
+def _check_fp16_form(got, st, n_orient, X, Y):
+    """MIP error (relative to the MIP scale) and z-score error of the FP16
+    tensor-core form against the FP64 oracle; the north-star bound on the MIP
+    error is 1e-2."""
+    sq = np.sqrt(float(X * Y))
+    mip_ref, z_ref, _, _ = O.finalize(st, n_orient, sq)
+    gs = O.SearchState(X, Y)
+    gs.mip[:], gs.sum[:], gs.sumsq[:] = got["mip"], got["sum"], got["sumsq"]
+    mip_got, z_got, _, _ = O.finalize(gs, n_orient, sq)
+    mip_err = float(np.abs(mip_got - mip_ref).max() / np.abs(mip_ref).max())
+    z_err = float(np.abs(z_got - z_ref).max())
+    print(f"FP16 tensor-core form vs FP64 oracle, {X}x{Y}, {n_orient} orientations: "
+          f"MIP max rel err {mip_err:.2e}, z max abs err {z_err:.2e}")
+    assert mip_err <= 1e-2
+    assert z_err <= 0.05
+    return mip_err, z_err
+
+
 def test_config1_whole_search_program_matches_oracle(tmp_path):
     T, PIXEL, DEFOCUS, STEP = 64, 1.5, 12000.0, 15.0
     vol = synthetic.template_volume(T, PIXEL, 3000, 40.0, seed=20261204)
@@ -125,6 +143,11 @@ def test_config1_whole_search_program_matches_oracle(tmp_path):
         sc.set_image(ispec)
         sc.run_plane(filt, ang)
         _check_search_state(sc.results(), st, X, Y)
+        # the FP16 tensor-core form of the same search: MIP and z-score error against the oracle
+        sc.reset()
+        sc.set_precision(core.PRECISION_FP16_TENSOR)
+        sc.run_plane(filt, ang)
+        _check_fp16_form(sc.results(), st, len(ang), X, Y)
 
 
 def test_config2_contiguous_orientations_match_oracle():
@@ -151,6 +174,13 @@ def test_config2_contiguous_orientations_match_oracle():
         sc.run_plane(filt, ang)
         got = sc.results()
     _check_search_state(got, st, X, Y)
+    with core.SearchCore(X, Y, T, histogram_min_scaled=hmin, histogram_step_scaled=hstep,
+                         orientation_batch=128) as sc:
+        sc.set_precision(core.PRECISION_FP16_TENSOR)
+        sc.set_template(tspec)
+        sc.set_image(ispec)
+        sc.run_plane(filt, ang)
+        _check_fp16_form(sc.results(), st, len(ang), X, Y)
     # the peak list over these orientations: the reference's loop on both z maps
     sq = np.sqrt(float(X * Y))
     _, z_ref, _, _ = O.finalize(st, len(ang), sq)

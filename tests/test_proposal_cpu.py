@@ -166,7 +166,7 @@ def test_window_variants_are_compiled():
     import os
     import re
     src = open(os.path.join(os.path.dirname(PR.__file__), "csrc", "tm_capi.cu")).read()
-    variants = {tuple(int(v) for v in m) for m in re.findall(r"TM_VARIANT\((\d+),\s*(\d+),\s*(\d+)\)", src)}
+    variants = {tuple(int(v) for v in m) for m in re.findall(r"TM_VARIANT(?:_TC)?\((\d+),\s*(\d+),\s*(\d+)\)", src)}
     for T in (64, 128, 256):
         W = PR.window_size(T)
         assert (T, W, W) in variants, (T, W)
