@@ -82,6 +82,16 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def tensor_peaks():
+    """Dense FP16/BF16 tensor throughput (TFLOP/s): burst (a kernel timed alone) and sustained."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["bf16_tflops_sustained"]), float(p["bf16_tflops"])
+    except Exception:
+        return 1400.0, 1590.0
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -302,35 +312,12 @@ def run_batched(args, seed=20261210):
         print(json.dumps(line), flush=True)
 
 
-def run_ours(args):
-    world, rank, local = dist_init(args)
-    from cistem_downstream_bah_b200 import core
-    inp = make_inputs()
-    X, Y, T = inp["X"], inp["Y"], inp["T"]
-    per_step = args.orientations_per_step
-    n_orient_total = len(inp["angles"])
-    npix_orig = WORKLOAD["nx"] * WORKLOAD["ny"]
-    sc = core.SearchCore(X, Y, T, histogram_min_scaled=inp["hmin"], histogram_step_scaled=inp["hstep"],
-                         orientation_batch=args.batch, device=local)
-    precision = core.PRECISION_FP16_TENSOR if args.precision == "fp16" else core.PRECISION_FP32
-    sc.set_precision(precision)
-    sc.set_template(inp["tspec"])
-    sc.set_image(inp["ispec"])
-    if args.batch == 0:
-        # the library's autotuner picks the orientations per device pass
-        sc.autotune(inp["filt"], inp["angles"][:256])
-    batch = sc.orientation_batch()
-
-    def chunk(i):
-        a = (i * per_step) % n_orient_total
-        return inp["angles"][a:a + per_step]
-
-    # ---- device-resident timing
+def _device_leg(sc, inp, args, world, local, chunk):
+    """Device-resident timing of K steps (CUDA events on the library's stream)."""
     for i in range(args.warmup):
         sc.run_plane(inp["filt"], chunk(i))
     barrier(world)
-    dev_ms = 0.0
-    b_ms = c_ms = prep_ms = 0.0
+    dev_ms = b_ms = c_ms = prep_ms = 0.0
     n_done = 0
     with ClockSampler(local) as clk:
         t_wall0 = time.perf_counter()
@@ -345,21 +332,25 @@ def run_ours(args):
             n_done += len(ang)
         barrier(world)
         wall_ms = (time.perf_counter() - t_wall0) * 1e3   # the sampler's start and stop excluded
-    dev_ms_max = max_over_ranks(world, dev_ms)
-    value = world * npix_orig * n_done / (dev_ms_max * 1e-3)
+    return dict(dev_ms=max_over_ranks(world, dev_ms), b_ms=b_ms, c_ms=c_ms, prep_ms=prep_ms, n_done=n_done,
+                clocks=clk.summary(), wall_ms=wall_ms)
 
-    # ---- end to end through the C ABI with pinned host buffers.  As the
-    # reference drives one GPU from several host threads, each with its own
-    # TemplateMatchingCore, the steps go round-robin to --e2e-contexts host
-    # threads, each with its own context (stream): one thread's copies and
-    # result decoding overlap another's search.
+
+def _e2e_leg(sc, inp, args, world, local, chunk, precision):
+    """End to end through the C ABI with pinned host buffers.  As the reference
+    drives one GPU from several host threads, each with its own
+    TemplateMatchingCore, the steps go round-robin to --e2e-contexts host
+    threads, each with its own context (stream): one thread's copies and result
+    decoding overlap another's search."""
+    from cistem_downstream_bah_b200 import core
+    X, Y, T = inp["X"], inp["Y"], inp["T"]
     ispec_h, tspec_h, filt_h = pinned_copy(inp["ispec"]), pinned_copy(inp["tspec"]), pinned_copy(inp["filt"])
     n = X * Y
     L = sc.L
     ptr = core._ptr
     n_ctx = max(1, min(args.e2e_contexts, args.steps))
     ctxs = [sc] + [core.SearchCore(X, Y, T, histogram_min_scaled=inp["hmin"], histogram_step_scaled=inp["hstep"],
-                                   orientation_batch=batch, device=local) for _ in range(n_ctx - 1)]
+                                   orientation_batch=sc.orientation_batch(), device=local) for _ in range(n_ctx - 1)]
     for c in ctxs[1:]:
         c.set_precision(precision)
     bufs = []
@@ -369,6 +360,7 @@ def run_ours(args):
         outs["hist"] = np.zeros(512, np.int64)
         bufs.append(outs)
     errors = []
+    n_done = [0] * n_ctx
 
     def e2e_worker(k):
         try:
@@ -382,6 +374,7 @@ def run_ours(args):
                 c._check(L.tm_get_results(c.h, ptr(outs["mip"]), ptr(outs["psi"]), ptr(outs["theta"]),
                                           ptr(outs["phi"]), ptr(outs["defocus"]), ptr(outs["pixel"]),
                                           ptr(outs["sum"]), ptr(outs["sumsq"]), ptr(outs["hist"])))
+                n_done[k] += len(ang)
         except Exception as e:   # re-raised below, after every thread has stopped
             errors.append(e)
 
@@ -398,25 +391,69 @@ def run_ours(args):
         raise errors[0]
     for c in ctxs[1:]:
         c.close()
-    e2e = world * npix_orig * n_done / e2e_s
-    h2d = ispec_h.nbytes + tspec_h.nbytes + filt_h.nbytes + per_step * 12
+    h2d = ispec_h.nbytes + tspec_h.nbytes + filt_h.nbytes + args.orientations_per_step * 12
     d2h = n * 4 + n * 4 + 2 * n * 8 + 512 * 8   # mip, best index, sum, sum of squares, histogram
+    return dict(e2e_s=e2e_s, n_done=sum(n_done), h2d=h2d, d2h=d2h, host_threads=n_ctx)
+
+
+# Issued tensor-core FLOPs of the FP16 form per launch (one orientation batch of nb):
+# column pass, per item of 4 columns: stage H 2*128*256*16, stages F, 1, 2 three times
+# two 128 x 128 x 128 MMAs; row pass, per block of R rows: stage 1 2*128*128*64 and
+# R stage-2 MMAs 2*128*(2 N1)*max(16, N1), N1 = X / 128.
+def tensor_flops_per_launch(X, Y, XP, nb):
+    col = (XP // 4) * nb * (2 * 128 * 256 * 16 + 3 * 2 * 2 * 128 ** 3) if Y == 4096 else 0.0
+    N1 = X // 128
+    R = 64 // N1
+    row = (Y // R) * nb * (2 * 128 * 128 * 64 + R * 2 * 128 * 2 * N1 * max(16, N1))
+    return col, row
+
+
+def run_ours(args):
+    world, rank, local = dist_init(args)
+    from cistem_downstream_bah_b200 import core
+    inp = make_inputs()
+    X, Y, T = inp["X"], inp["Y"], inp["T"]
+    per_step = args.orientations_per_step
+    n_orient_total = len(inp["angles"])
+    npix_orig = WORKLOAD["nx"] * WORKLOAD["ny"]
+    N = X * Y
+
+    def chunk(i):
+        a = (i * per_step) % n_orient_total
+        return inp["angles"][a:a + per_step]
+
+    def make_context(precision):
+        sc = core.SearchCore(X, Y, T, histogram_min_scaled=inp["hmin"], histogram_step_scaled=inp["hstep"],
+                             orientation_batch=args.batch, device=local)
+        sc.set_precision(precision)
+        sc.set_template(inp["tspec"])
+        sc.set_image(inp["ispec"])
+        if args.batch == 0:
+            # the library's autotuner picks the orientations per device pass
+            sc.autotune(inp["filt"], inp["angles"][:256])
+        return sc
+
+    # ---- the FP32 parity path: device-resident timing, then end to end
+    precision = core.PRECISION_FP16_TENSOR if args.precision == "fp16" else core.PRECISION_FP32
+    sc = make_context(precision)
+    nb = sc.orientation_batch()
+    dev = _device_leg(sc, inp, args, world, local, chunk)
+    value = world * npix_orig * dev["n_done"] / (dev["dev_ms"] * 1e-3)
+    e2e = _e2e_leg(sc, inp, args, world, local, chunk, precision)
 
     # ---- roofline for the dominant kernel (per launch = one orientation batch)
     hbm_peak, peak_kind = peaks()
-    N = X * Y
-    nb = batch
-    n_launch = n_done / nb
-    b_launch_ms = b_ms / max(n_launch, 1)
-    c_launch_ms = c_ms / max(n_launch, 1)
+    n_launch = dev["n_done"] / nb
+    b_launch_ms = dev["b_ms"] / max(n_launch, 1)
+    c_launch_ms = dev["c_ms"] / max(n_launch, 1)
     # algorithmic bytes per point: pass B reads the half spectrum (4 B) and
     # writes the intermediate (4 B); pass C reads the intermediate (4 B)
-    dominant = "k_pass_b" if b_ms >= c_ms else "k_pass_c"
+    dominant = "k_pass_b" if dev["b_ms"] >= dev["c_ms"] else "k_pass_c"
     alg_b = 8.0 * N * nb
     alg_c = 4.0 * N * nb
     # DRAM bytes per launch measured by ncu on this workload (dram__bytes_read.sum +
     # dram__bytes_write.sum); they apply to the default workload and its batches only
-    prof = PROFILED_TRAFFIC.get(nb) if (X, Y, T) == (4096, 4096, 256) else None
+    prof = PROFILED_TRAFFIC.get(nb) if (X, Y, T) == (4096, 4096, 256) and precision == core.PRECISION_FP32 else None
     if dominant == "k_pass_b":
         ach = alg_b / (b_launch_ms * 1e-3) / 1e9
         traffic = args.traffic_b if args.traffic_b is not None else (prof["k_pass_b"] if prof else None)
@@ -424,34 +461,81 @@ def run_ours(args):
         ach = alg_c / (c_launch_ms * 1e-3) / 1e9
         traffic = args.traffic_c if args.traffic_c is not None else (prof["k_pass_c"] if prof else None)
 
+    # ---- the FP16 tensor-core form on the same workload and orientation chunks
+    fp16 = None
+    if precision == core.PRECISION_FP32 and not args.no_fp16_leg:
+        try:
+            sc16 = make_context(core.PRECISION_FP16_TENSOR)
+        except core.TmError as e:
+            sc16 = None
+            fp16 = {"unavailable": str(e)}
+        if sc16 is not None:
+            nb16 = sc16.orientation_batch()
+            d16 = _device_leg(sc16, inp, args, world, local, chunk)
+            v16 = world * npix_orig * d16["n_done"] / (d16["dev_ms"] * 1e-3)
+            e16 = _e2e_leg(sc16, inp, args, world, local, chunk, core.PRECISION_FP16_TENSOR)
+            nl16 = d16["n_done"] / nb16
+            b16 = d16["b_ms"] / max(nl16, 1)
+            c16 = d16["c_ms"] / max(nl16, 1)
+            XP = -(-(X // 2 + 1) // 4) * 4      # row pitch: 4-column chunks of the column pass
+            fl_b, fl_c = tensor_flops_per_launch(X, Y, XP, nb16)
+            _, tflops_peak = tensor_peaks()
+            fp16 = {
+                "value": v16, "unit": UNIT, "ratio_to_fp32_value": v16 / value,
+                "ms_per_step": d16["dev_ms"] / args.steps, "orientation_batch": nb16,
+                "e2e": {"value": world * npix_orig * e16["n_done"] / e16["e2e_s"], "unit": UNIT,
+                        "h2d_bytes_per_step": int(e16["h2d"]), "d2h_bytes_per_step": int(e16["d2h"]),
+                        "host_threads": e16["host_threads"]},
+                "ms_per_launch": {"k_pass_b_tc": b16, "k_pass_c_tc": c16,
+                                  "prep_kernels": d16["prep_ms"] / max(nl16, 1)},
+                # algorithmic bytes per point in FP16 storage: pass B 4 B (half spectrum read
+                # and intermediate write), pass C 2 B (intermediate read)
+                "roofline": {"bound": "tensor", "kernel": "k_pass_b_tc" if b16 >= c16 else "k_pass_c_tc",
+                             "achieved": (fl_b / (b16 * 1e-3) if b16 >= c16 else fl_c / (c16 * 1e-3)) / 1e12,
+                             "peak": tflops_peak, "unit": "TFLOP/s",
+                             "frac": (fl_b / (b16 * 1e-3) if b16 >= c16 else fl_c / (c16 * 1e-3)) / 1e12 / tflops_peak,
+                             "traffic": None, "peak_source": peak_kind,
+                             "hbm_achieved_gbs": {"k_pass_b_tc": 4.0 * N * nb16 / (b16 * 1e-3) / 1e9,
+                                                  "k_pass_c_tc": 2.0 * N * nb16 / (c16 * 1e-3) / 1e9},
+                             "note": "issued DFT-matrix MMA FLOPs per launch (FP16 operands, FP32 accumulate)"},
+                "clocks": d16["clocks"],
+            }
+            if rank == 0 and world == 1 and args.accuracy > 0:
+                fp16["accuracy_vs_fp64_oracle"] = accuracy_vs_fp64(sc16, inp, args.accuracy)
+            sc16.close()
+
     # the CPU-baseline leg (rank 0, N=1): the oracle timed on the host cores,
     # then the FP64 oracle as the checker of a few orientations after timing
     cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
     cpu = cpu_baseline(inp, sample=args.cpu_sample) if cpu_leg else None
-    acc = accuracy_vs_fp64(sc, inp, args.accuracy) if (cpu_leg and args.accuracy > 0) else None
+    acc = accuracy_vs_fp64(sc, inp, args.accuracy) if (rank == 0 and world == 1 and args.accuracy > 0) else None
     prep_dev = preparation_ms(inp, local) if rank == 0 else None
     sc.close()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "warmup": args.warmup, "ms_per_step": dev["dev_ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if precision == core.PRECISION_FP32 else "f16",
+            "data": "synthetic",
             "config": {"workload": WORKLOAD["name"], "micrograph": [WORKLOAD["nx"], WORKLOAD["ny"]],
                        "padded": [X, Y], "template": T, "orientations_per_step": per_step,
                        "grid_orientations": n_orient_total, "orientation_batch": nb,
                        "orientation_batch_autotuned": args.batch == 0,
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2: each batch writes a %.1f GB intermediate" % (nb * Y * (X // 2 + 4) * 8 / 1e9)},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "host_threads": n_ctx},
+            "e2e": {"value": world * npix_orig * e2e["n_done"] / e2e["e2e_s"], "unit": UNIT,
+                    "h2d_bytes_per_step": int(e2e["h2d"]), "d2h_bytes_per_step": int(e2e["d2h"]),
+                    "host_threads": e2e["host_threads"]},
             "gpu_launches": int(6 * np.ceil(per_step / nb) * args.steps),
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
                          "frac": ach / hbm_peak, "traffic": traffic, "peak_source": peak_kind,
                          "ms_per_launch": {"k_pass_b": b_launch_ms, "k_pass_c": c_launch_ms,
-                                           "prep_kernels": prep_ms / max(n_launch, 1)}},
-            "clocks": clk.summary(),
-            "wall_ms_timed_region": wall_ms,
+                                           "prep_kernels": dev["prep_ms"] / max(n_launch, 1)}},
+            "clocks": dev["clocks"],
+            "wall_ms_timed_region": dev["wall_ms"],
         }
+        if fp16 is not None:
+            line["fp16"] = fp16
         if cpu is not None:
             line["cpu_baseline"] = cpu
         if acc is not None:
@@ -756,6 +840,8 @@ def main():
                     help="fp32 = the parity path; fp16 = FP16 correlation spectra with the tensor-core row transform")
     ap.add_argument("--cpu-sample", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp16-leg", action="store_true",
+                    help="skip the FP16 tensor-core form that the default run times beside the FP32 path")
     ap.add_argument("--accuracy", type=int, default=4,
                     help="orientations compared with the FP64 oracle after timing, in the CPU-baseline leg (0 = skip)")
     ap.add_argument("--workload", default="full", choices=sorted(WORKLOADS) + ["batched", "refine", "proposal"],

@@ -280,7 +280,7 @@ struct TcImpl {
         if (ev) cudaEventRecord(ev[0], s);
         LN::prep(a, s);
         if (ev) cudaEventRecord(ev[1], s);
-        LT::pass_b(a, s, c->nsm);
+        LT::pass_b(a, s, c->nsm, c->dft);
         if (ev) cudaEventRecord(ev[2], s);
         LT::pass_c(a, s, c->dft);
         if (ev) cudaEventRecord(ev[3], s);
@@ -440,9 +440,16 @@ tmk::BatchArgs make_args(tm_ctx* c) {
     a.twy.lmax = c->Y;
     a.twt.tab = c->twt;
     a.twt.lmax = c->T;
-    // FP16 form: correlation spectra times 2^e with 2^e ~ sqrt(X Y), so that the
-    // row outputs (correlation values ~ 1/sqrt(X Y)) are O(1) in FP16
-    a.half_scale_exp = (int)lround(0.5 * log2((double)c->X * (double)c->Y));
+    // FP16 form (powers of two): the correlation values are ~ 1/sqrt(N), N = X Y,
+    // and the column-transformed spectra ~ 1/sqrt(N X); they are stored times
+    // 2^e ~ sqrt(N X) so that the FP16 values are O(1).  The column pass holds I'
+    // (~ N^-1.5) times 2^iexp ~ N^1.5 and its stage-1 operand Z (~ 1/N) times N.
+    {
+        const double l2n = log2((double)c->X * (double)c->Y);
+        a.half_scale_exp = (int)lround(0.5 * (l2n + log2((double)c->X)));
+        a.tc_iexp = (int)lround(1.5 * l2n);
+        a.tc_zexp = (int)lround(l2n);
+    }
     return a;
 }
 

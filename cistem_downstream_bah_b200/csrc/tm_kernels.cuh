@@ -79,6 +79,7 @@ struct BatchArgs {
     int hist_bins;
     int* err;                     // device error flag (a bounded wait ran out)
     int half_scale_exp;           // FP16 form: the correlation spectra are stored times 2^half_scale_exp
+    int tc_iexp, tc_zexp;         // FP16 column pass: I' held times 2^tc_iexp, stage-1 operand Z times 2^tc_zexp
     long long norm_pixels;        // pixel count of the projection variance (0: X*Y, the box;
                                   // a window of a larger micrograph passes the micrograph's)
     int XP;                       // row pitch (complex values) of A, C and Ip: X/2+1 rounded
@@ -911,20 +912,37 @@ struct LaunchTc {
     using PB = PassB<T, Y>;
     using PCT = PassCTc<X>;
     static constexpr int R = PCT::R;
+    // height 4096: the tensor-core column pass; other heights: the FP32 column FFTs with FP16 output
+    static constexpr bool COL_TC = (Y == 4096);
+    using PBT = PassBTc<T, R>;
+    static constexpr size_t rows_tab_bytes = (size_t)PCT::B1_BYTES + PCT::B2_BYTES;
     static cudaError_t configure(int XP, int bins) {
-        cudaError_t e = cudaFuncSetAttribute(k_pass_b<T, Y, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB::SMEM);
+        cudaError_t e;
+        if constexpr (COL_TC)
+            e = cudaFuncSetAttribute(k_pass_b_tc<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, PBT::SMEM);
+        else
+            e = cudaFuncSetAttribute(k_pass_b<T, Y, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB::SMEM);
         if (e != cudaSuccess) return e;
         return cudaFuncSetAttribute(k_pass_c_tc<X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PCT::smem_bytes(XP, bins));
     }
-    static void pass_b(BatchArgs& a, cudaStream_t s, int nsm) {
-        const int n_items = (a.XP / PB::WG) * a.nb;
-        k_pass_b<T, Y, R><<<n_items < nsm ? n_items : nsm, PB::NT, PB::SMEM, s>>>(a, n_items);
+    static void pass_b(BatchArgs& a, cudaStream_t s, int nsm, const uint4* tabs) {
+        if constexpr (COL_TC) {
+            const int n_items = (a.XP / 4) * a.nb;
+            k_pass_b_tc<T, R><<<n_items < nsm ? n_items : nsm, PBT::NT, PBT::SMEM, s>>>(a, n_items, tabs + rows_tab_bytes / 16);
+        } else {
+            const int n_items = (a.XP / PB::WG) * a.nb;
+            k_pass_b<T, Y, R><<<n_items < nsm ? n_items : nsm, PB::NT, PB::SMEM, s>>>(a, n_items);
+        }
     }
     static void pass_c(BatchArgs& a, cudaStream_t s, const uint4* dft) {
         k_pass_c_tc<X><<<Y / R, PCT::NT, PCT::smem_bytes(a.XP, a.hist_bins), s>>>(a, Y, dft);
     }
-    static constexpr size_t dft_bytes = (size_t)PCT::B1_BYTES + PCT::B2_BYTES;
-    static void fill_dft(uint16_t* host) { fill_tc_dft<X>(host); }
+    // the row pass's DFT operands, then (height 4096) the column pass's
+    static constexpr size_t dft_bytes = rows_tab_bytes + (COL_TC ? PBT::dft_bytes : 0);
+    static void fill_dft(uint16_t* host) {
+        fill_tc_dft<X>(host);
+        if constexpr (COL_TC) fill_tc_cols<T, R>(host + rows_tab_bytes / 2);
+    }
 };
 
 }  // namespace tmk

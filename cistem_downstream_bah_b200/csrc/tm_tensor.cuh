@@ -424,4 +424,347 @@ k_pass_c_tc(BatchArgs a, int Y, const uint4* __restrict__ dft) {
     }
 }
 
+// ======================================================================================
+// k_pass_b_tc: the column pass on the tensor cores (FP16 form, height Y = 4096).
+//
+// Work item = 4 adjacent columns kx0..kx0+3 of one orientation (items ordered
+// orientation-fastest, so a block keeps the prepared micrograph spectrum I' of
+// its column group in shared memory, FP16, across orientations).  Per column
+// (a "vector"), with n = n1 + 64 n2 (n < T, the non-zero rows of A),
+// ky = a + 64 b and y = n2' + 64 n1':
+//
+//   stage H (MMA)  h[a][n1] = sum_n2 A[n1 + 64 n2] exp(-2 pi i n2 a / 64):
+//                  one 128 x 256 x 16 MMA for the 4 columns, A = the sparse
+//                  DFT E[(a, re/im)][(n2, re/im)], B = the data, N = (column, n1)
+//   epilogue H     lane pairs (a, re), (a, im) combine; g = h exp(-2 pi i n1 a / Y)
+//   stage F (MMA)  F[a + 64 b] = sum_n1 g[a][n1] exp(-2 pi i n1 b / 64), two
+//                  128 x 128 x 128 MMAs (M = (column of the pair, a))
+//   epilogue F     Z = I' conj(F) (the conjugate multiply of pass B), written
+//                  conjugated as the A operand of stage 1
+//   stage 1 (MMA)  conj(sum_k2 conj(Z[k1 + 64 k2]) exp(-2 pi i k2 n2 / 64))
+//   epilogue 1     twiddle exp(+2 pi i k1 n2 / Y), conjugated, MN-major A of stage 2
+//   stage 2 (MMA)  z[n2 + 64 n1] = conj(sum_k1 ... exp(-2 pi i k1 n1 / 64))
+//   epilogue 2     FP16 into a shared staging tile, then the item's 4 columns go
+//                  to C16[o][y / RB][kx][y % RB] in whole 32-byte sectors
+//
+// Complex values are 2 x 2 real blocks along K and N, so every TMEM lane holds
+// whole complex outputs (stage H excepted: its lanes hold real or imaginary
+// parts and pair up by shuffles).  One FP16 DFT matrix (the forward 64-point
+// DFT) serves stages F, 1 and 2; the inverse stages apply it to conjugates.
+// Scales (powers of two): the data enter stage H times 2^-6, I' is held
+// times 2^iexp (~ N^1.5), the stage-1 operand is Z N, and the stored spectra
+// are C 2^half_scale_exp, as k_pass_c_tc expects.
+template <int T, int RB>
+struct PassBTc {
+    static constexpr int Y = 4096;
+    static constexpr int NB = (T + 63) / 64;            // non-zero residues n2
+    static constexpr int NT = 512;
+    static constexpr int E_SBO = 128, E_LBO = 16 * 128;          // stage-H A: K-major, M 128, K 16
+    static constexpr int BH_SBO = 128, BH_LBO = 32 * 128;        // stage-H B: MN-major, N 256, K 16
+    static constexpr int BF_SBO = 128, BF_LBO = 16 * 128;        // DFT B: K-major, N 128, K 128
+    static constexpr int AK_SBO = 128, AK_LBO = 16 * 128;        // K-major A (stages F, 1)
+    static constexpr int AM_SBO = 128, AM_LBO = 16 * 128 + 16;   // MN-major A (stage 2), K groups skewed
+    static constexpr int E_BYTES = 2 * E_LBO;
+    static constexpr int BF_BYTES = 16 * BF_LBO;
+    static constexpr int BH_BYTES = 2 * BH_LBO;
+    static constexpr int OP_TILE = 16 * AM_LBO;                  // >= 16 * AK_LBO
+    static constexpr int OFF_E = 128;
+    static constexpr int OFF_BF = OFF_E + E_BYTES;
+    static constexpr int OFF_BH = OFF_BF + BF_BYTES;
+    static constexpr int OFF_OP = OFF_BH + BH_BYTES;
+    static constexpr int OFF_I = OFF_OP + 2 * OP_TILE;
+    static constexpr int SMEM = OFF_I + 4 * Y * 4;
+    static constexpr uint32_t TMEM_COLS = 256;
+    static_assert(2 * NB <= 16, "stage H takes at most 8 residues (T <= 512)");
+    static_assert(2 * OP_TILE >= 4 * Y * 4, "the operand buffer doubles as the output staging tile");
+    static_assert(SMEM <= 232448, "pass B tensor block exceeds shared memory");
+    static constexpr size_t dft_bytes = (size_t)E_BYTES + BF_BYTES;
+};
+
+__host__ __device__ constexpr int kmaj_off(int m, int k, int sbo, int lbo) {
+    return (m % 8) * 16 + (k % 8) * 2 + (m / 8) * sbo + (k / 8) * lbo;
+}
+__host__ __device__ constexpr int mnmaj_off(int m, int k, int sbo, int lbo) {
+    return (m % 8) * 2 + (k % 8) * 16 + (m / 8) * sbo + (k / 8) * lbo;
+}
+
+// E (stage-H A operand) then the forward 64-point DFT (B operand of stages F,
+// 1 and 2), FP16, in the kernel's shared-memory byte layout.
+template <int T, int RB>
+void fill_tc_cols(uint16_t* out) {
+    using PB = PassBTc<T, RB>;
+    auto put = [](uint16_t* base, int off, double v) {
+        const __half h = __double2half(v);
+        base[off / 2] = *reinterpret_cast<const uint16_t*>(&h);
+    };
+    for (size_t i = 0; i < PB::dft_bytes / 2; i++) out[i] = 0;
+    uint16_t* e = out;
+    uint16_t* bf = out + PB::E_BYTES / 2;
+    for (int a = 0; a < 64; a++)
+        for (int n2 = 0; n2 < PB::NB; n2++) {
+            const double th = 2.0 * M_PI * (double)((n2 * a) % 64) / 64.0, c = cos(th), s = sin(th);
+            // h = sum A exp(-i th): re = Ar c + Ai s, im = Ai c - Ar s
+            put(e, kmaj_off(2 * a, 2 * n2, PB::E_SBO, PB::E_LBO), c);
+            put(e, kmaj_off(2 * a, 2 * n2 + 1, PB::E_SBO, PB::E_LBO), s);
+            put(e, kmaj_off(2 * a + 1, 2 * n2, PB::E_SBO, PB::E_LBO), -s);
+            put(e, kmaj_off(2 * a + 1, 2 * n2 + 1, PB::E_SBO, PB::E_LBO), c);
+        }
+    for (int n1 = 0; n1 < 64; n1++)
+        for (int b = 0; b < 64; b++) {
+            const double th = 2.0 * M_PI * (double)((n1 * b) % 64) / 64.0, c = cos(th), s = sin(th);
+            put(bf, kmaj_off(2 * b, 2 * n1, PB::BF_SBO, PB::BF_LBO), c);
+            put(bf, kmaj_off(2 * b, 2 * n1 + 1, PB::BF_SBO, PB::BF_LBO), s);
+            put(bf, kmaj_off(2 * b + 1, 2 * n1, PB::BF_SBO, PB::BF_LBO), -s);
+            put(bf, kmaj_off(2 * b + 1, 2 * n1 + 1, PB::BF_SBO, PB::BF_LBO), c);
+        }
+}
+
+__device__ __forceinline__ float2 h2f(uint32_t bits) {
+    __half2 h = *reinterpret_cast<const __half2*>(&bits);
+    return __half22float2(h);
+}
+
+template <int T, int RB>
+__global__ void __launch_bounds__(512, 1)
+k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
+    using PB = PassBTc<T, RB>;
+    constexpr int Y = PB::Y;
+    constexpr uint32_t kWaitLimit = 1u << 24;
+    const int XP = a.XP;
+    extern __shared__ __align__(128) unsigned char smem_b16[];
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_b16);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem_b16 + 64);
+    unsigned char* sE = smem_b16 + PB::OFF_E;
+    unsigned char* sBF = smem_b16 + PB::OFF_BF;
+    unsigned char* sBH = smem_b16 + PB::OFF_BH;
+    unsigned char* sOP = smem_b16 + PB::OFF_OP;
+    uint32_t* sI = reinterpret_cast<uint32_t*>(smem_b16 + PB::OFF_I);   // I' as FP16 complex, [column][ky]
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int q = warp & 3, sub = warp >> 2;
+    const int m = 32 * q + lane;            // TMEM lane of this thread
+    const int per = (n_items + gridDim.x - 1) / gridDim.x;
+    const int it0 = blockIdx.x * per;
+    const int it1 = min(n_items, it0 + per);
+    if (it0 >= it1) return;
+    if (t == 0) tmptx::mbar_init(&mbar[0], 1);
+    if (warp == 0) {
+        tmptx::tmem_alloc(tmem_slot, PB::TMEM_COLS);
+        tmptx::tmem_relinquish();
+    }
+    for (int i = t; i < (PB::E_BYTES + PB::BF_BYTES) / 16; i += PB::NT) reinterpret_cast<uint4*>(sE)[i] = __ldg(tabs + i);
+    // stage-H data rows beyond 2 NB multiply zero columns of E and must be finite
+    for (int i = t; i < PB::BH_BYTES / 16; i += PB::NT) reinterpret_cast<uint4*>(sBH)[i] = make_uint4(0, 0, 0, 0);
+    tmptx::fence_proxy_async_smem();
+    tmptx::tmem_fence_before_sync();
+    __syncthreads();
+    tmptx::tmem_fence_after_sync();
+    const uint32_t tbase = *tmem_slot;
+    const uint32_t tlane = (uint32_t)(32 * q) << 16;
+    const float sA = 1.0f / 64.0f;
+    const float sI_scale = exp2f((float)a.tc_iexp);
+    const float sZ = exp2f((float)(a.tc_zexp - a.tc_iexp + 6));     // Z N = I'_held conj(F_held) 2^(6 - iexp + zexp)
+    const float sOut = exp2f((float)(a.half_scale_exp - a.tc_zexp));
+    const uint32_t idH = tmptx::idesc_f16_f32(128, 256, false, true);
+    const uint32_t idK = tmptx::idesc_f16_f32(128, 128, false, false);
+    const uint32_t idM = tmptx::idesc_f16_f32(128, 128, true, false);
+    const uint32_t e_addr = tmptx::smem_u32(sE), bf_addr = tmptx::smem_u32(sBF), bh_addr = tmptx::smem_u32(sBH);
+    const uint32_t op_addr = tmptx::smem_u32(sOP);
+    bool timed_out = false, mma_pending = false;
+    uint32_t phase = 0;
+    int cur_group = -1;
+    // one MMA group: thread 0 issues, every thread waits for its completion
+    auto wait_mma = [&]() {
+        mma_pending = true;
+        if (tmptx::mbar_wait_bounded(&mbar[0], phase & 1, kWaitLimit)) {
+            mma_pending = false;
+        } else {
+            timed_out = true;
+            atomicExch(a.err, 1);
+        }
+        phase++;
+        tmptx::tmem_fence_after_sync();
+    };
+    auto issue_pair = [&](int a_off_bytes, int a_lbo, int a_sbo, uint32_t idesc) {
+        // D_tile = A_tile (128 x 128) x DFT (128 x 128) for the two tiles
+        tmptx::tmem_fence_after_sync();
+#pragma unroll 1
+        for (int tt = 0; tt < 2; tt++)
+#pragma unroll
+            for (int kk = 0; kk < 8; kk++)
+                tmptx::mma_f16_ss(tbase + 128 * tt,
+                                  tmptx::smem_desc_noswizzle(op_addr + tt * PB::OP_TILE + a_off_bytes + kk * 2 * a_lbo,
+                                                             a_lbo, a_sbo),
+                                  tmptx::smem_desc_noswizzle(bf_addr + kk * 2 * PB::BF_LBO, PB::BF_LBO, PB::BF_SBO), idesc,
+                                  kk > 0);
+        tmptx::mma_commit(&mbar[0]);
+    };
+    for (int it = it0; it < it1; it++) {
+        const int group = it / a.nb, o = it % a.nb;
+        const int kx0 = group * 4;
+        // every thread is done with the previous item's staging tile and I'
+        if (__syncthreads_or(timed_out)) break;
+        if (group != cur_group) {
+            // I' of the 4 columns, FP16 times 2^iexp, [column][ky]
+#pragma unroll 4
+            for (int i = t; i < 4 * Y; i += PB::NT) {
+                const int c = i & 3, ky = i >> 2;
+                const float2 v = __ldg(a.Ip + (size_t)ky * XP + kx0 + c);
+                sI[c * Y + ky] = h2_bits(v.x * sI_scale, v.y * sI_scale);
+            }
+            cur_group = group;
+        }
+        // stage-H data: A[o][n][kx0 + c] times 2^-6 -> BH[(n2, re/im)][(c, n1)]
+        {
+            const float2* Ao = a.A + (size_t)o * T * XP + kx0;
+            for (int i = t; i < 4 * T; i += PB::NT) {
+                const int c = i & 3, n = i >> 2;
+                const float2 v = __ldg(Ao + (size_t)n * XP + c);
+                const int nn = 64 * c + (n & 63), n2 = n >> 6;
+                *reinterpret_cast<__half*>(sBH + mnmaj_off(nn, 2 * n2, PB::BH_SBO, PB::BH_LBO)) = __float2half_rn(v.x * sA);
+                *reinterpret_cast<__half*>(sBH + mnmaj_off(nn, 2 * n2 + 1, PB::BH_SBO, PB::BH_LBO)) = __float2half_rn(v.y * sA);
+            }
+        }
+        tmptx::fence_proxy_async_smem();
+        tmptx::tmem_fence_before_sync();
+        if (__syncthreads_or(timed_out)) break;
+        if (t == 0) {
+            tmptx::tmem_fence_after_sync();
+            tmptx::mma_f16_ss(tbase, tmptx::smem_desc_noswizzle(e_addr, PB::E_LBO, PB::E_SBO),
+                              tmptx::smem_desc_noswizzle(bh_addr, PB::BH_LBO, PB::BH_SBO), idH, false);
+            tmptx::mma_commit(&mbar[0]);
+        }
+        wait_mma();
+        // ---- epilogue H: lane m = (a, p); columns (v = sub, n1); p = 0 keeps n1 < 32, p = 1 the rest
+        {
+            const int p = m & 1, av = m >> 1, v = sub;
+            const int tt = v >> 1, vl = v & 1;
+#pragma unroll 1
+            for (int j = 0; j < 2; j++) {
+                float lo[16], hi[16];
+                tmptx::tmem_ld16(tbase + tlane + 64 * v + 16 * j, lo);        // n1 = 16 j + i
+                tmptx::tmem_ld16(tbase + tlane + 64 * v + 32 + 16 * j, hi);   // n1 = 32 + 16 j + i
+                tmptx::tmem_wait_ld16(lo);
+                tmptx::tmem_wait_ld16(hi);
+                const int n1_0 = 32 * p + 16 * j;
+                uint32_t packed[16];
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    const float r = __shfl_xor_sync(0xffffffffu, p ? lo[i] : hi[i], 1);
+                    const float2 h = p ? make_float2(r, hi[i]) : make_float2(lo[i], r);
+                    const float2 g = cmul(h, a.twy.template w<-1>((n1_0 + i) * av, Y));
+                    packed[i] = h2_bits(g.x, g.y);
+                }
+                unsigned char* dst = sOP + tt * PB::OP_TILE;
+                const int mF = 64 * vl + av;
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+                    *reinterpret_cast<uint4*>(dst + kmaj_off(mF, 2 * n1_0 + 8 * r, PB::AK_SBO, PB::AK_LBO)) =
+                        make_uint4(packed[4 * r], packed[4 * r + 1], packed[4 * r + 2], packed[4 * r + 3]);
+            }
+        }
+        tmptx::fence_proxy_async_smem();
+        tmptx::tmem_fence_before_sync();
+        if (__syncthreads_or(timed_out)) break;
+        if (t == 0) issue_pair(0, PB::AK_LBO, PB::AK_SBO, idK);
+        wait_mma();
+        // ---- epilogue F: lane m = (vl, a); tile tt = sub / 2, b in [32 (sub & 1), +32)
+        const int tt = sub >> 1, vl = m >> 6, av = m & 63;
+        const int v = 2 * tt + vl;
+        unsigned char* tile = sOP + tt * PB::OP_TILE;
+        const uint32_t tcol = tbase + tlane + 128 * tt;
+#pragma unroll 1
+        for (int j = 0; j < 2; j++) {
+            const int b0 = 32 * (sub & 1) + 16 * j;
+            float d[32];
+            tmptx::tmem_ld16(tcol + 2 * b0, d);
+            tmptx::tmem_ld16(tcol + 2 * b0 + 16, d + 16);
+            tmptx::tmem_wait_ld32(d);
+            uint32_t packed[16];
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                const float2 iv = h2f(sI[v * Y + av + 64 * (b0 + i)]);
+                const float2 z = cmul_conj(iv, make_float2(d[2 * i], d[2 * i + 1]));
+                packed[i] = h2_bits(z.x * sZ, -z.y * sZ);      // conj(Z) for the inverse stages
+            }
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+                *reinterpret_cast<uint4*>(tile + kmaj_off(m, 2 * b0 + 8 * r, PB::AK_SBO, PB::AK_LBO)) =
+                    make_uint4(packed[4 * r], packed[4 * r + 1], packed[4 * r + 2], packed[4 * r + 3]);
+        }
+        tmptx::fence_proxy_async_smem();
+        tmptx::tmem_fence_before_sync();
+        if (__syncthreads_or(timed_out)) break;
+        if (t == 0) issue_pair(0, PB::AK_LBO, PB::AK_SBO, idK);
+        wait_mma();
+        // ---- epilogue 1: lane m = (vl, k1); Y = conj(D1), Y' = Y exp(+2 pi i k1 n2 / Y), A2 = conj(Y') MN-major
+#pragma unroll 1
+        for (int j = 0; j < 2; j++) {
+            const int n2_0 = 32 * (sub & 1) + 16 * j;
+            float d[32];
+            tmptx::tmem_ld16(tcol + 2 * n2_0, d);
+            tmptx::tmem_ld16(tcol + 2 * n2_0 + 16, d + 16);
+            tmptx::tmem_wait_ld32(d);
+            float re[16], im[16];
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                const float2 yv = cmul(make_float2(d[2 * i], -d[2 * i + 1]), a.twy.template w<+1>(av * (n2_0 + i), Y));
+                re[i] = yv.x;
+                im[i] = -yv.y;
+            }
+            // K index 2 k1 (re) and 2 k1 + 1 (im); M = 64 vl + n2, 8 per 16-byte row
+#pragma unroll
+            for (int g = 0; g < 2; g++) {
+                const int m2 = 64 * vl + n2_0 + 8 * g;
+                *reinterpret_cast<uint4*>(tile + mnmaj_off(m2, 2 * av, PB::AM_SBO, PB::AM_LBO)) =
+                    make_uint4(h2_bits(re[8 * g], re[8 * g + 1]), h2_bits(re[8 * g + 2], re[8 * g + 3]),
+                               h2_bits(re[8 * g + 4], re[8 * g + 5]), h2_bits(re[8 * g + 6], re[8 * g + 7]));
+                *reinterpret_cast<uint4*>(tile + mnmaj_off(m2, 2 * av + 1, PB::AM_SBO, PB::AM_LBO)) =
+                    make_uint4(h2_bits(im[8 * g], im[8 * g + 1]), h2_bits(im[8 * g + 2], im[8 * g + 3]),
+                               h2_bits(im[8 * g + 4], im[8 * g + 5]), h2_bits(im[8 * g + 6], im[8 * g + 7]));
+            }
+        }
+        tmptx::fence_proxy_async_smem();
+        tmptx::tmem_fence_before_sync();
+        if (__syncthreads_or(timed_out)) break;
+        if (t == 0) issue_pair(0, PB::AM_LBO, PB::AM_SBO, idM);
+        wait_mma();
+        // ---- epilogue 2 (stage 2 has read A2: the tiles become the staging area): lane m = (vl, n2); z[n2 + 64 n1] = conj(D2) -> staging [column][y], FP16
+        uint32_t* stage = reinterpret_cast<uint32_t*>(sOP);
+#pragma unroll 1
+        for (int j = 0; j < 2; j++) {
+            const int n1_0 = 32 * (sub & 1) + 16 * j;
+            float d[32];
+            tmptx::tmem_ld16(tcol + 2 * n1_0, d);
+            tmptx::tmem_ld16(tcol + 2 * n1_0 + 16, d + 16);
+            tmptx::tmem_wait_ld32(d);
+#pragma unroll
+            for (int i = 0; i < 16; i++)
+                stage[v * Y + av + 64 * (n1_0 + i)] = h2_bits(d[2 * i] * sOut, -d[2 * i + 1] * sOut);
+        }
+        tmptx::tmem_fence_before_sync();
+        if (__syncthreads_or(timed_out)) break;
+        // ---- the item's columns to C16[o][y / RB][kx][y % RB]: 16-byte chunks of 4 (column, row) values
+        {
+            __half2* C16 = reinterpret_cast<__half2*>(a.C) + (size_t)o * Y * XP;
+            for (int ch = t; ch < Y; ch += PB::NT) {
+                // chunk ch: row block rb, elements e = 4 (ch % RB) .. + 3 of its 4 RB (column, row) values
+                const int rb = ch / RB, e0 = 4 * (ch % RB);
+                uint32_t w4[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const int c = (e0 + e) / RB, r = (e0 + e) % RB;
+                    w4[e] = stage[c * Y + rb * RB + r];
+                }
+                *reinterpret_cast<uint4*>(C16 + ((size_t)rb * XP + kx0) * RB + e0) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+            }
+        }
+    }
+    const bool failed = __syncthreads_or(timed_out);
+    if (failed && mma_pending) tmptx::mbar_wait_bounded(&mbar[0], (phase - 1) & 1, kWaitLimit);
+    tmptx::tmem_fence_before_sync();
+    __syncthreads();
+    tmptx::tmem_fence_after_sync();
+    if (warp == 0) tmptx::tmem_dealloc(tbase, PB::TMEM_COLS);
+}
+
 }  // namespace tmk
