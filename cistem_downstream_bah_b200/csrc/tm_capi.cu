@@ -21,6 +21,7 @@
 #include "tm_kernels.cuh"
 #include "tm_whiten.cuh"
 #include "tm_template.cuh"
+#include "tm_generic.cuh"
 
 namespace tmcg {
 #include "tm_gemm.cuh"
@@ -62,6 +63,7 @@ struct tm_ctx {
     int* err_flag = nullptr;
     int* best_host = nullptr;   // page-locked copy of the best-orientation map (tm_get_results)
     int precision = TM_PRECISION_FP32;
+    tmk::GenPlan gen_px{}, gen_py{}, gen_ph{};   // radix plans of X, Y and X/2 (sizes without compiled kernels)
     uint4* dft = nullptr;       // DFT operands of the tensor-core row pass (FP16 form)
     long long rot_capacity = 0;
     bool has_template = false, has_image = false;
@@ -116,6 +118,7 @@ struct WhitenBuffers {
     double* scratch;      // 3 + 3 * npts doubles
     float* xs;            // npts abscissae
     tmfft::Twiddles twx, twy;
+    int X, Y;             // sizes (read by the run-time-length whitening)
 };
 using WhitenFn = int (*)(cudaStream_t, int nsm, const WhitenBuffers&, std::vector<double>& curve, std::string& err);
 
@@ -150,8 +153,11 @@ int curve_points(int X) { return (int)((X / 2.0 + 1.0) * sqrtf(2.0f) + 1.0); }
         }                                                                            \
     } while (0)
 
-template <int X, int Y>
-int whiten_on_device(cudaStream_t s, int nsm, const WhitenBuffers& b, std::vector<double>& curve, std::string& err) {
+// The whitening steps around the two transforms; `transforms(mean, vmin, vmax)`
+// launches the row r2c and the column FFT with the quadrant swap.
+template <class Transforms>
+int whiten_steps(cudaStream_t s, int nsm, const WhitenBuffers& b, int X, int Y, std::vector<double>& curve,
+                 std::string& err, Transforms transforms) {
     const int hc = X / 2 + 1;
     const long long n = (long long)X * Y;
     const int npts = curve_points(X);
@@ -169,13 +175,7 @@ int whiten_on_device(cudaStream_t s, int nsm, const WhitenBuffers& b, std::vecto
     const float mean = (float)(st[0] / n);
     const float sigma = sqrtf(fabsf((float)(st[1] / n - (st[0] / n) * (st[0] / n))));
     const float vmax = mean + 5.0f * sigma, vmin = mean - 5.0f * sigma;
-    using R = tmw::WRows<X>;
-    using C = tmw::WCols<Y>;
-    tmw::k_w_rows<X><<<(Y + R::ROWS - 1) / R::ROWS, R::NT, 0, s>>>(b.img, b.spec, Y, mean, vmin, vmax, b.twx);
-    TW_CHECK(cudaGetLastError());
-    if (C::SMEM > 48 * 1024) TW_CHECK(cudaFuncSetAttribute(tmw::k_w_cols<Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
-    tmw::k_w_cols<Y><<<(hc + C::CB - 1) / C::CB, C::NT, C::SMEM, s>>>(b.spec, X, b.twy);
-    TW_CHECK(cudaGetLastError());
+    TW_CHECK(transforms(mean, vmin, vmax));
     // the curve's abscissae (Curve::SetupXAxis(0, sqrt(2)/2, npts)), float
     const float hi = 0.5f * sqrtf(2.0f);
     std::vector<float> xs(npts);
@@ -209,6 +209,48 @@ int whiten_on_device(cudaStream_t s, int nsm, const WhitenBuffers& b, std::vecto
     TW_CHECK(cudaGetLastError());
     TW_CHECK(cudaStreamSynchronize(s));
     return TM_OK;
+}
+
+template <int X, int Y>
+int whiten_on_device(cudaStream_t s, int nsm, const WhitenBuffers& b, std::vector<double>& curve, std::string& err) {
+    return whiten_steps(s, nsm, b, X, Y, curve, err, [&](float mean, float vmin, float vmax) {
+        using R = tmw::WRows<X>;
+        using C = tmw::WCols<Y>;
+        constexpr int hc = X / 2 + 1;
+        tmw::k_w_rows<X><<<(Y + R::ROWS - 1) / R::ROWS, R::NT, 0, s>>>(b.img, b.spec, Y, mean, vmin, vmax, b.twx);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        if (C::SMEM > 48 * 1024) {
+            e = cudaFuncSetAttribute(tmw::k_w_cols<Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+            if (e != cudaSuccess) return e;
+        }
+        tmw::k_w_cols<Y><<<(hc + C::CB - 1) / C::CB, C::NT, C::SMEM, s>>>(b.spec, X, b.twy);
+        return cudaGetLastError();
+    });
+}
+
+// any size whose sides have radix plans (tm_generic.cuh)
+int whiten_generic(cudaStream_t s, int nsm, const WhitenBuffers& b, std::vector<double>& curve, std::string& err) {
+    const int X = b.X, Y = b.Y;
+    const bool odd = X % 2 != 0;
+    tmk::GenPlan ph, py;
+    if (!tmk::gen_plan(odd ? X : X / 2, ph) || !tmk::gen_plan(Y, py)) {
+        err = "no radix plan for the micrograph size";
+        return TM_ERR_UNSUPPORTED;
+    }
+    return whiten_steps(s, nsm, b, X, Y, curve, err, [&](float mean, float vmin, float vmax) {
+        const int smem_r = (int)sizeof(float2) * 2 * ph.L, smem_c = (int)sizeof(float2) * 2 * Y;
+        auto rows = odd ? tmk::k_w_rows_gen<true> : tmk::k_w_rows_gen<false>;
+        cudaError_t e = cudaFuncSetAttribute(rows, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_r);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(tmk::k_w_cols_gen, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_c);
+        if (e != cudaSuccess) return e;
+        rows<<<Y, tmk::kGenNT, smem_r, s>>>(b.img, b.spec, X, mean, vmin, vmax, b.twx, ph);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        tmk::k_w_cols_gen<<<X / 2 + 1, tmk::kGenNT, smem_c, s>>>(b.spec, X, Y, b.twy, py);
+        return cudaGetLastError();
+    });
 }
 
 template <int T, int X, int Y>
@@ -291,6 +333,78 @@ struct TcImpl {
     static constexpr TensorForm form = {&TcImpl::configure, &TcImpl::run_batch, LT::dft_bytes, &LT::fill_dft};
 };
 
+// Sizes without compiled kernels: the slice and projection kernels of the
+// template box T and the run-time-length passes of tm_generic.cuh.
+template <int T>
+struct GenImpl {
+    static int configure(tm_ctx* c) {
+        TM_CUDA(c, cudaFuncSetAttribute(tmk::k_pass_a_gen<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sizeof(float2) * 2 * c->X));
+        TM_CUDA(c, cudaFuncSetAttribute(tmk::k_pass_b_gen, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sizeof(float2) * 2 * c->Y));
+        TM_CUDA(c, cudaFuncSetAttribute(tmk::k_pass_c_gen<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sizeof(float2) * 2 * c->X + 4 * c->d.histogram_bins));
+        TM_CUDA(c, cudaFuncSetAttribute(tmk::k_pass_c_gen<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)sizeof(float2) * c->X + 4 * c->d.histogram_bins));
+        return TM_OK;
+    }
+    static void prep(tm_ctx* c, tmk::BatchArgs& a, cudaStream_t s) {
+        using SC = tmk::SliceCol<T>;
+        using RC = tmk::RowC2R<T>;
+        tmk::k_slice_colfft<T><<<dim3((T / 2 + 1 + SC::CB - 1) / SC::CB, a.nb), SC::NT, 0, s>>>(a);
+        tmk::k_row_c2r<T><<<dim3(T / RC::ROWS, a.nb), RC::NT, 0, s>>>(a);
+        tmk::k_norm<T><<<(a.nb + 7) / 8, 256, 0, s>>>(a, a.norm_pixels > 0 ? a.norm_pixels : (long long)c->X * c->Y);
+        tmk::k_pass_a_gen<T><<<dim3(T, a.nb), tmk::kGenNT, sizeof(float2) * 2 * c->X, s>>>(a, c->X, c->gen_px);
+    }
+    static void pass_b(tm_ctx* c, tmk::BatchArgs& a, cudaStream_t s) {
+        tmk::k_pass_b_gen<<<dim3(a.XP, a.nb), tmk::kGenNT, sizeof(float2) * 2 * c->Y, s>>>(a, T, c->Y, c->gen_py);
+    }
+    static void pass_c(tm_ctx* c, tmk::BatchArgs& a, cudaStream_t s) {
+        if (c->X % 2)
+            tmk::k_pass_c_gen<true><<<c->Y, tmk::kGenNT, sizeof(float2) * 2 * c->X + 4 * a.hist_bins, s>>>(a, c->X, c->Y,
+                                                                                                      c->gen_ph);
+        else
+            tmk::k_pass_c_gen<false><<<c->Y, tmk::kGenNT, sizeof(float2) * c->X + 4 * a.hist_bins, s>>>(a, c->X, c->Y,
+                                                                                                       c->gen_ph);
+    }
+    static int done(tm_ctx* c) {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return set_err(c, TM_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+        return TM_OK;
+    }
+    static int run_stages(tm_ctx* c, tmk::BatchArgs& a) {
+        prep(c, a, c->stream);
+        pass_b(c, a, c->stream);
+        return done(c);
+    }
+    static int run_batch(tm_ctx* c, tmk::BatchArgs& a, cudaEvent_t* ev) {
+        cudaStream_t s = c->stream;
+        if (ev) cudaEventRecord(ev[0], s);
+        prep(c, a, s);
+        if (ev) cudaEventRecord(ev[1], s);
+        pass_b(c, a, s);
+        if (ev) cudaEventRecord(ev[2], s);
+        pass_c(c, a, s);
+        if (ev) cudaEventRecord(ev[3], s);
+        return done(c);
+    }
+    static int run_batch_images(tm_ctx* c, tmk::BatchArgs& a, const int* ids, int n_ids) {
+        prep(c, a, c->stream);
+        for (int k = 0; k < n_ids; k++) {
+            const tm_ctx::Slot& sl = c->slots[ids[k]];
+            a.Ip = sl.Ip;
+            a.mip = sl.mip;
+            a.best = sl.best;
+            a.sum = sl.sum;
+            a.sumsq = sl.sumsq;
+            a.hist = sl.hist;
+            pass_b(c, a, c->stream);
+            pass_c(c, a, c->stream);
+        }
+        return done(c);
+    }
+};
+
 #define TM_VARIANT(T, X, Y)                                                                                 \
     {T, X, Y, tmk::Launch<T, X, Y>::pass_b_width, &Impl<T, X, Y>::run_batch, &Impl<T, X, Y>::configure,          \
      &Impl<T, X, Y>::run_stages, &whiten_on_device<X, Y>, &Impl<T, X, Y>::run_batch_images, nullptr}
@@ -341,6 +455,33 @@ const Variant kVariants[] = {
 const Variant* find_variant(int T, int X, int Y) {
     for (const Variant& v : kVariants)
         if (v.T == T && v.X == X && v.Y == Y) return &v;
+    return nullptr;
+}
+
+// the run-time-length variants, one per template box (X = Y = 0: any size with radix plans)
+#define TM_GENERIC(T)                                                                                  \
+    {T, 0, 0, 2, &GenImpl<T>::run_batch, &GenImpl<T>::configure, &GenImpl<T>::run_stages, &whiten_generic, \
+     &GenImpl<T>::run_batch_images, nullptr}
+const Variant kGenericVariants[] = {TM_GENERIC(32), TM_GENERIC(48), TM_GENERIC(64), TM_GENERIC(128), TM_GENERIC(256),
+                                    TM_GENERIC(384)};
+
+// a size the run-time-length kernels take: sides 64..8192 whose lengths (and the
+// half width, when the width is even) have radix plans (prime factors 2, 3, 5,
+// 7, 11, 13); ph receives the row pass's plan (X/2, or X when X is odd)
+bool generic_size(int X, int Y, tmk::GenPlan* px, tmk::GenPlan* py, tmk::GenPlan* ph) {
+    tmk::GenPlan a, b, h;
+    if (X < 64 || Y < 64) return false;
+    if (!tmk::gen_plan(X, a) || !tmk::gen_plan(Y, b) || !tmk::gen_plan(X % 2 ? X : X / 2, h)) return false;
+    if (px) *px = a;
+    if (py) *py = b;
+    if (ph) *ph = h;
+    return true;
+}
+
+const Variant* find_generic_variant(int T, int X, int Y) {
+    if (!generic_size(X, Y, nullptr, nullptr, nullptr)) return nullptr;
+    for (const Variant& v : kGenericVariants)
+        if (v.T == T) return &v;
     return nullptr;
 }
 
@@ -690,6 +831,8 @@ int tm_create(const tm_dims* dims, tm_ctx** out) {
         return set_err(c, TM_ERR_INVALID, "histogram_bins must be 1..1024 and the step positive");
     }
     c->var = find_variant(c->T, c->X, c->Y);
+    if (!c->var && (c->var = find_generic_variant(c->T, c->X, c->Y)) != nullptr)
+        generic_size(c->X, c->Y, &c->gen_px, &c->gen_py, &c->gen_ph);
     if (!c->var) {
         *out = c;
         return set_err(c, TM_ERR_UNSUPPORTED, "no kernel variant for template %d and image %d x %d", c->T, c->X, c->Y);
@@ -825,7 +968,7 @@ int tm_set_micrograph(tm_ctx* c, const float* image, int image_x, int image_y, d
     }
     if (rc == TM_OK) {
         // the whitened spectrum is staged in the correlation buffer C, as tm_set_image stages its input
-        WhitenBuffers wb{d_img, c->C, d_scratch, d_xs, make_args(c).tw, make_args(c).twy};
+        WhitenBuffers wb{d_img, c->C, d_scratch, d_xs, make_args(c).tw, make_args(c).twy, c->X, c->Y};
         std::string err;
         rc = c->var->whiten(c->stream, c->nsm, wb, h_curve, err);
         if (rc != TM_OK) set_err(c, rc, "whitening: %s", err.c_str());
@@ -852,6 +995,7 @@ int tm_whiten_micrograph(int device, const float* image, int image_x, int image_
     const Variant* var = nullptr;
     for (const Variant& v : kVariants)
         if (v.X == image_x && v.Y == image_y) var = &v;
+    if (!var) var = find_generic_variant(64, image_x, image_y);   // the whitening does not depend on T
     if (!var) return TM_ERR_UNSUPPORTED;
     const int X = image_x, Y = image_y, hc = X / 2 + 1;
     const int npts = curve_points(X);
@@ -889,7 +1033,7 @@ int tm_whiten_micrograph(int device, const float* image, int image_x, int image_
     std::vector<double> h_curve;
     if (rc == TM_OK) {
         tmfft::Twiddles twx{d_twx, X}, twy{d_twy, Y};
-        WhitenBuffers wb{d_img, d_spec, d_scratch, d_xs, twx, twy};
+        WhitenBuffers wb{d_img, d_spec, d_scratch, d_xs, twx, twy, X, Y};
         std::string err;
         rc = var->whiten(s, dev_sms > 0 ? dev_sms : 148, wb, h_curve, err);
     }

@@ -29,9 +29,12 @@ def test_library_loads_and_exports_all_symbols():
 
 
 def test_unsupported_geometry_rejected_without_gpu():
-    with pytest.raises(core.TmError) as e:
-        core.SearchCore(300, 300, 48, histogram_min_scaled=-0.1, histogram_step_scaled=0.001)
-    assert e.value.code == core.TM_ERR_UNSUPPORTED
+    # 302 = 2 x 151: no compiled kernels and no radix plan (a prime factor above 13);
+    # a box of 50 has no slice kernels
+    for x, y, t in ((302, 302, 48), (512, 512, 50), (16384, 512, 64)):
+        with pytest.raises(core.TmError) as e:
+            core.SearchCore(x, y, t, histogram_min_scaled=-0.1, histogram_step_scaled=0.001)
+        assert e.value.code == core.TM_ERR_UNSUPPORTED
 
 
 def test_bad_histogram_rejected_without_gpu():

@@ -145,3 +145,32 @@ def test_epilogue_pixel_ownership_covers_each_pixel_once():
                 seen[r, x] += 1
                 seen[r, x + 1] += 1
         assert np.all(seen == 1)
+
+
+def _factorized(n, template):
+    """The padded size the reference chooses (functions.cpp:529-577 through match_template.cpp:527-575)."""
+    from cistem_downstream_bah_b200 import hostprep as H
+    return H.factorize_dimension(n, template)
+
+
+def _radix_plannable(L):
+    m = L
+    for r in (2, 3, 5, 7, 11, 13):
+        while m % r == 0:
+            m //= r
+    return m == 1
+
+
+def test_every_padded_size_has_a_transform():
+    """Every side length the reference's factorisation produces for sides
+    256..8000 has radix plans for the run-time-length kernels (the side, and
+    its half when even, with prime factors up to 13); the factorisation's
+    "multiple of four" step does not always reach one (e.g. 6556 -> 6561 = 3^8),
+    so odd and 2 (mod 4) sides occur and are covered."""
+    odd = 0
+    for n in range(256, 8001):
+        p = _factorized(n, 64)
+        assert 64 <= p <= 8192 and _radix_plannable(p), (n, p)
+        assert p % 2 or _radix_plannable(p // 2), (n, p)
+        odd += p % 2
+    assert odd > 0
