@@ -122,7 +122,7 @@ k_pass_c_tc(BatchArgs a, int Y, const uint4* __restrict__ dft) {
     constexpr uint32_t kWaitLimit = 1u << 24;
     const int XP = a.XP;
     extern __shared__ __align__(128) unsigned char smem_t[];
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_t);   // [0], [1]: row blocks; [2]: MMA completion
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_t);   // [0], [1]: row blocks; [2], [3]: stage-1 / stage-2 MMAs
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem_t + 64);
     unsigned char* sB1 = smem_t + PC::OFF_B1;
     unsigned char* sB2 = smem_t + PC::OFF_B2;
@@ -143,6 +143,7 @@ k_pass_c_tc(BatchArgs a, int Y, const uint4* __restrict__ dft) {
         tmptx::mbar_init(&mbar[0], 1);
         tmptx::mbar_init(&mbar[1], 1);
         tmptx::mbar_init(&mbar[2], 1);
+        tmptx::mbar_init(&mbar[3], 1);
     }
     if (warp == 0) {
         tmptx::tmem_alloc(tmem_slot, PC::TMEM_COLS);
@@ -164,7 +165,7 @@ k_pass_c_tc(BatchArgs a, int Y, const uint4* __restrict__ dft) {
     if (t == 0 && a.nb > 0) {
         tmptx::mbar_arrive_expect_tx(&mbar[0], blk_bytes);
         tmptx::bulk_g2s(rows, C16 + (size_t)blockIdx.x * XP * R, blk_bytes, &mbar[0]);
-    }
+    }   // copy 0 (counted in the pipeline below)
 
     // ---- this thread's 16 pixels: items u = 8 * (2 sub + p) + i of the lane pair
     // (n2 = m / 2), item = (row r, n1); pixel x = 2 (n2 + 64 n1) + h
@@ -196,43 +197,50 @@ k_pass_c_tc(BatchArgs a, int Y, const uint4* __restrict__ dft) {
     const uint32_t id2 = tmptx::idesc_f16_f32(128, PC::B2_N, true, false);
     const uint32_t a1_addr = tmptx::smem_u32(sA1), a2_addr = tmptx::smem_u32(sA2);
     const uint32_t b1_addr = tmptx::smem_u32(sB1), b2_addr = tmptx::smem_u32(sB2);
+    // mbar[2]: stage-1 MMAs (one commit per orientation), mbar[3]: stage-2 MMAs.
+    // The orientations are software-pipelined: the stage-1 MMAs of orientation
+    // o + 1 run while the threads finish orientation o (epilogue 2), and the
+    // stage-2 MMAs of o while they prepare o + 1, so the tensor core works
+    // behind the CUDA-core stages.
     bool timed_out = false;
-    bool mma_pending = false;   // a commit whose wait ran out
-    uint32_t mma_phase = 0;     // commits completed and waited for
-    int o = 0;
-    for (; o < a.nb; o++) {
-        const int buf = o & 1;
-        // iteration o-1 is done with row buffer buf ^ 1, A1 and the accumulators
-        if (__syncthreads_or(timed_out)) break;
-        if (t == 0 && o + 1 < a.nb) {
-            tmptx::mbar_arrive_expect_tx(&mbar[buf ^ 1], blk_bytes);
-            tmptx::bulk_g2s(rows + (buf ^ 1) * blk, C16 + ((size_t)(o + 1) * (Y / R) + blockIdx.x) * XP * R, blk_bytes,
-                            &mbar[buf ^ 1]);
+    int issued1 = 0, issued2 = 0, waited1 = 0, waited2 = 0;   // commits (uniform across the block)
+    int copies = a.nb > 0 ? 1 : 0, copies_waited = 0;         // row-block copies issued / waited for
+    auto fail = [&]() {
+        timed_out = true;
+        atomicExch(a.err, 1);
+    };
+    auto issue_copy = [&](int oo) {   // row block of orientation oo into buffer oo & 1
+        if (t == 0) {
+            tmptx::mbar_arrive_expect_tx(&mbar[oo & 1], blk_bytes);
+            tmptx::bulk_g2s(rows + (oo & 1) * blk, C16 + ((size_t)oo * (Y / R) + blockIdx.x) * XP * R, blk_bytes,
+                            &mbar[oo & 1]);
         }
-        if (!tmptx::mbar_wait_bounded(&mbar[buf], (o >> 1) & 1, kWaitLimit)) {
-            timed_out = true;
-            atomicExch(a.err, 1);
-        }
-        // ---- pre-processing: v[r][k] -> A1[(r, k1, re/im)][k2], k = k1 + N1 k2
-        {
-            const __half2* zb = reinterpret_cast<const __half2*>(rows + buf * blk);
+        copies++;
+    };
+    // a wait that runs out leaves its counter behind, so the drain below waits for it again
+    auto wait_copy = [&](int oo) {
+        if (tmptx::mbar_wait_bounded(&mbar[oo & 1], (oo >> 1) & 1, kWaitLimit)) copies_waited++;
+        else fail();
+    };
+    // pre-processing of orientation oo: v[r][k] -> A1[(r, k1, re/im)][k2], k = k1 + N1 k2
+    auto pre = [&](int oo) {
+        const __half2* zb = reinterpret_cast<const __half2*>(rows + (oo & 1) * blk);
 #pragma unroll
-            for (int i = 0; i < (R * H) / PC::NT; i++) {
-                const int idx = t + PC::NT * i;
-                const int r = idx / H, k = idx % H;
-                float2 hk = __half22float2(zb[k * R + r]);
-                float2 hm = __half22float2(zb[(H - k) * R + r]);
-                if (k == 0) { hk.y = 0.f; hm.y = 0.f; }
-                const float2 e = make_float2(hk.x + hm.x, hk.y - hm.y);
-                const float2 d = make_float2(hk.x - hm.x, hk.y + hm.y);
-                const float2 od = cmul(d, a.tw.template w<+1>(k, X));
-                const int k1 = k % N1, k2 = k / N1;
-                *reinterpret_cast<uint32_t*>(sA1 + a_off<X>(2 * (k1 + N1 * r), k2)) = h2_bits(e.x - od.y, e.y + od.x);
-            }
+        for (int i = 0; i < (R * H) / PC::NT; i++) {
+            const int idx = t + PC::NT * i;
+            const int r = idx / H, k = idx % H;
+            float2 hk = __half22float2(zb[k * R + r]);
+            float2 hm = __half22float2(zb[(H - k) * R + r]);
+            if (k == 0) { hk.y = 0.f; hm.y = 0.f; }
+            const float2 e = make_float2(hk.x + hm.x, hk.y - hm.y);
+            const float2 d = make_float2(hk.x - hm.x, hk.y + hm.y);
+            const float2 od = cmul(d, a.tw.template w<+1>(k, X));
+            const int k1 = k % N1, k2 = k / N1;
+            *reinterpret_cast<uint32_t*>(sA1 + a_off<X>(2 * (k1 + N1 * r), k2)) = h2_bits(e.x - od.y, e.y + od.x);
         }
         tmptx::fence_proxy_async_smem();
-        if (__syncthreads_or(timed_out)) break;
-        // ---- stage 1: D1 = A1 (128 x 64) x B1 (64 x 128)
+    };
+    auto issue1 = [&]() {   // D1 = A1 (128 x 64) x B1 (64 x 128)
         if (t == 0) {
             tmptx::tmem_fence_after_sync();
 #pragma unroll
@@ -243,50 +251,9 @@ k_pass_c_tc(BatchArgs a, int Y, const uint4* __restrict__ dft) {
                                   kk > 0);
             tmptx::mma_commit(&mbar[2]);
         }
-        mma_pending = true;
-        if (tmptx::mbar_wait_bounded(&mbar[2], mma_phase & 1, kWaitLimit)) {
-            mma_pending = false;
-        } else {
-            timed_out = true;
-            atomicExch(a.err, 1);
-        }
-        mma_phase++;
-        tmptx::tmem_fence_after_sync();
-        // ---- epilogue 1: lane m = (r, k1, p); columns n2 in [16 sub, 16 sub + 16) of the cos and sin halves
-        {
-            const int p = m & 1, k1 = (m >> 1) % N1, r = (m >> 1) / N1;
-            float c[16], sn[16];
-            tmptx::tmem_ld16(tbase + tlane + PC::TM_D1 + 16 * sub, c);
-            tmptx::tmem_ld16(tbase + tlane + PC::TM_D1 + 64 + 16 * sub, sn);
-            tmptx::tmem_wait_ld16(c);
-            tmptx::tmem_wait_ld16(sn);
-            // the pair (p = 0, 1) splits the 16 n2: p = 0 takes the first 8, p = 1 the last 8;
-            // each sends the partner the products it needs
-            float rc[8], rs[8];
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                rc[i] = __shfl_xor_sync(0xffffffffu, p ? c[i] : c[8 + i], 1);
-                rs[i] = __shfl_xor_sync(0xffffffffu, p ? sn[i] : sn[8 + i], 1);
-            }
-            const int n2_0 = 16 * sub + 8 * p;
-            uint32_t packed[8];
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                // Y = (P_re,c - P_im,s) + i (P_re,s + P_im,c)
-                const float yr = p ? rc[i] - sn[8 + i] : c[i] - rs[i];
-                const float yi = p ? rs[i] + c[8 + i] : sn[i] + rc[i];
-                const float2 yv = cmul(make_float2(yr, yi), a.tw.template w<+1>(k1 * (n2_0 + i), H));
-                packed[i] = h2_bits(yv.x, yv.y);
-            }
-            // A2_r[(n2, re/im)][k1]: two 16-byte rows (4 n2 each) of two M groups
-            unsigned char* dst = sA2 + r * PC::A2_BYTES;
-            *reinterpret_cast<uint4*>(dst + a_off<X>(2 * n2_0, k1)) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
-            *reinterpret_cast<uint4*>(dst + a_off<X>(2 * n2_0 + 8, k1)) = make_uint4(packed[4], packed[5], packed[6], packed[7]);
-        }
-        tmptx::fence_proxy_async_smem();
-        tmptx::tmem_fence_before_sync();
-        if (__syncthreads_or(timed_out)) break;
-        // ---- stage 2: per row, D2_r = A2_r (128 x K2) x B2 (K2 x 2 N1)
+        issued1++;
+    };
+    auto issue2 = [&]() {   // per row, D2_r = A2_r (128 x K2) x B2 (K2 x 2 N1)
         if (t == 0) {
             tmptx::tmem_fence_after_sync();
 #pragma unroll
@@ -298,89 +265,153 @@ k_pass_c_tc(BatchArgs a, int Y, const uint4* __restrict__ dft) {
                                                                  PC::SBO_A),
                                       tmptx::smem_desc_noswizzle(b2_addr + kk * 2 * PC::LBO_B2, PC::LBO_B2, PC::SBO_B), id2,
                                       kk > 0);
-            tmptx::mma_commit(&mbar[2]);
+            tmptx::mma_commit(&mbar[3]);
         }
-        mma_pending = true;
-        if (tmptx::mbar_wait_bounded(&mbar[2], mma_phase & 1, kWaitLimit)) {
-            mma_pending = false;
-        } else {
-            timed_out = true;
-            atomicExch(a.err, 1);
-        }
-        mma_phase++;
+        issued2++;
+    };
+    auto wait1 = [&]() {
+        if (tmptx::mbar_wait_bounded(&mbar[2], waited1 & 1, kWaitLimit)) waited1++;
+        else fail();
         tmptx::tmem_fence_after_sync();
-        // ---- epilogue 2: lane m = (n2, p); the 16 items [16 sub, 16 sub + 16) of the lane pair
-        {
-            const int p = p_own;
-            float c[16], sn[16];
-            const int it0 = 16 * sub;
-            if constexpr (N1 >= 16) {
-                const int r = it0 / N1, n1_0 = it0 % N1;
-                const uint32_t col = tbase + tlane + PC::TM_D2 + r * PC::B2_N + n1_0;
-                tmptx::tmem_ld16(col, c);
-                tmptx::tmem_ld16(col + N1, sn);
-            } else {
-                // N1 = 8: the 16 items are two whole rows, [cos 8 | sin 8] each
-                const uint32_t col = tbase + tlane + PC::TM_D2 + (it0 / N1) * PC::B2_N;
-                float w[32];
-                tmptx::tmem_ld16(col, w);
-                tmptx::tmem_ld16(col + 16, w + 16);
-                tmptx::tmem_wait_ld32(w);
+    };
+    auto wait2 = [&]() {
+        if (tmptx::mbar_wait_bounded(&mbar[3], waited2 & 1, kWaitLimit)) waited2++;
+        else fail();
+        tmptx::tmem_fence_after_sync();
+    };
+    // epilogue 1: lane m = (r, k1, p); columns n2 in [16 sub, 16 sub + 16) of the cos and sin halves
+    auto epi1 = [&]() {
+        const int p = m & 1, k1 = (m >> 1) % N1, r = (m >> 1) / N1;
+        float c[16], sn[16];
+        tmptx::tmem_ld16(tbase + tlane + PC::TM_D1 + 16 * sub, c);
+        tmptx::tmem_ld16(tbase + tlane + PC::TM_D1 + 64 + 16 * sub, sn);
+        tmptx::tmem_wait_ld16(c);
+        tmptx::tmem_wait_ld16(sn);
+        // the pair (p = 0, 1) splits the 16 n2: p = 0 takes the first 8, p = 1 the last 8;
+        // each sends the partner the products it needs
+        float rc[8], rs[8];
 #pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    c[i] = w[i]; sn[i] = w[8 + i];
-                    c[8 + i] = w[16 + i]; sn[8 + i] = w[24 + i];
-                }
-            }
-            tmptx::tmem_wait_ld16(c);
-            tmptx::tmem_wait_ld16(sn);
-            float rc[8], rs[8];
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                rc[i] = __shfl_xor_sync(0xffffffffu, p ? c[i] : c[8 + i], 1);
-                rs[i] = __shfl_xor_sync(0xffffffffu, p ? sn[i] : sn[8 + i], 1);
-            }
-            // every read of D2 is done before the next stage-2 MMA (the next iteration's barriers)
-            tmptx::tmem_fence_before_sync();
-            const int g = (int)(a.gidx0 + o);
-            float val[16];
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                val[2 * i] = (p ? rc[i] - sn[8 + i] : c[i] - rs[i]) * out_scale;
-                val[2 * i + 1] = (p ? rs[i] + c[8 + i] : sn[i] + rc[i]) * out_scale;
-            }
-            float st[32];
-            // sweep 0: MIP / argmax, histogram and the sum (compensation in TMEM columns 0-15)
-            tmptx::tmem_ld16(tstate, st);
-            tmptx::tmem_wait_ld16(st);
-#pragma unroll
-            for (int pi = 0; pi < 16; pi++) {
-                const float v = val[pi];
-                if (v > mip[pi]) { mip[pi] = v; best[pi] = g; }
-                const float ys = v - st[pi];
-                const float ts = fs[pi] + ys;
-                st[pi] = (ts - fs[pi]) - ys;
-                fs[pi] = ts;
-                const int bin = __float2int_rz((v - a.hist_min) * a.hist_inv_step);
-                if (bin >= 0 && bin < a.hist_bins) atomicAdd(&shist[bin], 1u);
-            }
-            tmptx::tmem_st16(tstate, st);
-            // sweep 1: the sum of squares (columns 32-47) and its compensation (16-31)
-            tmptx::tmem_ld16(tstate + 16, st);
-            tmptx::tmem_ld16(tstate + 32, st + 16);
-            tmptx::tmem_wait_ld32(st);
-#pragma unroll
-            for (int pi = 0; pi < 16; pi++) {
-                const float v = val[pi];
-                const float yq = fmaf(v, v, -st[pi]);
-                const float tq = st[16 + pi] + yq;
-                st[pi] = (tq - st[16 + pi]) - yq;
-                st[16 + pi] = tq;
-            }
-            tmptx::tmem_st16(tstate + 16, st);
-            tmptx::tmem_st16(tstate + 32, st + 16);
-            tmptx::tmem_wait_st();
+        for (int i = 0; i < 8; i++) {
+            rc[i] = __shfl_xor_sync(0xffffffffu, p ? c[i] : c[8 + i], 1);
+            rs[i] = __shfl_xor_sync(0xffffffffu, p ? sn[i] : sn[8 + i], 1);
         }
+        const int n2_0 = 16 * sub + 8 * p;
+        // twiddles exp(+2 pi i k1 n2 / H) for n2 = n2_0 .. n2_0 + 7 by recurrence
+        const float2 wstep = a.tw.template w<+1>(k1, H);
+        float2 w = a.tw.template w<+1>(k1 * n2_0, H);
+        uint32_t packed[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            // Y = (P_re,c - P_im,s) + i (P_re,s + P_im,c)
+            const float yr = p ? rc[i] - sn[8 + i] : c[i] - rs[i];
+            const float yi = p ? rs[i] + c[8 + i] : sn[i] + rc[i];
+            const float2 yv = cmul(make_float2(yr, yi), w);
+            w = cmul(w, wstep);
+            packed[i] = h2_bits(yv.x, yv.y);
+        }
+        // A2_r[(n2, re/im)][k1]: two 16-byte rows (4 n2 each) of two M groups
+        unsigned char* dst = sA2 + r * PC::A2_BYTES;
+        *reinterpret_cast<uint4*>(dst + a_off<X>(2 * n2_0, k1)) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+        *reinterpret_cast<uint4*>(dst + a_off<X>(2 * n2_0 + 8, k1)) = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+        tmptx::fence_proxy_async_smem();
+        tmptx::tmem_fence_before_sync();
+    };
+    // epilogue 2: lane m = (n2, p); the 16 items [16 sub, 16 sub + 16) of the lane pair
+    auto epi2 = [&](int oo) {
+        const int p = p_own;
+        float c[16], sn[16];
+        const int it0 = 16 * sub;
+        if constexpr (N1 >= 16) {
+            const int r = it0 / N1, n1_0 = it0 % N1;
+            const uint32_t col = tbase + tlane + PC::TM_D2 + r * PC::B2_N + n1_0;
+            tmptx::tmem_ld16(col, c);
+            tmptx::tmem_ld16(col + N1, sn);
+        } else {
+            // N1 = 8: the 16 items are two whole rows, [cos 8 | sin 8] each
+            const uint32_t col = tbase + tlane + PC::TM_D2 + (it0 / N1) * PC::B2_N;
+            float w[32];
+            tmptx::tmem_ld16(col, w);
+            tmptx::tmem_ld16(col + 16, w + 16);
+            tmptx::tmem_wait_ld32(w);
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                c[i] = w[i]; sn[i] = w[8 + i];
+                c[8 + i] = w[16 + i]; sn[8 + i] = w[24 + i];
+            }
+        }
+        tmptx::tmem_wait_ld16(c);
+        tmptx::tmem_wait_ld16(sn);
+        float rc[8], rs[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            rc[i] = __shfl_xor_sync(0xffffffffu, p ? c[i] : c[8 + i], 1);
+            rs[i] = __shfl_xor_sync(0xffffffffu, p ? sn[i] : sn[8 + i], 1);
+        }
+        const int g = (int)(a.gidx0 + oo);
+        float val[16];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            val[2 * i] = (p ? rc[i] - sn[8 + i] : c[i] - rs[i]) * out_scale;
+            val[2 * i + 1] = (p ? rs[i] + c[8 + i] : sn[i] + rc[i]) * out_scale;
+        }
+        // every read of D2 is done before the next stage-2 MMA (after the next barrier)
+        tmptx::tmem_fence_before_sync();
+        float st[32];
+        // sweep 0: MIP / argmax, histogram and the sum (compensation in TMEM columns 0-15)
+        tmptx::tmem_ld16(tstate, st);
+        tmptx::tmem_wait_ld16(st);
+#pragma unroll
+        for (int pi = 0; pi < 16; pi++) {
+            const float v = val[pi];
+            if (v > mip[pi]) { mip[pi] = v; best[pi] = g; }
+            const float ys = v - st[pi];
+            const float ts = fs[pi] + ys;
+            st[pi] = (ts - fs[pi]) - ys;
+            fs[pi] = ts;
+            const int bin = __float2int_rz((v - a.hist_min) * a.hist_inv_step);
+            if (bin >= 0 && bin < a.hist_bins) atomicAdd(&shist[bin], 1u);
+        }
+        tmptx::tmem_st16(tstate, st);
+        // sweep 1: the sum of squares (columns 32-47) and its compensation (16-31)
+        tmptx::tmem_ld16(tstate + 16, st);
+        tmptx::tmem_ld16(tstate + 32, st + 16);
+        tmptx::tmem_wait_ld32(st);
+#pragma unroll
+        for (int pi = 0; pi < 16; pi++) {
+            const float v = val[pi];
+            const float yq = fmaf(v, v, -st[pi]);
+            const float tq = st[16 + pi] + yq;
+            st[pi] = (tq - st[16 + pi]) - yq;
+            st[16 + pi] = tq;
+        }
+        tmptx::tmem_st16(tstate + 16, st);
+        tmptx::tmem_st16(tstate + 32, st + 16);
+        tmptx::tmem_wait_st();
+    };
+
+    // ---- prologue: orientation 0 prepared and its stage 1 issued; the row block of 1 in flight
+    int o = 0;
+    bool stop = __syncthreads_or(timed_out);
+    if (!stop && a.nb > 1) issue_copy(1);
+    if (!stop) {
+        wait_copy(0);
+        pre(0);
+    }
+    if (!(stop = __syncthreads_or(timed_out))) issue1();
+    for (; !stop && o < a.nb; o++) {
+        wait1();
+        epi1();                                       // D1(o) -> A2 (stage 2 of o - 1 is complete)
+        if ((stop = __syncthreads_or(timed_out))) break;
+        issue2();                                     // stage 2 of o
+        if (o + 1 < a.nb) {
+            wait_copy(o + 1);
+            if (o + 2 < a.nb) issue_copy(o + 2);      // into the buffer pre(o) has finished with
+            pre(o + 1);                               // A1 is free: stage 1 of o is complete
+        }
+        if ((stop = __syncthreads_or(timed_out))) break;
+        if (o + 1 < a.nb) issue1();                   // stage 1 of o + 1 runs during epilogue 2 of o
+        wait2();
+        epi2(o);
     }
     // ---- end of the batch: the FP64 flush, or the drain after a wait ran out
     float st[48];
@@ -392,10 +423,11 @@ k_pass_c_tc(BatchArgs a, int Y, const uint4* __restrict__ dft) {
     tmptx::tmem_fence_before_sync();
     const bool failed = __syncthreads_or(timed_out);
     if (failed) {
-        // no MMA or bulk copy may still be writing TMEM or shared memory when the block exits
-        if (mma_pending) tmptx::mbar_wait_bounded(&mbar[2], (mma_phase - 1) & 1, kWaitLimit);
-        if (o > 0) tmptx::mbar_wait_bounded(&mbar[(o - 1) & 1], ((o - 1) >> 1) & 1, kWaitLimit);
-        if (o < a.nb) tmptx::mbar_wait_bounded(&mbar[o & 1], (o >> 1) & 1, kWaitLimit);
+        // no MMA or bulk copy may still be writing TMEM or shared memory when the block exits:
+        // wait (bounded) for every commit and copy issued and not yet waited for
+        for (int k = waited1; k < issued1; k++) tmptx::mbar_wait_bounded(&mbar[2], k & 1, kWaitLimit);
+        for (int k = waited2; k < issued2; k++) tmptx::mbar_wait_bounded(&mbar[3], k & 1, kWaitLimit);
+        for (int k = copies_waited; k < copies; k++) tmptx::mbar_wait_bounded(&mbar[k & 1], (k >> 1) & 1, kWaitLimit);
     }
     tmptx::tmem_fence_before_sync();
     __syncthreads();
@@ -546,7 +578,11 @@ k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
     const int it0 = blockIdx.x * per;
     const int it1 = min(n_items, it0 + per);
     if (it0 >= it1) return;
-    if (t == 0) tmptx::mbar_init(&mbar[0], 1);
+    if (t == 0) {
+        tmptx::mbar_init(&mbar[0], 1);
+        tmptx::mbar_init(&mbar[1], 1);
+        tmptx::mbar_init(&mbar[2], 1);
+    }
     if (warp == 0) {
         tmptx::tmem_alloc(tmem_slot, PB::TMEM_COLS);
         tmptx::tmem_relinquish();
@@ -569,34 +605,40 @@ k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
     const uint32_t idM = tmptx::idesc_f16_f32(128, 128, true, false);
     const uint32_t e_addr = tmptx::smem_u32(sE), bf_addr = tmptx::smem_u32(sBF), bh_addr = tmptx::smem_u32(sBH);
     const uint32_t op_addr = tmptx::smem_u32(sOP);
-    bool timed_out = false, mma_pending = false;
-    uint32_t phase = 0;
+    // mbar[0]: stage H (one commit per item, the whole block waits); mbar[1 + h]:
+    // stages F, 1 and 2 of tile h.  After stage H the two tiles (columns 2h, 2h + 1)
+    // are independent chains run by the two halves of the block (warps 8h .. 8h + 7,
+    // named barrier 1 + h), so one half's MMAs run during the other half's epilogues.
+    const int h = sub >> 1;                      // this thread's tile
+    const int lead = 256 * h;                    // the thread that issues the tile's MMAs
+    bool timed_out = false;
+    int issuedH = 0, waitedH = 0, issuedT = 0, waitedT = 0;   // commits of stage H and of this thread's tile
     int cur_group = -1;
-    // one MMA group: thread 0 issues, every thread waits for its completion
-    auto wait_mma = [&]() {
-        mma_pending = true;
-        if (tmptx::mbar_wait_bounded(&mbar[0], phase & 1, kWaitLimit)) {
-            mma_pending = false;
-        } else {
-            timed_out = true;
-            atomicExch(a.err, 1);
-        }
-        phase++;
-        tmptx::tmem_fence_after_sync();
+    auto fail = [&]() {
+        timed_out = true;
+        atomicExch(a.err, 1);
     };
-    auto issue_pair = [&](int a_off_bytes, int a_lbo, int a_sbo, uint32_t idesc) {
-        // D_tile = A_tile (128 x 128) x DFT (128 x 128) for the two tiles
-        tmptx::tmem_fence_after_sync();
-#pragma unroll 1
-        for (int tt = 0; tt < 2; tt++)
+    auto half_sync = [h]() { asm volatile("bar.sync %0, 256;" ::"r"(1 + h) : "memory"); };
+    unsigned char* tile = sOP + h * PB::OP_TILE;
+    const uint32_t tile_addr = op_addr + h * PB::OP_TILE;
+    const uint32_t tcol = tbase + tlane + 128 * h;
+    // D_tile = A_tile (128 x 128) x DFT (128 x 128), issued by the half's lead thread
+    auto issue_tile = [&](int a_lbo, int a_sbo, uint32_t idesc) {
+        if (t == lead) {
+            tmptx::tmem_fence_after_sync();
 #pragma unroll
             for (int kk = 0; kk < 8; kk++)
-                tmptx::mma_f16_ss(tbase + 128 * tt,
-                                  tmptx::smem_desc_noswizzle(op_addr + tt * PB::OP_TILE + a_off_bytes + kk * 2 * a_lbo,
-                                                             a_lbo, a_sbo),
+                tmptx::mma_f16_ss(tbase + 128 * h, tmptx::smem_desc_noswizzle(tile_addr + kk * 2 * a_lbo, a_lbo, a_sbo),
                                   tmptx::smem_desc_noswizzle(bf_addr + kk * 2 * PB::BF_LBO, PB::BF_LBO, PB::BF_SBO), idesc,
                                   kk > 0);
-        tmptx::mma_commit(&mbar[0]);
+            tmptx::mma_commit(&mbar[1 + h]);
+        }
+        issuedT++;
+    };
+    auto wait_tile = [&]() {
+        if (tmptx::mbar_wait_bounded(&mbar[1 + h], waitedT & 1, kWaitLimit)) waitedT++;
+        else fail();
+        tmptx::tmem_fence_after_sync();
     };
     for (int it = it0; it < it1; it++) {
         const int group = it / a.nb, o = it % a.nb;
@@ -633,11 +675,13 @@ k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
                               tmptx::smem_desc_noswizzle(bh_addr, PB::BH_LBO, PB::BH_SBO), idH, false);
             tmptx::mma_commit(&mbar[0]);
         }
-        wait_mma();
+        issuedH++;
+        if (tmptx::mbar_wait_bounded(&mbar[0], waitedH & 1, kWaitLimit)) waitedH++;
+        else fail();
+        tmptx::tmem_fence_after_sync();
         // ---- epilogue H: lane m = (a, p); columns (v = sub, n1); p = 0 keeps n1 < 32, p = 1 the rest
         {
-            const int p = m & 1, av = m >> 1, v = sub;
-            const int tt = v >> 1, vl = v & 1;
+            const int p = m & 1, av = m >> 1, v = sub, vl = v & 1;
 #pragma unroll 1
             for (int j = 0; j < 2; j++) {
                 float lo[16], hi[16];
@@ -646,32 +690,33 @@ k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
                 tmptx::tmem_wait_ld16(lo);
                 tmptx::tmem_wait_ld16(hi);
                 const int n1_0 = 32 * p + 16 * j;
+                // exp(-2 pi i n1 a / Y) for n1 = n1_0 .. n1_0 + 15 by recurrence
+                const float2 wstep = a.twy.template w<-1>(av, Y);
+                float2 w = a.twy.template w<-1>(n1_0 * av, Y);
                 uint32_t packed[16];
 #pragma unroll
                 for (int i = 0; i < 16; i++) {
                     const float r = __shfl_xor_sync(0xffffffffu, p ? lo[i] : hi[i], 1);
-                    const float2 h = p ? make_float2(r, hi[i]) : make_float2(lo[i], r);
-                    const float2 g = cmul(h, a.twy.template w<-1>((n1_0 + i) * av, Y));
+                    const float2 hv = p ? make_float2(r, hi[i]) : make_float2(lo[i], r);
+                    const float2 g = cmul(hv, w);
+                    w = cmul(w, wstep);
                     packed[i] = h2_bits(g.x, g.y);
                 }
-                unsigned char* dst = sOP + tt * PB::OP_TILE;
                 const int mF = 64 * vl + av;
 #pragma unroll
                 for (int r = 0; r < 4; r++)
-                    *reinterpret_cast<uint4*>(dst + kmaj_off(mF, 2 * n1_0 + 8 * r, PB::AK_SBO, PB::AK_LBO)) =
+                    *reinterpret_cast<uint4*>(tile + kmaj_off(mF, 2 * n1_0 + 8 * r, PB::AK_SBO, PB::AK_LBO)) =
                         make_uint4(packed[4 * r], packed[4 * r + 1], packed[4 * r + 2], packed[4 * r + 3]);
             }
         }
         tmptx::fence_proxy_async_smem();
         tmptx::tmem_fence_before_sync();
-        if (__syncthreads_or(timed_out)) break;
-        if (t == 0) issue_pair(0, PB::AK_LBO, PB::AK_SBO, idK);
-        wait_mma();
-        // ---- epilogue F: lane m = (vl, a); tile tt = sub / 2, b in [32 (sub & 1), +32)
-        const int tt = sub >> 1, vl = m >> 6, av = m & 63;
-        const int v = 2 * tt + vl;
-        unsigned char* tile = sOP + tt * PB::OP_TILE;
-        const uint32_t tcol = tbase + tlane + 128 * tt;
+        half_sync();
+        issue_tile(PB::AK_LBO, PB::AK_SBO, idK);
+        wait_tile();
+        // ---- epilogue F: lane m = (vl, a); b in [32 (sub & 1), +32)
+        const int vl = m >> 6, av = m & 63;
+        const int v = 2 * h + vl;
 #pragma unroll 1
         for (int j = 0; j < 2; j++) {
             const int b0 = 32 * (sub & 1) + 16 * j;
@@ -693,9 +738,9 @@ k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
         }
         tmptx::fence_proxy_async_smem();
         tmptx::tmem_fence_before_sync();
-        if (__syncthreads_or(timed_out)) break;
-        if (t == 0) issue_pair(0, PB::AK_LBO, PB::AK_SBO, idK);
-        wait_mma();
+        half_sync();
+        issue_tile(PB::AK_LBO, PB::AK_SBO, idK);
+        wait_tile();
         // ---- epilogue 1: lane m = (vl, k1); Y = conj(D1), Y' = Y exp(+2 pi i k1 n2 / Y), A2 = conj(Y') MN-major
 #pragma unroll 1
         for (int j = 0; j < 2; j++) {
@@ -704,10 +749,13 @@ k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
             tmptx::tmem_ld16(tcol + 2 * n2_0, d);
             tmptx::tmem_ld16(tcol + 2 * n2_0 + 16, d + 16);
             tmptx::tmem_wait_ld32(d);
+            const float2 wstep = a.twy.template w<+1>(av, Y);
+            float2 w = a.twy.template w<+1>(av * n2_0, Y);
             float re[16], im[16];
 #pragma unroll
             for (int i = 0; i < 16; i++) {
-                const float2 yv = cmul(make_float2(d[2 * i], -d[2 * i + 1]), a.twy.template w<+1>(av * (n2_0 + i), Y));
+                const float2 yv = cmul(make_float2(d[2 * i], -d[2 * i + 1]), w);
+                w = cmul(w, wstep);
                 re[i] = yv.x;
                 im[i] = -yv.y;
             }
@@ -725,11 +773,12 @@ k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
         }
         tmptx::fence_proxy_async_smem();
         tmptx::tmem_fence_before_sync();
-        if (__syncthreads_or(timed_out)) break;
-        if (t == 0) issue_pair(0, PB::AM_LBO, PB::AM_SBO, idM);
-        wait_mma();
-        // ---- epilogue 2 (stage 2 has read A2: the tiles become the staging area): lane m = (vl, n2); z[n2 + 64 n1] = conj(D2) -> staging [column][y], FP16
-        uint32_t* stage = reinterpret_cast<uint32_t*>(sOP);
+        half_sync();
+        issue_tile(PB::AM_LBO, PB::AM_SBO, idM);
+        wait_tile();
+        // ---- epilogue 2 (stage 2 has read A2: the tile becomes its columns' staging area):
+        // lane m = (vl, n2); z[n2 + 64 n1] = conj(D2) -> staging [column vl][y], FP16
+        uint32_t* stage = reinterpret_cast<uint32_t*>(tile) + vl * Y;
 #pragma unroll 1
         for (int j = 0; j < 2; j++) {
             const int n1_0 = 32 * (sub & 1) + 16 * j;
@@ -738,14 +787,15 @@ k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
             tmptx::tmem_ld16(tcol + 2 * n1_0 + 16, d + 16);
             tmptx::tmem_wait_ld32(d);
 #pragma unroll
-            for (int i = 0; i < 16; i++)
-                stage[v * Y + av + 64 * (n1_0 + i)] = h2_bits(d[2 * i] * sOut, -d[2 * i + 1] * sOut);
+            for (int i = 0; i < 16; i++) stage[av + 64 * (n1_0 + i)] = h2_bits(d[2 * i] * sOut, -d[2 * i + 1] * sOut);
         }
         tmptx::tmem_fence_before_sync();
         if (__syncthreads_or(timed_out)) break;
         // ---- the item's columns to C16[o][y / RB][kx][y % RB]: 16-byte chunks of 4 (column, row) values
         {
             __half2* C16 = reinterpret_cast<__half2*>(a.C) + (size_t)o * Y * XP;
+            const uint32_t* st0 = reinterpret_cast<const uint32_t*>(sOP);
+            const uint32_t* st1 = reinterpret_cast<const uint32_t*>(sOP + PB::OP_TILE);
             for (int ch = t; ch < Y; ch += PB::NT) {
                 // chunk ch: row block rb, elements e = 4 (ch % RB) .. + 3 of its 4 RB (column, row) values
                 const int rb = ch / RB, e0 = 4 * (ch % RB);
@@ -753,14 +803,18 @@ k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
                     const int c = (e0 + e) / RB, r = (e0 + e) % RB;
-                    w4[e] = stage[c * Y + rb * RB + r];
+                    w4[e] = ((c >> 1) ? st1 : st0)[(c & 1) * Y + rb * RB + r];
                 }
                 *reinterpret_cast<uint4*>(C16 + ((size_t)rb * XP + kx0) * RB + e0) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
             }
         }
     }
     const bool failed = __syncthreads_or(timed_out);
-    if (failed && mma_pending) tmptx::mbar_wait_bounded(&mbar[0], (phase - 1) & 1, kWaitLimit);
+    if (failed) {
+        // no MMA may still be writing TMEM when the block exits
+        for (int k = waitedH; k < issuedH; k++) tmptx::mbar_wait_bounded(&mbar[0], k & 1, kWaitLimit);
+        for (int k = waitedT; k < issuedT; k++) tmptx::mbar_wait_bounded(&mbar[1 + h], k & 1, kWaitLimit);
+    }
     tmptx::tmem_fence_before_sync();
     __syncthreads();
     tmptx::tmem_fence_after_sync();

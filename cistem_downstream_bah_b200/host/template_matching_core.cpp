@@ -1,4 +1,6 @@
 // template_matching_core.cpp -- see template_matching_core.hpp.
+#include <cstdlib>
+#include <cstdio>
 #include "template_matching_core.hpp"
 
 #include <cfloat>
@@ -138,6 +140,20 @@ void TemplateMatchingCore::Init(void*, Image& template_reconstruction, Image& in
     dims_.orientation_batch = 0;
     dims_.device = device;
     check(tm_create(&dims_, &ctx_), "tm_create");
+    // Opt-in FP16 tensor-core form of the correlation transforms (the reference has
+    // no counterpart; its default, the FP32 path, is the one that matches the CPU
+    // program).  TM_B200_PRECISION=fp16 selects it where the geometry has the kernels.
+    if (const char* prec = std::getenv("TM_B200_PRECISION")) {
+        if (std::string(prec) == "fp16") {
+            const int rc = tm_set_precision(ctx_, TM_PRECISION_FP16_TENSOR);
+            if (rc == TM_ERR_UNSUPPORTED)
+                std::fprintf(stderr, "TM_B200_PRECISION=fp16: %s; the FP32 path is used\n", tm_last_error(ctx_));
+            else
+                check(rc, "tm_set_precision");
+        } else if (std::string(prec) != "fp32") {
+            throw CoreError(TM_ERR_INVALID, "TM_B200_PRECISION must be fp32 or fp16");
+        }
+    }
     psi_max_ = psi_max;
     psi_start_ = psi_start;
     psi_step_ = psi_step;
