@@ -786,6 +786,70 @@ def run_proposal(args):
         dist.destroy_process_group()
 
 
+def run_recall16(args):
+    """The FP16 tensor-core form as the fast exhaustive search: the metric's
+    configuration searched over the whole 2.5 / 1.5 deg grid (1,595,420
+    orientations) once in FP32 (the parity path, the judge) and once in FP16.
+    Reported: both rates, their ratio, the MIP error of the FP16 search against
+    the FP32 one, and the recall of the FP32 search's z >= 7 peaks (the
+    reference's result-aggregation loop): a peak is recovered when the FP16 z
+    map reaches 7 within 1 px, or (strict) when the FP16 peak list has a peak
+    within 2 px."""
+    from cistem_downstream_bah_b200 import core
+    from cistem_downstream_bah_b200 import proposal as PR
+    world, rank, local = dist_init(args)
+    inp = make_inputs()
+    X, Y, T = inp["X"], inp["Y"], inp["T"]
+    angles = inp["angles"] if args.recall_orientations <= 0 else inp["angles"][:args.recall_orientations]
+    out = {}
+    for name, prec in (("fp32", core.PRECISION_FP32), ("fp16", core.PRECISION_FP16_TENSOR)):
+        sc = core.SearchCore(X, Y, T, histogram_min_scaled=inp["hmin"], histogram_step_scaled=inp["hstep"], device=local)
+        sc.set_precision(prec)
+        sc.set_template(inp["tspec"])
+        sc.set_image(inp["ispec"])
+        sc.autotune(inp["filt"], inp["angles"][:256])
+        PR.search_maps(sc, inp["filt"], angles[:512], X, Y)    # warm-up
+        with ClockSampler(local) as clk:
+            out[name] = PR.search_maps(sc, inp["filt"], angles, X, Y)
+        out[name]["clocks"] = clk.summary()
+        out[name]["batch"] = sc.orientation_batch()
+        sc.close()
+    e, f = out["fp32"], out["fp16"]
+    pk32 = PR.find_peaks(e, 7.0, T, WORKLOAD["pixel_size"])
+    pk16 = PR.find_peaks(f, 7.0, T, WORKLOAD["pixel_size"])
+    hit_z = hit_list = 0
+    dz = []
+    for x, y, z, *_ in pk32:
+        x, y = int(x), int(y)
+        win = f["z"][max(0, y - 1):y + 2, max(0, x - 1):x + 2]
+        hit_z += float(win.max()) >= 7.0
+        dz.append(float(f["z"][y, x]) - float(z))
+        if len(pk16):
+            hit_list += float(np.min(np.hypot(pk16[:, 0] - x, pk16[:, 1] - y))) <= 2.0
+    n = max(len(pk32), 1)
+    npix_orig = WORKLOAD["nx"] * WORKLOAD["ny"]
+    v32 = npix_orig * len(angles) / e["seconds"]
+    v16 = npix_orig * len(angles) / f["seconds"]
+    scale = float(np.abs(e["mip"]).max())
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": v16, "unit": UNIT, "n_gpus": world, "steps": 1, "warmup": 1,
+            "ms_per_step": f["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f16 tensor-core transforms, f32 MIP, f64 sums", "data": "synthetic",
+            "config": {"workload": "exhaustive search, FP16 tensor-core form against the FP32 path: " + WORKLOAD["name"],
+                       "orientations": int(len(angles)), "orientation_batch": {"fp32": e["batch"], "fp16": f["batch"]}},
+            "e2e": {"value": v16, "unit": UNIT, "h2d_bytes_per_step": int(inp["ispec"].nbytes + inp["tspec"].nbytes),
+                    "d2h_bytes_per_step": int(24 * X * Y),
+                    "note": "each search: one tm_run_plane over the whole grid and the results to the host"},
+            "fp32_value": v32, "ratio_fp16_to_fp32": v16 / v32,
+            "fp32_seconds": e["seconds"], "fp16_seconds": f["seconds"],
+            "mip_max_rel_err_fp16_vs_fp32": float(np.abs(f["mip"] - e["mip"]).max() / scale),
+            "z_peaks_fp32": int(len(pk32)), "z_peaks_fp16": int(len(pk16)),
+            "recall_z7_within_1px": hit_z / n, "recall_z7_peak_list_within_2px": hit_list / n,
+            "z_diff_at_fp32_peaks": {"min": float(min(dz)) if dz else None, "max": float(max(dz)) if dz else None},
+            "gpu_launches": None, "clocks": {"fp32": e["clocks"], "fp16": f["clocks"]}}), flush=True)
+
+
 def _cpu_threads():
     """Host threads for the CPU legs (each thread holds ~0.6 GB of 4096^2 buffers)."""
     threads = min(os.cpu_count() or 1, 32)
@@ -844,7 +908,10 @@ def main():
                     help="skip the FP16 tensor-core form that the default run times beside the FP32 path")
     ap.add_argument("--accuracy", type=int, default=4,
                     help="orientations compared with the FP64 oracle after timing, in the CPU-baseline leg (0 = skip)")
-    ap.add_argument("--workload", default="full", choices=sorted(WORKLOADS) + ["batched", "refine", "proposal"],
+    ap.add_argument("--recall-orientations", type=int, default=0,
+                    help="--workload recall16: orientations searched (0 = the whole grid)")
+    ap.add_argument("--workload", default="full",
+                    choices=sorted(WORKLOADS) + ["batched", "refine", "proposal", "recall16"],
                     help="full = the metric's 4096^2 configuration; the others are the uneven and stress geometries")
     ap.add_argument("--e2e-contexts", type=int, default=2,
                     help="host threads (each with its own search context) sharing the GPU in the e2e leg")
@@ -869,6 +936,8 @@ def main():
         run_refine(args)
     elif args.workload == "proposal":
         run_proposal(args)
+    elif args.workload == "recall16":
+        run_recall16(args)
     else:
         run_ours(args)
 

@@ -451,19 +451,10 @@ k_pass_b(BatchArgs a, int n_items) {
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const bool tmem_warp = warp < PB::FULL_WARPS;   // uniform per warp
-    constexpr int G = PB::G, WG = PB::WG;
-    // Column-major threads (thread = j + P c) when a column is whole warps: each
-    // column's FFT stages then wait only on its own warps (named barrier 1 + c);
-    // the item's outputs go out through shared memory in whole row segments.
-    // Otherwise columns interleave in each warp (thread = c + W j) and the
-    // stages take the block-wide barrier.
-    constexpr bool CM = (P % 32 == 0) && (G == 1) && (RB == 0);
-    const int c = CM ? tid / P : tid % W, j = CM ? tid % P : tid / W;
+    const int c = tid % W, j = tid / W;
     const int s = j % MY, tp = j / MY;
-    auto sync = [c] __device__() {
-        if constexpr (CM) asm volatile("bar.sync %0, %1;" ::"r"(1 + c), "r"(P) : "memory");
-        else __syncthreads();
-    };
+    constexpr int G = PB::G, WG = PB::WG;
+    auto sync = [] __device__() { __syncthreads(); };
     const int per = (n_items + gridDim.x - 1) / gridDim.x;
     const int it0 = blockIdx.x * per;
     const int it1 = min(n_items, it0 + per);
@@ -589,10 +580,6 @@ k_pass_b(BatchArgs a, int n_items) {
                               ((size_t)(j / RB) * XP + kx0 + col) * RB + (j % RB);
 #pragma unroll
                 for (int r = 0; r < V; r++) Co[(size_t)r * P * XP] = __floats2half2_rn(v[r].x * sc, v[r].y * sc);
-            } else if constexpr (CM) {
-                sync();   // the column's threads have read their last-stage inputs from colbuf
-#pragma unroll
-                for (int r = 0; r < V; r++) colbuf[tmfft::pad16(j + P * r)] = v[r];
             } else if constexpr (G == 1) {
                 float2* Co = a.C + (size_t)o * Y * XP + kx0 + col;
 #pragma unroll
@@ -603,9 +590,9 @@ k_pass_b(BatchArgs a, int n_items) {
                 for (int r = 0; r < V; r++) colbuf[tmfft::pad16(j + P * r)] = v[r];
             }
         }
-        if constexpr (G > 1 || CM) {
+        if constexpr (G > 1) {
             // the item's WG columns, row by row: whole 32-byte sectors per row
-            __syncthreads();
+            sync();
             float2* Co = a.C + (size_t)o * Y * XP + kx0;
             for (int e = tid; e < Y * WG; e += NT) {
                 const int row = e / WG, cc = e % WG;

@@ -640,6 +640,20 @@ k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
         else fail();
         tmptx::tmem_fence_after_sync();
     };
+    // the item's stage-H data (4 T values, at most NPF per thread) are loaded one item
+    // ahead, so that their latency hides behind the previous item's epilogues
+    constexpr int NPF = (4 * T + PB::NT - 1) / PB::NT;
+    float2 pf[NPF];
+    auto prefetch = [&](int itn) {
+        const int gn = itn / a.nb, on = itn % a.nb;
+        const float2* Ao = a.A + (size_t)on * T * XP + gn * 4;
+#pragma unroll
+        for (int q = 0; q < NPF; q++) {
+            const int i = t + PB::NT * q;
+            pf[q] = i < 4 * T ? __ldg(Ao + (size_t)(i >> 2) * XP + (i & 3)) : make_float2(0.f, 0.f);
+        }
+    };
+    prefetch(it0);
     for (int it = it0; it < it1; it++) {
         const int group = it / a.nb, o = it % a.nb;
         const int kx0 = group * 4;
@@ -656,16 +670,18 @@ k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
             cur_group = group;
         }
         // stage-H data: A[o][n][kx0 + c] times 2^-6 -> BH[(n2, re/im)][(c, n1)]
-        {
-            const float2* Ao = a.A + (size_t)o * T * XP + kx0;
-            for (int i = t; i < 4 * T; i += PB::NT) {
+#pragma unroll
+        for (int q = 0; q < NPF; q++) {
+            const int i = t + PB::NT * q;
+            if (i < 4 * T) {
                 const int c = i & 3, n = i >> 2;
-                const float2 v = __ldg(Ao + (size_t)n * XP + c);
                 const int nn = 64 * c + (n & 63), n2 = n >> 6;
-                *reinterpret_cast<__half*>(sBH + mnmaj_off(nn, 2 * n2, PB::BH_SBO, PB::BH_LBO)) = __float2half_rn(v.x * sA);
-                *reinterpret_cast<__half*>(sBH + mnmaj_off(nn, 2 * n2 + 1, PB::BH_SBO, PB::BH_LBO)) = __float2half_rn(v.y * sA);
+                *reinterpret_cast<__half*>(sBH + mnmaj_off(nn, 2 * n2, PB::BH_SBO, PB::BH_LBO)) = __float2half_rn(pf[q].x * sA);
+                *reinterpret_cast<__half*>(sBH + mnmaj_off(nn, 2 * n2 + 1, PB::BH_SBO, PB::BH_LBO)) =
+                    __float2half_rn(pf[q].y * sA);
             }
         }
+        if (it + 1 < it1) prefetch(it + 1);
         tmptx::fence_proxy_async_smem();
         tmptx::tmem_fence_before_sync();
         if (__syncthreads_or(timed_out)) break;
