@@ -263,6 +263,7 @@ def run_batched(args, seed=20261210):
     # one search context per padded geometry, set up as a long-running service keeps it: template
     # uploaded, orientation batch autotuned, kernels warmed
     contexts = {}
+    precisions = {}
     for m in mics:
         key = (m["X"], m["Y"])
         if key in contexts:
@@ -270,6 +271,12 @@ def run_batched(args, seed=20261210):
         hmin, hstep = prep.histogram_scaled(*key)
         sc = core.SearchCore(key[0], key[1], b["T"], histogram_min_scaled=hmin, histogram_step_scaled=hstep,
                              orientation_batch=args.batch, device=local)
+        if args.precision == "fp16":
+            try:
+                sc.set_precision(core.PRECISION_FP16_TENSOR)
+            except core.TmError:
+                pass   # geometries without the FP16 kernels (5832-high) stay FP32
+        precisions[key] = "f16" if sc.precision() == core.PRECISION_FP16_TENSOR else "f32"
         sc.set_template(tspec)
         sc.set_image(m["ispec"])
         if args.batch == 0:
@@ -301,8 +308,10 @@ def run_batched(args, seed=20261210):
     if rank == 0:
         line = {"metric": METRIC, "value": world * points / (dev_ms * 1e-3), "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "mixed",
+                "data": "synthetic",
                 "config": {"workload": b["name"], "orientations_per_plane_per_step": per_plane,
+                           "precision_by_padded_geometry": {f"{k[0]}x{k[1]}": v for k, v in precisions.items()},
                            "defocus_planes": n_planes, "parallelism": f"replicas x{world}",
                            "l2": "inputs larger than L2"},
                 "e2e": {"value": world * points / e2e_s, "unit": UNIT,
@@ -408,6 +417,90 @@ def tensor_flops_per_launch(X, Y, XP, nb):
     return col, row
 
 
+STRESS = dict(name="stress: 5760x4092 micrograph (padded 5832x4096, rotated), 384^3 template @0.8 A/px, "
+                   "9 pixel-size planes (+-2 %, 0.5 % steps) x 21 defocus planes (+-1000 A, 100 A steps)",
+              nx=5760, ny=4092, T=384, pixel_size=0.8, n_atoms=250000, radius_A=150.0, particles=40, snr=0.03,
+              defocus=12000.0, angular_step=2.5, psi_step=1.5, pixel_range=0.02, pixel_step=0.005,
+              defocus_range=1000.0, defocus_step=100.0)
+
+
+def run_stress5(args, seed=20261220):
+    """The stress configuration's plane loops on one micrograph: for each of the
+    9 pixel-size planes the template spectrum is prepared on the device at that
+    pixel size (ChangePixelSize, tm_set_template_volume), then the 21 defocus
+    planes are searched over a chunk of the orientation grid; a step is one
+    chunk over all 189 planes.  Timed end to end on the host clock (template
+    preparation included); points = original pixels x orientations x planes."""
+    from cistem_downstream_bah_b200 import core, hostprep, prep, synthetic
+    from cistem_downstream_bah_b200.core import orientation_list
+    w = STRESS
+    world, rank, local = dist_init(args)
+    vol = synthetic.template_volume(w["T"], w["pixel_size"], w["n_atoms"], w["radius_A"], seed=seed)
+    mic, _ = synthetic.micrograph(w["ny"], w["nx"], w["pixel_size"], w["n_atoms"], w["radius_A"], w["particles"],
+                                  w["snr"], w["defocus"], seed=seed + 1, atom_seed=seed)
+    X, Y = hostprep.factorize_dimension(w["nx"], w["T"]), hostprep.factorize_dimension(w["ny"], w["T"])
+    mic = hostprep.clip_into(mic, X, Y, hostprep.edge_mean(mic))
+    if not hostprep.lib().tmh_is_power_of_two(X) and hostprep.lib().tmh_is_power_of_two(Y):
+        mic = hostprep.rotate90(mic, True)
+        X, Y = Y, X
+    hmin, hstep = prep.histogram_scaled(X, Y)
+    angles = orientation_list(prep.search_grid(w["angular_step"]), 0.0, w["psi_step"], 360.0)
+    n_pix = 2 * int(round(w["pixel_range"] / w["pixel_step"])) + 1
+    n_def = 2 * int(round(w["defocus_range"] / w["defocus_step"])) + 1
+    per_plane = args.orientations_per_step // 16 or 32
+    sc = core.SearchCore(X, Y, w["T"], histogram_min_scaled=hmin, histogram_step_scaled=hstep,
+                         orientation_batch=args.batch, device=local)
+    precision = "f32"
+    if args.precision == "fp16":
+        try:
+            sc.set_precision(core.PRECISION_FP16_TENSOR)
+            precision = "f16"
+        except core.TmError:
+            pass   # the 5832-high geometry has no FP16 kernels
+    curve = sc.set_micrograph(mic)
+    # the projection filters of the defocus planes (CTF x whitening curve)
+    filts = [prep.projection_filter(w["T"], curve, kv=300.0, cs_mm=2.7, amplitude_contrast=0.07,
+                                    defocus1=w["defocus"], defocus2=w["defocus"], pixel_size=w["pixel_size"],
+                                    defocus_offset=(i - n_def // 2) * w["defocus_step"]) for i in range(n_def)]
+    factors = [1.0 + (j - n_pix // 2) * w["pixel_step"] for j in range(n_pix)]
+    sc.set_template_volume(vol, 1.0)
+    for _ in range(max(args.warmup, 1)):
+        sc.run_plane(filts[0], angles[:per_plane])
+    barrier(world)
+    points = 0.0
+    dev_ms = 0.0
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for step in range(args.steps):
+            chunk = angles[(step * per_plane) % len(angles):][:per_plane]
+            sc.reset()
+            for j, f in enumerate(factors):
+                sc.set_template_volume(vol, f)
+                for i in range(n_def):
+                    sc.run_plane(filts[i], chunk, defocus_offset=(i - n_def // 2) * w["defocus_step"],
+                                 pixel_size_offset=(j - n_pix // 2) * w["pixel_step"] * w["pixel_size"])
+                    dev_ms += sc.last_timing()["total_ms"]
+                    points += w["nx"] * w["ny"] * len(chunk)
+            sc.results()
+        el = time.perf_counter() - t0
+    sc.close()
+    el = max_over_ranks(world, el)
+    dev_ms = max_over_ranks(world, dev_ms)
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": world * points / el, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": precision, "data": "synthetic",
+            "config": {"workload": w["name"], "padded": [X, Y], "orientations_per_plane_per_step": per_plane,
+                       "pixel_size_planes": n_pix, "defocus_planes": n_def, "l2": "inputs larger than L2"},
+            "search_points_per_s_device": world * points / (dev_ms * 1e-3),
+            "e2e": {"value": world * points / el, "unit": UNIT, "h2d_bytes_per_step": int(vol.nbytes * n_pix),
+                    "d2h_bytes_per_step": int(24 * X * Y),
+                    "note": "host clock: per pixel plane the template volume upload and preparation, every plane's "
+                            "search, the results download"},
+            "gpu_launches": None, "clocks": clk.summary()}), flush=True)
+
+
 def run_ours(args):
     world, rank, local = dist_init(args)
     from cistem_downstream_bah_b200 import core
@@ -504,6 +597,29 @@ def run_ours(args):
                 fp16["accuracy_vs_fp64_oracle"] = accuracy_vs_fp64(sc16, inp, args.accuracy)
             sc16.close()
 
+    # ---- the fast form on the same workload: coarse search (FP16 where it has kernels), network,
+    # window search of the proposed tiles; the FP32 exhaustive search of the whole fine grid is the
+    # judge of its recall (about three minutes)
+    fast = None
+    if args.workload == "full" and not args.no_fast_form and world == 1:
+        pl = proposal_leg(args, inp, world, rank, local,
+                          coarse_fp16=fp16 is not None and "unavailable" not in fp16)
+        pr = pl["proposal"]
+        rc = pr["recall"]
+        fast = {"value": pl["value"], "unit": UNIT, "dtype": pl["dtype"],
+                "speedup_vs_exhaustive_fp32": pr["speedup_vs_exhaustive"],
+                "ratio_to_fp32_value": pl["value"] / value,
+                "seconds": pl["ms_per_step"] / 1e3, "exhaustive_fp32_seconds": pr["exhaustive_s"],
+                "recall_all_z7_peaks": rc["min_radius_T8"]["network_recall_z"],
+                "recall_all_z7_peaks_mip": rc["min_radius_T8"]["network_recall_mip"],
+                "recall_above_expected_threshold": rc["min_radius_T8"]["network_recall_above_expected_threshold"],
+                "expected_threshold": rc["expected_threshold"], "z7_peaks": rc["min_radius_T8"]["z7_peaks"],
+                "mip_max_rel_err_same_orientation": pr["mip_max_rel_err_same_orientation"],
+                "without_network_same_tiles": pr["without_network_same_tiles"],
+                "stages_s": {"coarse": pr["coarse_s"], "network": pr["network_s"], "windows": pr["windows_s"]},
+                "note": "effective rate = points of the exhaustive fine search / time of the proposal path "
+                        "(host buffers, synchronous calls); recall judged on the FP32 exhaustive search"}
+
     # the CPU-baseline leg (rank 0, N=1): the oracle timed on the host cores,
     # then the FP64 oracle as the checker of a few orientations after timing
     cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
@@ -536,6 +652,8 @@ def run_ours(args):
         }
         if fp16 is not None:
             line["fp16"] = fp16
+        if fast is not None:
+            line["fast_form"] = fast
         if cpu is not None:
             line["cpu_baseline"] = cpu
         if acc is not None:
@@ -657,7 +775,7 @@ def run_refine(args, seed=20261215):
 PROPOSAL_WEIGHTS = os.path.join(ROOT, "cistem_downstream_bah_b200", "data", "proposal_net.npz")
 
 
-def run_proposal(args):
+def proposal_leg(args, inp, world, rank, local, coarse_fp16=False):
     """The learned proposal on the metric's configuration (4096^2, 256^3,
     fine grid 2.5 / 1.5 deg): coarse search (7.5 / 5 deg) -> network over the
     64 x 64 tiles -> window search of the proposed tiles over the fine
@@ -668,31 +786,38 @@ def run_proposal(args):
     (thresholded coarse z, bins around the coarse best direction)."""
     from cistem_downstream_bah_b200 import core, hostprep
     from cistem_downstream_bah_b200 import proposal as PR
-    world, rank, local = dist_init(args)
     w = np.load(args.proposal_weights)
     params = w["params"]
     net_thr = float(w["network_logit_threshold"])
     heur_thr = float(w["heuristic_z_threshold"])
-    inp = make_inputs()
     X, Y, T = inp["X"], inp["Y"], inp["T"]
     angular = PR.AngularBins(7.5, WORKLOAD["angular_step"], WORKLOAD["psi_step"])
     coarse_angles = core.orientation_list(hostprep.search_grid(7.5), 0.0, 5.0, 360.0)
     sc = core.SearchCore(X, Y, T, histogram_min_scaled=inp["hmin"], histogram_step_scaled=inp["hstep"], device=local)
     sc.set_image(inp["ispec"])
     sc.set_template(inp["tspec"])
+    # the exhaustive judge runs on this context in FP32; the coarse search optionally in FP16
+    sc16 = None
+    if coarse_fp16:
+        sc16 = core.SearchCore(X, Y, T, histogram_min_scaled=inp["hmin"], histogram_step_scaled=inp["hstep"],
+                               device=local)
+        sc16.set_precision(core.PRECISION_FP16_TENSOR)
+        sc16.set_image(inp["ispec"])
+        sc16.set_template(inp["tspec"])
+    sc_coarse = sc16 if sc16 is not None else sc
     net = PR.ProposalNet(PR.FEATURES, PR.TILE, max_batch=256, device=local)
     net.set_params(params)
     ws = PR.WindowSearch(inp["ispec"], X, Y, T, inp["tspec"], inp["filt"], angular, inp["hmin"], inp["hstep"],
                          device=local)
     # warm-up: kernels of both geometries, the network
     for _ in range(max(args.warmup, 1)):
-        PR.search_maps(sc, inp["filt"], coarse_angles[:256], X, Y)
+        PR.search_maps(sc_coarse, inp["filt"], coarse_angles[:256], X, Y)
         ws.run(PR.Proposal([0], [angular.nearest([0.0, 0.0, 1.0], 1)], None))
         net.forward(np.zeros((4, PR.FEATURES, PR.TILE, PR.TILE), np.float32))
     barrier(world)
     with ClockSampler(local) as clk:
         t0 = time.perf_counter()
-        coarse = PR.search_maps(sc, inp["filt"], coarse_angles, X, Y)
+        coarse = PR.search_maps(sc_coarse, inp["filt"], coarse_angles, X, Y)
         t1 = time.perf_counter()
         frames = PR.tile_frames(coarse["z"], coarse["theta"], coarse["phi"])
         feats = PR.tile_features(coarse["z"], coarse["theta"], coarse["phi"], frames=frames)
@@ -759,12 +884,15 @@ def run_proposal(args):
     ws.close()
     net.close()
     sc.close()
+    if sc16 is not None:
+        sc16.close()
     pts_exh = exh["points"]
-    if rank == 0:
-        print(json.dumps({
+    line = {
             "metric": METRIC, "value": pts_exh / t_prop, "unit": UNIT, "n_gpus": world, "steps": 1,
             "warmup": args.warmup, "ms_per_step": t_prop * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 search, bf16 network weights", "data": "synthetic",
+            "vs_baseline": None,
+            "dtype": ("f16 tensor-core coarse search, " if sc16 is not None else "f32 coarse search, ") +
+                     "f32 window search and exhaustive judge, bf16 network weights", "data": "synthetic",
             "config": {"workload": "learned proposal: " + WORKLOAD["name"] + ", coarse 7.5/5.0 deg, 16 bins per tile",
                        "flush_l2": "inputs > L2"},
             "e2e": {"value": pts_exh / t_prop, "unit": UNIT, "h2d_bytes_per_step": int(inp["ispec"].nbytes),
@@ -780,10 +908,9 @@ def run_proposal(args):
                                                "speedup_vs_exhaustive": exh["seconds"] / t_top},
                 "without_network_threshold": {"tiles": int(len(heur.tiles)), "z_threshold": heur_thr},
                 "network_logit_threshold": net_thr},
-            "gpu_launches": n_launch_coarse + n_launch_net + res["launches"], "clocks": clk.summary()}), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+            "gpu_launches": n_launch_coarse + n_launch_net + res["launches"], "clocks": clk.summary()}
+    return line
+
 
 
 def run_recall16(args):
@@ -850,6 +977,16 @@ def run_recall16(args):
             "gpu_launches": None, "clocks": {"fp32": e["clocks"], "fp16": f["clocks"]}}), flush=True)
 
 
+def run_proposal(args):
+    world, rank, local = dist_init(args)
+    line = proposal_leg(args, make_inputs(), world, rank, local, coarse_fp16=args.precision == "fp16")
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def _cpu_threads():
     """Host threads for the CPU legs (each thread holds ~0.6 GB of 4096^2 buffers)."""
     threads = min(os.cpu_count() or 1, 32)
@@ -904,6 +1041,8 @@ def main():
                     help="fp32 = the parity path; fp16 = FP16 correlation spectra with the tensor-core row transform")
     ap.add_argument("--cpu-sample", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fast-form", action="store_true",
+                    help="skip the learned-proposal fast form (and its three-minute exhaustive judge)")
     ap.add_argument("--no-fp16-leg", action="store_true",
                     help="skip the FP16 tensor-core form that the default run times beside the FP32 path")
     ap.add_argument("--accuracy", type=int, default=4,
@@ -911,7 +1050,7 @@ def main():
     ap.add_argument("--recall-orientations", type=int, default=0,
                     help="--workload recall16: orientations searched (0 = the whole grid)")
     ap.add_argument("--workload", default="full",
-                    choices=sorted(WORKLOADS) + ["batched", "refine", "proposal", "recall16"],
+                    choices=sorted(WORKLOADS) + ["batched", "refine", "proposal", "recall16", "stress5"],
                     help="full = the metric's 4096^2 configuration; the others are the uneven and stress geometries")
     ap.add_argument("--e2e-contexts", type=int, default=2,
                     help="host threads (each with its own search context) sharing the GPU in the e2e leg")
@@ -938,6 +1077,8 @@ def main():
         run_proposal(args)
     elif args.workload == "recall16":
         run_recall16(args)
+    elif args.workload == "stress5":
+        run_stress5(args)
     else:
         run_ours(args)
 
