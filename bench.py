@@ -692,10 +692,13 @@ def accuracy_vs_fp64(sc, inp, k):
     gpu.mip[:], gpu.sum[:], gpu.sumsq[:] = r["mip"], r["sum"], r["sumsq"]
     mip_got, z_got, _, _ = O.finalize(gpu, k, sq)
     scale = float(np.abs(mip_ref).max())
+    from cistem_downstream_bah_b200 import core
+    form = "FP16 tensor-core" if sc.precision() == core.PRECISION_FP16_TENSOR else "FP32"
     return {"orientations": int(k),
             "mip_max_rel_err": float(np.abs(mip_got - mip_ref).max() / scale),
             "z_max_abs_err": float(np.abs(z_got - z_ref).max()),
-            "note": "FP32 search vs FP64 oracle, MIP error relative to the MIP scale"}
+            "note": f"{form} search vs FP64 oracle, MIP error relative to the MIP scale; z over these "
+                    f"{int(k)} orientations only"}
 
 
 def _oracle_sample(inp, n_orient, bits=32):

@@ -62,8 +62,12 @@ typedef struct tm_dims {
 typedef int (*tm_progress_fn)(long long orientations_done, long long orientations_total, void *user);
 
 /* Replaces TemplateMatchingCore::Init's device set-up (TemplateMatchingCore.cu:49-138):
- * allocates every device buffer for the geometry.  Status TM_ERR_UNSUPPORTED
- * if no kernel variant exists for (image_x, image_y, template_size). */
+ * allocates every device buffer for the geometry.  Geometries with compiled
+ * kernel variants run those; any other micrograph with both sides in 64..8192
+ * whose lengths (and half width, when even) factor into 2, 3, 5, 7, 11 and 13
+ * -- every size the reference's padding picks -- runs the run-time-length
+ * kernels, for templates of 32, 48, 64, 128, 256 or 384.  Status
+ * TM_ERR_UNSUPPORTED otherwise. */
 TM_API int tm_create(const tm_dims *dims, tm_ctx **out);
 
 /* Uploads the template spectrum: the quadrant-swapped Fourier transform of the
