@@ -38,7 +38,7 @@ EXPORTED = [
     "tm_set_template_volume", "tm_template_spectrum", "tm_set_normalization_pixels", "tm_pnet_create",
     "tm_pnet_param_count", "tm_pnet_set_params", "tm_pnet_get_params", "tm_pnet_forward", "tm_pnet_gradients",
     "tm_pnet_train_step", "tm_pnet_last_error", "tm_pnet_destroy", "tm_set_image_set", "tm_run_plane_images",
-    "tm_get_image_results", "tm_set_precision", "tm_get_precision",
+    "tm_get_image_results", "tm_set_precision", "tm_get_precision", "tm_debug_gemm",
 ]
 
 
@@ -113,6 +113,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.tm_run_plane_images.argtypes = [vp, vp, vp, ip, vp, ip, fp, fp]
     L.tm_get_image_results.argtypes = [vp, ip, vp, vp, vp, vp]
     L.tm_set_precision.argtypes = [vp, ip]
+    L.tm_debug_gemm.argtypes = [ip, ip, ip, ip, vp, vp, vp, fp, ip, ip]
     L.tm_get_precision.argtypes = [vp]
     _LIB = L
     return L
@@ -415,6 +416,21 @@ def whiten_micrograph(image, device=0):
     if rc != TM_OK:
         raise TmError(rc, "tm_whiten_micrograph failed")
     return spec, curve[:n.value].copy()
+
+
+def debug_gemm(A, B, C=None, s=0.0, accumulate=False, tensor=True, device=0):
+    """(A - s) B (+ C) through the library's device GEMM (tm_debug_gemm):
+    tensor=True the tensor-core form, False the CUDA-core form."""
+    L = load()
+    a = np.ascontiguousarray(A, dtype=np.float32)
+    b = np.ascontiguousarray(B, dtype=np.float32)
+    M, K = a.shape
+    N = b.shape[1]
+    c = np.zeros((M, N), np.float32) if C is None else np.array(C, dtype=np.float32, order="C")
+    rc = L.tm_debug_gemm(device, M, N, K, _ptr(a), _ptr(b), _ptr(c), float(s), int(bool(accumulate)), int(bool(tensor)))
+    if rc != TM_OK:
+        raise TmError(rc, "tm_debug_gemm failed")
+    return c
 
 
 def template_spectrum_device(volume, pixel_size_factor=1.0, device=0):

@@ -659,6 +659,7 @@ struct TemplateBuffers {
     float* pad;           // 1 float
     tmcg::GemmJob* jobs;  // 4 + 4 T jobs
     tmfft::Twiddles tw;   // lmax = T
+    int* gemm_err;        // 1 int: set by a tensor-core GEMM whose completion wait ran out
 };
 using TemplateFn = int (*)(cudaStream_t, int nsm, const TemplateBuffers&, float factor, std::string& err);
 
@@ -737,18 +738,14 @@ int template_on_device(cudaStream_t s, int nsm, const TemplateBuffers& b, float 
                 jobs.push_back({A, Bm, Cm, nullptr});
             }
         TW_CHECK(cudaMemcpyAsync(b.jobs, jobs.data(), sizeof(tmcg::GemmJob) * jobs.size(), cudaMemcpyHostToDevice, s));
+        TW_CHECK(cudaMemsetAsync(b.gemm_err, 0, sizeof(int), s));
+        // the separable operators on the tensor cores (split TF32, FP32 accumulation)
         const int TT = T * T;
-        tmcg::k_gemm<<<dim3((T + 127) / 128, (TT + 127) / 128, 2), 256, 0, s>>>(b.jobs, TT, T, T, T, T, T, 0);
-        TW_CHECK(cudaGetLastError());
-        for (int pass = 0; pass < 4; pass++) {
-            tmcg::k_gemm<<<dim3((T + 127) / 128, (T + 127) / 128, T), 256, 0, s>>>(b.jobs + 4 + pass * T, T, T, T, T, T, T,
-                                                                              pass % 2);
-            TW_CHECK(cudaGetLastError());
-        }
-        tmcg::k_gemm<<<dim3((TT + 127) / 128, (T + 127) / 128, 1), 256, 0, s>>>(b.jobs + 2, T, TT, T, T, TT, TT, 0);
-        TW_CHECK(cudaGetLastError());
-        tmcg::k_gemm<<<dim3((TT + 127) / 128, (T + 127) / 128, 1), 256, 0, s>>>(b.jobs + 3, T, TT, T, T, TT, TT, 1);
-        TW_CHECK(cudaGetLastError());
+        TW_CHECK(tmcg::gemm_tc(b.jobs, 2, TT, T, T, T, T, T, 0, b.gemm_err, s));
+        for (int pass = 0; pass < 4; pass++)
+            TW_CHECK(tmcg::gemm_tc(b.jobs + 4 + pass * T, T, T, T, T, T, T, T, pass % 2, b.gemm_err, s));
+        TW_CHECK(tmcg::gemm_tc(b.jobs + 2, 1, T, TT, T, T, TT, TT, 0, b.gemm_err, s));
+        TW_CHECK(tmcg::gemm_tc(b.jobs + 3, 1, T, TT, T, T, TT, TT, 1, b.gemm_err, s));
         rows_src = out;
         add = padding_value;
     }
@@ -762,7 +759,13 @@ int template_on_device(cudaStream_t s, int nsm, const TemplateBuffers& b, float 
     TW_CHECK(cudaGetLastError());
     tmt::k_t_cols<T><<<(unsigned)((ncols + C::CB - 1) / C::CB), C::NT, 0, s>>>(b.spec, ncols, ncols, 0, ncols, 1, b.tw);
     TW_CHECK(cudaGetLastError());
+    int gemm_failed = 0;
+    if (rows_src != b.vol) TW_CHECK(cudaMemcpyAsync(&gemm_failed, b.gemm_err, sizeof(int), cudaMemcpyDeviceToHost, s));
     TW_CHECK(cudaStreamSynchronize(s));
+    if (gemm_failed) {
+        err = "a tensor-core GEMM of the pixel-size change timed out";
+        return TM_ERR_TIMEOUT;
+    }
     return TM_OK;
 }
 
@@ -789,8 +792,9 @@ struct TemplateScratch {
     double* acc = nullptr;
     float* pad = nullptr;
     tmcg::GemmJob* jobs = nullptr;
+    int* gemm_err = nullptr;
     void release() {
-        void* p[] = {vol, work, ops, acc, pad, jobs};
+        void* p[] = {vol, work, ops, acc, pad, jobs, gemm_err};
         for (void* q : p)
             if (q) cudaFree(q);
         *this = TemplateScratch{};
@@ -803,6 +807,7 @@ struct TemplateScratch {
         if (e == cudaSuccess && resample) e = cudaMalloc((void**)&work, sizeof(float) * 5 * n3);
         if (e == cudaSuccess && resample) e = cudaMalloc((void**)&ops, sizeof(float) * 7 * (size_t)T * T);
         if (e == cudaSuccess && resample) e = cudaMalloc((void**)&jobs, sizeof(tmcg::GemmJob) * (4 + 4 * (size_t)T));
+        if (e == cudaSuccess && resample) e = cudaMalloc((void**)&gemm_err, sizeof(int));
         return e;
     }
 };
@@ -1068,7 +1073,7 @@ int tm_set_template_volume(tm_ctx* c, const float* volume, int template_size, fl
     e = cudaMemcpyAsync(sc.vol, volume, sizeof(float) * (size_t)c->T * c->T * c->T, cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) rc = set_err(c, TM_ERR_CUDA, "template upload: %s", cudaGetErrorString(e));
     if (rc == TM_OK) {
-        TemplateBuffers tb{sc.vol, c->tmpl, sc.work, sc.ops, sc.acc, sc.pad, sc.jobs, make_args(c).twt};
+        TemplateBuffers tb{sc.vol, c->tmpl, sc.work, sc.ops, sc.acc, sc.pad, sc.jobs, make_args(c).twt, sc.gemm_err};
         std::string err;
         rc = fn(c->stream, c->nsm, tb, pixel_size_factor, err);
         if (rc != TM_OK) set_err(c, rc, "template preparation: %s", err.c_str());
@@ -1109,7 +1114,7 @@ int tm_template_spectrum(int device, const float* volume, int template_size, flo
     }
     if (rc == TM_OK) fail(cudaMemcpyAsync(sc.vol, volume, sizeof(float) * (size_t)T * T * T, cudaMemcpyHostToDevice, s));
     if (rc == TM_OK) {
-        TemplateBuffers tb{sc.vol, d_spec, sc.work, sc.ops, sc.acc, sc.pad, sc.jobs, tmfft::Twiddles{d_tw, T}};
+        TemplateBuffers tb{sc.vol, d_spec, sc.work, sc.ops, sc.acc, sc.pad, sc.jobs, tmfft::Twiddles{d_tw, T}, sc.gemm_err};
         std::string err;
         rc = fn(s, nsm > 0 ? nsm : 148, tb, pixel_size_factor, err);
     }
@@ -1119,6 +1124,54 @@ int tm_template_spectrum(int device, const float* volume, int template_size, flo
     if (d_spec) cudaFree(d_spec);
     if (d_tw) cudaFree(d_tw);
     if (s) cudaStreamDestroy(s);
+    return rc;
+}
+
+int tm_debug_gemm(int device, int M, int N, int K, const float* A, const float* B, float* C, float s, int accumulate,
+                  int tensor) {
+    if (!A || !B || !C || M <= 0 || N <= 0 || K <= 0) return TM_ERR_INVALID;
+    if (cudaSetDevice(device) != cudaSuccess) return TM_ERR_CUDA;
+    float *dA = nullptr, *dB = nullptr, *dC = nullptr, *ds = nullptr;
+    int* derr = nullptr;
+    tmcg::GemmJob* dj = nullptr;
+    cudaStream_t st = nullptr;
+    int rc = TM_OK;
+    auto fail = [&](cudaError_t e) {
+        if (e != cudaSuccess && rc == TM_OK) rc = e == cudaErrorMemoryAllocation ? TM_ERR_OOM : TM_ERR_CUDA;
+    };
+    fail(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    if (rc == TM_OK) fail(cudaMalloc((void**)&dA, sizeof(float) * (size_t)M * K));
+    if (rc == TM_OK) fail(cudaMalloc((void**)&dB, sizeof(float) * (size_t)K * N));
+    if (rc == TM_OK) fail(cudaMalloc((void**)&dC, sizeof(float) * (size_t)M * N));
+    if (rc == TM_OK) fail(cudaMalloc((void**)&ds, sizeof(float)));
+    if (rc == TM_OK) fail(cudaMalloc((void**)&derr, sizeof(int)));
+    if (rc == TM_OK) fail(cudaMalloc((void**)&dj, sizeof(tmcg::GemmJob)));
+    if (rc == TM_OK) fail(cudaMemcpy(dA, A, sizeof(float) * (size_t)M * K, cudaMemcpyHostToDevice));
+    if (rc == TM_OK) fail(cudaMemcpy(dB, B, sizeof(float) * (size_t)K * N, cudaMemcpyHostToDevice));
+    if (rc == TM_OK) fail(cudaMemcpy(dC, C, sizeof(float) * (size_t)M * N, cudaMemcpyHostToDevice));
+    if (rc == TM_OK) fail(cudaMemcpy(ds, &s, sizeof(float), cudaMemcpyHostToDevice));
+    if (rc == TM_OK) fail(cudaMemset(derr, 0, sizeof(int)));
+    if (rc == TM_OK) {
+        const tmcg::GemmJob job{dA, dB, dC, ds};
+        fail(cudaMemcpy(dj, &job, sizeof job, cudaMemcpyHostToDevice));
+    }
+    if (rc == TM_OK) {
+        if (tensor) {
+            fail(tmcg::gemm_tc(dj, 1, M, N, K, K, N, N, accumulate, derr, st));
+        } else {
+            tmcg::k_gemm<<<dim3((N + 127) / 128, (M + 127) / 128, 1), 256, 0, st>>>(dj, M, N, K, K, N, N, accumulate);
+            fail(cudaGetLastError());
+        }
+    }
+    int failed = 0;
+    if (rc == TM_OK) fail(cudaStreamSynchronize(st));
+    if (rc == TM_OK) fail(cudaMemcpy(&failed, derr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (rc == TM_OK && failed) rc = TM_ERR_TIMEOUT;
+    if (rc == TM_OK) fail(cudaMemcpy(C, dC, sizeof(float) * (size_t)M * N, cudaMemcpyDeviceToHost));
+    void* p[] = {dA, dB, dC, ds, derr, dj};
+    for (void* q : p)
+        if (q) cudaFree(q);
+    if (st) cudaStreamDestroy(st);
     return rc;
 }
 

@@ -399,10 +399,20 @@ struct PassB {
     // cover whole 32-byte sectors of a row (G > 1 only for 2-column chunks)
     static constexpr int G = W >= 4 ? 1 : 4 / W;
     static constexpr int WG = W * G;                                // columns per work item
-    // bank skews (float2 units, half-warp = 16 lanes = (16/W) values of j x W columns)
+    // A 1024-thread block of at least 8 columns runs as NH = 2 independent
+    // halves of 512 threads (W/2 columns each, own named barrier), so that one
+    // half's transforms issue while the other waits at a barrier.  A warp then
+    // covers W/2 >= 4 adjacent columns, whole 32-byte sectors of each row.  (With
+    // 4 columns each half would write 16-byte halves of the sectors; measured at
+    // 4096 x 4096, the L2 did not merge them and the DRAM traffic of the pass
+    // rose from 11 to 30 GB per 128 orientations, so 4-column blocks stay whole.)
+    static constexpr int NH = (NT == 1024 && G == 1 && W >= 8) ? 2 : 1;
+    static constexpr int WL = W / NH;                               // columns interleaved in a warp
+    static constexpr int NTH = NT / NH;                             // threads per half
+    // bank skews (float2 units, half-warp = 16 lanes = (16/WL) values of j x WL columns)
     static constexpr int RST = (tmfft::padded_len(L) + 15) / 16 * 16 + 1;       // == 1 (mod 16)
     static constexpr int CS0 = (MY * RST > tmfft::padded_len(Y)) ? MY * RST : tmfft::padded_len(Y);
-    static constexpr int CS = (CS0 + 15) / 16 * 16 + 16 / W;                  // == 16/W (mod 16)
+    static constexpr int CS = (CS0 + 15) / 16 * 16 + 16 / WL;                 // == 16/WL (mod 16)
     static constexpr size_t EXCH = (sizeof(float2) * WG * CS + 15) / 16 * 16;
     static constexpr size_t ASZ = sizeof(float2) * T * WG;          // one A staging buffer
     static constexpr int ABUFS = (EXCH + 2 * ASZ + 64 <= 232448) ? 2 : 1;
@@ -419,6 +429,7 @@ struct PassB {
     static_assert(NT <= 1024 && SMEM <= 232448, "pass B block exceeds the per-block limits");
     static_assert(TMEM_COLS <= 512, "pass B TMEM layout exceeds 512 columns");
     static_assert(V == 16 || V == 18 || V == 32, "TMEM load sequence covers 16, 18 or 32 values");
+    static_assert(NH == 1 || (NTH % 32 == 0 && W % NH == 0), "halves must be whole warps and whole columns");
 };
 
 // I' values of one thread (V complex, 2V floats) into its TMEM columns
@@ -451,10 +462,17 @@ k_pass_b(BatchArgs a, int n_items) {
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const bool tmem_warp = warp < PB::FULL_WARPS;   // uniform per warp
-    const int c = tid % W, j = tid / W;
+    constexpr int NH = PB::NH, WL = PB::WL, NTH = PB::NTH;
+    // half h owns columns h*WL .. h*WL + WL - 1; within it thread = c' + WL*j
+    const int h = tid / NTH, loc = tid % NTH;
+    const int c = h * WL + loc % WL, j = loc / WL;
     const int s = j % MY, tp = j / MY;
     constexpr int G = PB::G, WG = PB::WG;
-    auto sync = [] __device__() { __syncthreads(); };
+    // the barrier over the threads that share this thread's columns
+    auto sync = [h]() {
+        if constexpr (NH == 1) __syncthreads();
+        else asm volatile("bar.sync %0, %1;" ::"r"(1 + h), "n"(NTH) : "memory");
+    };
     const int per = (n_items + gridDim.x - 1) / gridDim.x;
     const int it0 = blockIdx.x * per;
     const int it1 = min(n_items, it0 + per);
@@ -467,10 +485,16 @@ k_pass_b(BatchArgs a, int n_items) {
     __syncthreads();
     tmptx::tmem_fence_after_sync();
     const uint32_t tmem = *tmem_slot + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(PB::TCOLS * G * (warp >> 2));
+    // the item's T rows of A into dst[row][WG]: each half copies (and later
+    // reads) only its own columns
+    constexpr int WGH = WG / NH;   // the item's columns per half
     auto issue_rows = [&](int it, float2* dst) {
         const int grp = it / a.nb, oo = it % a.nb;
-        const float2* src = a.A + (size_t)oo * T * XP + grp * WG;
-        for (int e = tid; e < T * WG; e += NT) tmptx::cp_async8(dst + e, src + (size_t)(e / WG) * XP + (e % WG));
+        const float2* src = a.A + (size_t)oo * T * XP + grp * WG + h * WGH;
+        for (int e = loc; e < T * WGH; e += NTH) {
+            const int row = e / WGH, cc = e % WGH;
+            tmptx::cp_async8(dst + row * WG + h * WGH + cc, src + (size_t)row * XP + cc);
+        }
     };
     if (PB::ABUFS == 2) {
         issue_rows(it0, abuf);
@@ -491,7 +515,8 @@ k_pass_b(BatchArgs a, int n_items) {
         // previous item's forward transform, whose barriers every thread has
         // passed; the exchange buffers are guarded by the transforms' own barriers.
         // With a single staging buffer the rows are reloaded in place, after a barrier.
-        if (PB::ABUFS == 1) __syncthreads();
+        // (Each half copies and reads only its own columns, so its own barrier suffices.)
+        if (PB::ABUFS == 1) sync();
         if (PB::ABUFS == 2) {
             if (it + 1 < it1) issue_rows(it + 1, anext);
             tmptx::cp_async_commit();
@@ -501,7 +526,7 @@ k_pass_b(BatchArgs a, int n_items) {
             tmptx::cp_async_commit();
             tmptx::cp_async_wait<0>();
         }
-        __syncthreads();  // this item's rows of A are visible to every thread
+        sync();  // this item's rows of A are visible to every thread of the half
         if (group != cur_group && tmem_warp) {
             // the V I' values this thread multiplies with in each chunk of the
             // group, into its TMEM columns
@@ -615,6 +640,17 @@ k_pass_b(BatchArgs a, int n_items) {
 // X = 4096 (256 threads, two blocks per SM, 128 registers) a thread parks the
 // compensation terms of both sums and its sums of squares in its TMEM lane
 // between orientations (columns 0-15, 16-31 and 32-47 of its 64).
+// Copies of a block's shared-memory histogram: lane l counts into copy
+// l % n, bin b of copy c at word b * n + c, so that lanes of one warp whose
+// values fall in the same bin (the bins near zero take most of them) rarely
+// update the same word or bank.  n is the largest power of two up to
+// max_copies whose copies fit in 32 KB.
+__host__ __device__ inline int hist_copies(int bins, int max_copies) {
+    int n = max_copies;
+    while (n > 1 && (long long)bins * n * 4 > 32768) n >>= 1;
+    return n;
+}
+
 template <int X>
 struct PassC {
     static constexpr int H = X / 2;
@@ -623,8 +659,13 @@ struct PassC {
     static constexpr int RSF = tmfft::padded_len(H);
     static constexpr bool COMP_IN_TMEM = X >= 4096 && P % 32 == 0;
     static constexpr uint32_t TMEM_COLS = 64 * ((P / 32 + 3) / 4);   // warps of a lane quadrant side by side
+    // one histogram copy: measured at X = 4096, 16 lane-striped copies (32 KB
+    // more shared memory per block, less L1) made this pass 5 % slower
+    static constexpr int HIST_COPIES = 1;
     // dynamic shared memory for a row pitch XP and `bins` histogram bins
-    static size_t smem_bytes(int XP, int bins) { return 128 + sizeof(float2) * (2 * (size_t)XP + RSF) + 4 * (size_t)bins; }
+    static size_t smem_bytes(int XP, int bins) {
+        return 128 + sizeof(float2) * (2 * (size_t)XP + RSF) + 4 * (size_t)bins * hist_copies(bins, HIST_COPIES);
+    }
 };
 
 template <int X>
@@ -659,7 +700,9 @@ k_pass_c(BatchArgs a, int Y) {
             tmptx::tmem_relinquish();
         }
     }
-    for (int b = t; b < a.hist_bins; b += P) shist[b] = 0u;
+    const int hcopies = hist_copies(a.hist_bins, PC::HIST_COPIES);
+    const int hcopy = t & (hcopies - 1);
+    for (int b = t; b < a.hist_bins * hcopies; b += P) shist[b] = 0u;
     if constexpr (kTm) tmptx::tmem_fence_before_sync();
     __syncthreads();
     if constexpr (kTm) tmptx::tmem_fence_after_sync();
@@ -772,7 +815,7 @@ k_pass_c(BatchArgs a, int Y) {
                         comp[pi] = (ts - fs[pi]) - ys;
                         fs[pi] = ts;
                         const int bin = __float2int_rz((val - a.hist_min) * a.hist_inv_step);
-                        if (bin >= 0 && bin < a.hist_bins) atomicAdd(&shist[bin], 1u);
+                        if (bin >= 0 && bin < a.hist_bins) atomicAdd(&shist[bin * hcopies + hcopy], 1u);
                     } else {
                         const float yq = fmaf(val, val, -comp[pi]);
                         const float tq = fq[pi] + yq;
@@ -829,7 +872,8 @@ k_pass_c(BatchArgs a, int Y) {
     }
     __syncthreads();
     for (int b = t; b < a.hist_bins; b += P) {
-        const unsigned int cnt = shist[b];
+        unsigned int cnt = 0;
+        for (int k = 0; k < hcopies; k++) cnt += shist[b * hcopies + k];
         if (cnt) atomicAdd(a.hist + b, (unsigned long long)cnt);
     }
 }
@@ -918,17 +962,23 @@ struct LaunchTc {
     static constexpr size_t rows_tab_bytes = (size_t)PCT::B1_BYTES + PCT::B2_BYTES;
     static cudaError_t configure(int XP, int bins) {
         cudaError_t e;
-        if constexpr (COL_TC)
+        if constexpr (COL_TC) {
             e = cudaFuncSetAttribute(k_pass_b_tc<T, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, PBT::SMEM);
-        else
+            // two CTAs of a pair per SM need the largest shared-memory carveout
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_pass_b_tc<T, R>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared);
+        } else
             e = cudaFuncSetAttribute(k_pass_b<T, Y, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB::SMEM);
         if (e != cudaSuccess) return e;
         return cudaFuncSetAttribute(k_pass_c_tc<X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PCT::smem_bytes(XP, bins));
     }
     static void pass_b(BatchArgs& a, cudaStream_t s, int nsm, const uint4* tabs) {
         if constexpr (COL_TC) {
+            // items = (group of 4 columns, orientation); two CTAs (the group's two column pairs) per item range
             const int n_items = (a.XP / 4) * a.nb;
-            k_pass_b_tc<T, R><<<n_items < nsm ? n_items : nsm, PBT::NT, PBT::SMEM, s>>>(a, n_items, tabs + rows_tab_bytes / 16);
+            k_pass_b_tc<T, R><<<2 * (n_items < nsm ? n_items : nsm), PBT::NT, PBT::SMEM, s>>>(a, n_items,
+                                                                                          tabs + rows_tab_bytes / 16);
         } else {
             const int n_items = (a.XP / PB::WG) * a.nb;
             k_pass_b<T, Y, R><<<n_items < nsm ? n_items : nsm, PB::NT, PB::SMEM, s>>>(a, n_items);

@@ -175,6 +175,24 @@ __device__ __forceinline__ void mma_f16_ss(uint32_t d_tmem, uint64_t a_desc, uin
         : "memory");
 }
 
+// kind::tf32: A and B are 32-bit elements in shared memory of which the
+// tensor core uses the TF32 part (sign, exponent, 10 mantissa bits); a core
+// matrix row is 16 bytes = 4 elements, one instruction covers K = 8.
+// Instruction descriptor: D format F32, A and B format TF32 (2 in bits [7,10)
+// and [10,13)), both operands K-major, N >> 3 in bits [17,23), M >> 4 in [24,29).
+__host__ __device__ constexpr uint32_t idesc_tf32_f32(int M, int N) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void mma_tf32_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                            bool accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate ? 1u : 0u)
+        : "memory");
+}
+
 // The mbarrier receives one arrival when every MMA this thread issued before
 // has completed.
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {

@@ -57,6 +57,7 @@ using tmrk::tmfft::Twiddles;
 using tmrk::tmk::skewed;
 namespace tmfft = tmrk::tmfft;
 namespace tmk = tmrk::tmk;
+namespace tmptx = tmrk::tmptx;
 
 struct ScoreArgs {
     int nb;
@@ -357,6 +358,7 @@ struct tm_refine_ctx {
     double *rowstat = nullptr, *sumsq = nullptr, *pvsum = nullptr;
     long long disc_count = 1;
     int *cand = nullptr, *rowarg = nullptr, *jobs = nullptr, *has_pad = nullptr;
+    int* gemm_err = nullptr;   // set by a tensor-core GEMM whose completion wait ran out
     tmr::GemmJob* gjobs = nullptr;
     int* op_has_pad_host = nullptr;
     // page-locked staging of the per-batch inputs and outputs
@@ -365,6 +367,7 @@ struct tm_refine_ctx {
     int* h_jobs = nullptr;
     tmr::GemmJob* h_gjobs = nullptr;
     float* h_out = nullptr;
+    int* h_gemm_err = nullptr;
     std::vector<char> op_set;
     int (*run)(tm_refine_ctx*, int n, int n_jobs) = nullptr;
     std::string err;
@@ -427,17 +430,12 @@ int run_batch(tm_refine_ctx* c, int n, int n_jobs) {
         tmr::k_disc_mean<<<(n_jobs + 127) / 128, 128, 0, s>>>(c->jobs, c->has_pad, c->pvsum, c->pv, n_jobs,
                                                               1.0 / (double)c->disc_count);
         TR_LAUNCHED("k_disc_mean");
+        // on the tensor cores (split TF32, FP32 accumulation):
         // Z = (P - pv) [brt | bit]            (TP x 2T)
-        tmr::k_gemm<<<dim3((2 * T + 127) / 128, (TP + 127) / 128, n_jobs), 256, 0, s>>>(c->gjobs, TP, 2 * T, TP, TP,
-                                                                                    2 * T, 2 * T, 0);
-        TR_LAUNCHED("k_gemm (1)");
+        TR_CUDA(c, tmr::gemm_tc(c->gjobs, n_jobs, TP, 2 * T, TP, TP, 2 * T, 2 * T, 0, c->gemm_err, s));
         // Q = Ar Z[:, :T] + (-Ai) Z[:, T:]     (T x T)
-        tmr::k_gemm<<<dim3((T + 127) / 128, (T + 127) / 128, n_jobs), 256, 0, s>>>(c->gjobs + n_jobs, T, T, TP, 2 * TP,
-                                                                              2 * T, T, 0);
-        TR_LAUNCHED("k_gemm (2)");
-        tmr::k_gemm<<<dim3((T + 127) / 128, (T + 127) / 128, n_jobs), 256, 0, s>>>(c->gjobs + 2 * n_jobs, T, T, TP,
-                                                                              2 * TP, 2 * T, T, 1);
-        TR_LAUNCHED("k_gemm (3)");
+        TR_CUDA(c, tmr::gemm_tc(c->gjobs + n_jobs, n_jobs, T, T, TP, 2 * TP, 2 * T, T, 0, c->gemm_err, s));
+        TR_CUDA(c, tmr::gemm_tc(c->gjobs + 2 * n_jobs, n_jobs, T, T, TP, 2 * TP, 2 * T, T, 1, c->gemm_err, s));
     }
     TR_CUDA(c, cudaMemsetAsync(c->sumsq, 0, sizeof(double) * n, s));
     tmr::ScoreArgs sa{};
@@ -488,10 +486,10 @@ const RefineVariant kRefineVariants[] = {
 void rfree(tm_refine_ctx* c) {
     void* d[] = {c->tmpl, c->particles, c->S, c->R, c->tw_tp, c->tw_t, c->filters, c->ops, c->ones, c->rot, c->P,
                  c->Z, c->Q, c->pv, c->rowmax, c->out, c->rowstat, c->sumsq, c->pvsum, c->cand, c->rowarg,
-                 c->jobs, c->gjobs};   // has_pad lives inside jobs
+                 c->jobs, c->gjobs, c->gemm_err};   // has_pad lives inside jobs
     for (void* p : d)
         if (p) cudaFree(p);
-    void* h[] = {c->h_rot, c->h_cand, c->h_jobs, c->h_gjobs, c->h_out, c->op_has_pad_host};
+    void* h[] = {c->h_rot, c->h_cand, c->h_jobs, c->h_gjobs, c->h_out, c->op_has_pad_host, c->h_gemm_err};
     for (void* p : h)
         if (p) cudaFreeHost(p);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -592,12 +590,14 @@ int tm_refine_create(int device, int template_box, int projection_box, const flo
     TRY(dalloc(c, &c->cand, (size_t)3 * max_batch));
     TRY(dalloc(c, &c->jobs, (size_t)2 * max_batch));
     TRY(dalloc(c, &c->gjobs, (size_t)3 * max_batch));
+    TRY(dalloc(c, &c->gemm_err, 1));
     c->has_pad = c->jobs + max_batch;
     TR_CUDA(c, cudaMallocHost((void**)&c->h_rot, sizeof(float) * 6 * max_batch));
     TR_CUDA(c, cudaMallocHost((void**)&c->h_cand, sizeof(int) * 3 * max_batch));
     TR_CUDA(c, cudaMallocHost((void**)&c->h_jobs, sizeof(int) * 2 * max_batch));
     TR_CUDA(c, cudaMallocHost((void**)&c->h_gjobs, sizeof(tmr::GemmJob) * 3 * max_batch));
     TR_CUDA(c, cudaMallocHost((void**)&c->h_out, sizeof(float) * 3 * max_batch));
+    TR_CUDA(c, cudaMallocHost((void**)&c->h_gemm_err, sizeof(int)));
     TR_CUDA(c, cudaMallocHost((void**)&c->op_has_pad_host, sizeof(int) * (max_operators ? max_operators : 1)));
     c->op_set.assign(max_operators, 0);
     // twiddle tables for the projection box and the template box
@@ -706,12 +706,16 @@ int tm_refine_score(tm_refine_ctx* c, int n, const float* euler, const int* part
             // jobs[0:n_jobs] and has_pad[0:n_jobs] (has_pad = jobs + max_batch)
             TR_CUDA(c, cudaMemcpyAsync(c->jobs, c->h_jobs, sizeof(int) * 2 * c->max_batch, cudaMemcpyHostToDevice, s));
             TR_CUDA(c, cudaMemcpyAsync(c->gjobs, c->h_gjobs, sizeof(tmr::GemmJob) * 3 * n_jobs, cudaMemcpyHostToDevice, s));
+            TR_CUDA(c, cudaMemsetAsync(c->gemm_err, 0, sizeof(int), s));
         }
         int rc = c->run(c, m, n_jobs);
         if (rc != TM_OK) return rc;
         TR_CUDA(c, cudaMemcpyAsync(c->h_out, c->out, sizeof(float) * 3 * m, cudaMemcpyDeviceToHost, s));
+        *c->h_gemm_err = 0;
+        if (n_jobs > 0) TR_CUDA(c, cudaMemcpyAsync(c->h_gemm_err, c->gemm_err, sizeof(int), cudaMemcpyDeviceToHost, s));
         rc = wait_refine(c, 120.0);
         if (rc != TM_OK) return rc;
+        if (*c->h_gemm_err) return rset_err(c, TM_ERR_TIMEOUT, "a tensor-core GEMM of the pixel-size change timed out");
         memcpy(out + 3 * (size_t)base, c->h_out, sizeof(float) * 3 * m);
     }
     return TM_OK;

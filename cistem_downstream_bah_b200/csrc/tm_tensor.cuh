@@ -70,7 +70,10 @@ struct PassCTc {
     static_assert(OFF_ROWS % 16 == 0, "operand regions 16-byte aligned");
     // bytes of one staged row block: R rows x XP FP16 complex values
     __host__ __device__ static size_t block_bytes(int XP) { return (size_t)XP * R * 4; }
-    static size_t smem_bytes(int XP, int bins) { return OFF_ROWS + 2 * block_bytes(XP) + 4 * (size_t)bins; }
+    static constexpr int HIST_COPIES = 16;           // copies of the shared histogram (hist_copies)
+    static size_t smem_bytes(int XP, int bins) {
+        return OFF_ROWS + 2 * block_bytes(XP) + 4 * (size_t)bins * hist_copies(bins, HIST_COPIES);
+    }
 };
 
 // The DFT matrices of the two stages as FP16 B operands, in the byte layout the
@@ -154,7 +157,9 @@ k_pass_c_tc(BatchArgs a, int Y, const uint4* __restrict__ dft) {
     for (int i = t; i < (PC::B1_BYTES + PC::B2_BYTES) / 16; i += PC::NT)
         reinterpret_cast<uint4*>(sB1)[i] = __ldg(dft + i);
     for (int i = t; i < R * PC::A2_BYTES / 16; i += PC::NT) reinterpret_cast<uint4*>(sA2)[i] = make_uint4(0, 0, 0, 0);
-    for (int b = t; b < a.hist_bins; b += PC::NT) shist[b] = 0u;
+    const int hcopies = hist_copies(a.hist_bins, PC::HIST_COPIES);
+    const int hcopy = t & (hcopies - 1);
+    for (int b = t; b < a.hist_bins * hcopies; b += PC::NT) shist[b] = 0u;
     tmptx::fence_proxy_async_smem();
     tmptx::tmem_fence_before_sync();
     __syncthreads();
@@ -369,7 +374,7 @@ k_pass_c_tc(BatchArgs a, int Y, const uint4* __restrict__ dft) {
             st[pi] = (ts - fs[pi]) - ys;
             fs[pi] = ts;
             const int bin = __float2int_rz((v - a.hist_min) * a.hist_inv_step);
-            if (bin >= 0 && bin < a.hist_bins) atomicAdd(&shist[bin], 1u);
+            if (bin >= 0 && bin < a.hist_bins) atomicAdd(&shist[bin * hcopies + hcopy], 1u);
         }
         tmptx::tmem_st16(tstate, st);
         // sweep 1: the sum of squares (columns 32-47) and its compensation (16-31)
@@ -451,7 +456,8 @@ k_pass_c_tc(BatchArgs a, int Y, const uint4* __restrict__ dft) {
     }
     __syncthreads();
     for (int b = t; b < a.hist_bins; b += PC::NT) {
-        const unsigned int cnt = shist[b];
+        unsigned int cnt = 0;
+        for (int k = 0; k < hcopies; k++) cnt += shist[b * hcopies + k];
         if (cnt) atomicAdd(a.hist + b, (unsigned long long)cnt);
     }
 }

@@ -207,6 +207,15 @@ TM_API int tm_last_timing(const tm_ctx *ctx, double *total_ms, double *pass_b_ms
 TM_API int tm_debug_stage_buffers(tm_ctx *ctx, const float *projection_filter, const float *euler_angle, float *slice,
                                   float *projection, float *normalisation, float *rows, float *columns);
 
+/* One product C = (A - s) B (+ C when accumulate) of the dense-operator GEMMs
+ * that the pixel-size change runs on the device (template volume and
+ * refine_template), on `device`: tensor = 1 the tensor-core form (split TF32,
+ * FP32 accumulation) the library uses, 0 the FP32 CUDA-core form.  Row-major
+ * host arrays A (M x K), B (K x N), C (M x N).  For kernel-level tests; it
+ * has no counterpart in the reference. */
+TM_API int tm_debug_gemm(int device, int M, int N, int K, const float *A, const float *B, float *C, float s,
+                         int accumulate, int tensor);
+
 /* Plane search that allocates no device memory, for callers that cannot call
  * cudaMalloc: code inside a host framework that owns every device allocation
  * through its own pool, and plugins that are only handed pre-allocated
