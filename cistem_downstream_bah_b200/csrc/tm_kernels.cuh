@@ -633,6 +633,262 @@ k_pass_b(BatchArgs a, int n_items) {
 }
 
 // --------------------------------------------------------------------------------------
+// Work items of the column passes: (column group, orientation).  A block owns
+// whole column groups, every orientation of a group in turn (its micrograph
+// values stay in TMEM), and the blocks take adjacent groups in rounds: block b
+// has groups b, b + nblk, b + 2 nblk, ...  All blocks then write rows of the
+// same orientation at about the same time, into adjacent 32-byte sectors of
+// each row, which the L2 merges into whole lines before writing them back.
+// (With each block on a contiguous run of items, the blocks wrote rows of
+// unrelated orientations one sector at a time, and the 4096 x 4096 column pass
+// took 2.3 times as long as with its stores going to L2-resident addresses.)
+// Groups left over after the whole rounds are split by orientation ranges over
+// the blocks that would otherwise idle.
+struct ColSchedule {
+    int nb, nblk, b, rounds, tail_g, o_lo, n;
+    __host__ __device__ ColSchedule(int ngroups, int nbatch, int blk, int nblocks) : nb(nbatch), nblk(nblocks), b(blk) {
+        rounds = ngroups / nblk;
+        const int rem = ngroups % nblk;
+        const int parts = rem ? min(nb, nblk / rem) : 1;
+        int o_hi = 0;
+        tail_g = -1;
+        o_lo = 0;
+        if (rem && b < rem * parts) {
+            const int p = b / rem;
+            tail_g = rounds * nblk + b % rem;
+            o_lo = p * nb / parts;
+            o_hi = (p + 1) * nb / parts;
+        }
+        n = rounds * nb + (o_hi - o_lo);
+    }
+    // most items a block gets
+    __host__ __device__ static int max_items(int ngroups, int nbatch, int nblocks) {
+        return (ngroups + nblocks - 1) / nblocks * nbatch;
+    }
+    __host__ __device__ void locate(int idx, int& g, int& o) const {
+        if (idx < rounds * nb) {
+            g = (idx / nb) * nblk + b;
+            o = idx % nb;
+        } else {
+            g = tail_g;
+            o = o_lo + idx - rounds * nb;
+        }
+    }
+};
+
+// --------------------------------------------------------------------------------------
+// k_pass_b_rg: the column pass of 4096-high micrographs with 256-row pruned
+// transforms (T = 256), arranged so that two of its three exchanges stay
+// inside a warp.  Write the column spectrum index k = s + 16 k1 + 256 k2 and
+// the output row m = m' + 256 M (s, k1, k2, M in 0..15, m' in 0..255).  Both
+// transforms split by the residue s = k mod 16:
+//   F[s + 16 k'] = sum_{n<256} (a[n] W4096^(-n s)) W256^(-n k')
+//   y[m' + 256 M] = sum_s (W4096^(m' s) G_s[m']) W16^(M s),
+//   G_s[m'] = sum_{k'} Z[s + 16 k'] W256^(m' k'),   Z = I' conj(F)
+// (W_N^e = exp(2 pi i e / N)).  A residue's 256 values live in the 16 lanes of
+// one half-warp from the forward 256-point transform through the multiply by
+// I' to G_s: each 256-point transform is 16 x 16 with one transpose through
+// the warp's own shared memory (__syncwarp only).  One block-wide exchange
+// then gathers the 16 residues of each output row m' for the last 16-point
+// DFT.  Per item (4 columns of one orientation) that is two block barriers
+// instead of the six of k_pass_b's Stockham stages.
+//
+// Roles: residue phases -- warp w holds residue s = w >> 1 of columns
+// 2 (w & 1) + (lane >> 4), lane q = lane & 15; final phase -- thread t holds
+// row m' = t >> 2 of column t & 3 (a warp stores 8 rows x 4 columns, whole
+// 32-byte row sectors).  The block buffer is blk[c][m'][s] (row stride 17,
+// column stride CS = 4 mod 16: conflict-free 8-byte accesses in every phase).
+// A warp's transposes use the block-buffer ranges that the same warp reads in
+// the final phase, so they need no barrier of their own: nobody else touches
+// those ranges between the warp's final read and the next block-wide write.
+struct PassBRg {
+    static constexpr int T = 256, Y = 4096, W = 4, NT = 1024;
+    static constexpr int RS = 17;                       // row stride of blk (float2)
+    static constexpr int CS = 256 * RS + 4;             // column stride, == 4 (mod 16)
+    static constexpr int APITCH = 260;                  // A staging: [c][row], 4 columns
+    static constexpr size_t EXCH = sizeof(float2) * W * CS;
+    static constexpr size_t ASZ = sizeof(float2) * W * APITCH;
+    static constexpr int ABUFS = 3;                     // rows of A prefetched two items ahead
+    static constexpr size_t TWB = sizeof(float2) * Y;   // W4096^m, m = 0..4095
+    static constexpr int MAX_ITEMS = 2048;              // a block's item list (group << 16 | orientation)
+    static constexpr size_t LIST = sizeof(int) * MAX_ITEMS;
+    static constexpr size_t SMEM = EXCH + ABUFS * ASZ + TWB + LIST + 64;
+    static constexpr uint32_t TMEM_COLS = 256;          // 8 warps per lane quadrant x 32 columns
+    static_assert(SMEM <= 232448, "pass B block exceeds shared memory");
+};
+
+__global__ void __launch_bounds__(PassBRg::NT, 1)
+k_pass_b_rg(BatchArgs a, int ngroups) {
+    using PB = PassBRg;
+    constexpr int T = PB::T, Y = PB::Y, RS = PB::RS, CS = PB::CS, AP = PB::APITCH;
+    extern __shared__ __align__(16) unsigned char smem_b[];
+    float2* const blk = reinterpret_cast<float2*>(smem_b);
+    float2* const abuf = reinterpret_cast<float2*>(smem_b + PB::EXCH);
+    float2* const tws = reinterpret_cast<float2*>(smem_b + PB::EXCH + PB::ABUFS * PB::ASZ);
+    int* const items = reinterpret_cast<int*>(smem_b + PB::EXCH + PB::ABUFS * PB::ASZ + PB::TWB);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem_b + PB::EXCH + PB::ABUFS * PB::ASZ + PB::TWB + PB::LIST);
+    const int tid = threadIdx.x;
+    // this block's items (the launcher checks that they fit the list)
+    int n_items;
+    {
+        const ColSchedule sch(ngroups, a.nb, blockIdx.x, gridDim.x);
+        n_items = sch.n;
+        for (int i = tid; i < sch.n; i += PB::NT) {
+            int g, o;
+            sch.locate(i, g, o);
+            items[i] = (g << 16) | o;
+        }
+    }
+    if (n_items == 0) return;
+    if ((tid >> 5) == 0) {
+        tmptx::tmem_alloc(tmem_slot, PB::TMEM_COLS);
+        tmptx::tmem_relinquish();
+    }
+    // the item's 256 rows of A, column-major into the staging buffer [c][row]
+    // (thread: row tid / 4, column tid % 4); items are (column group, orientation),
+    // orientation fastest
+    const float2* const Asrc = a.A + (size_t)(tid >> 2) * a.XP + (tid & 3);
+    const uint32_t adst = tmptx::smem_u32(abuf + (tid & 3) * AP + (tid >> 2));
+    auto issue_rows = [&](int grp, int oo, int buf) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(adst + buf * (uint32_t)(PB::ASZ)),
+                     "l"(Asrc + (size_t)oo * T * a.XP + grp * 4)
+                     : "memory");
+    };
+    // twiddle table in shared memory: tw(m) = W4096^(-m)
+    for (int m = tid; m < Y; m += PB::NT) tws[m] = __ldg(a.twy.tab + m);
+    auto tw = [tws](int m) { return tws[m & (Y - 1)]; };
+    __syncthreads();   // the item list
+    issue_rows(items[0] >> 16, items[0] & 0xffff, 0);
+    tmptx::cp_async_commit();
+    if (n_items > 1) issue_rows(items[1] >> 16, items[1] & 0xffff, 1);
+    tmptx::cp_async_commit();
+    tmptx::cp_async_wait<1>();
+    tmptx::tmem_fence_before_sync();
+    __syncthreads();
+    tmptx::tmem_fence_after_sync();
+    const uint32_t tmem = *tmem_slot + ((uint32_t)(32 * ((tid >> 5) & 3)) << 16) + (uint32_t)(32 * (tid >> 7));
+    int cur_group = -1;
+    int buf = 0;
+#pragma unroll 1
+    for (int it = 0; it < n_items; it++) {
+        const int group = items[it] >> 16, o = items[it] & 0xffff;
+        // residue phases: residue s = warp / 2, column c = 2 (warp % 2) + lane / 16, lane q = lane % 16
+        const int s = tid >> 6, q = tid & 15, c = (tid >> 4) & 3;
+        {
+            // rows of item it + 2 into the buffer that item it - 1 used
+            if (it + 2 < n_items) issue_rows(items[it + 2] >> 16, items[it + 2] & 0xffff, buf == 0 ? 2 : buf - 1);
+            tmptx::cp_async_commit();
+        }
+        if (group != cur_group) {
+            // this thread's 16 I' values, k = s + 16 q + 256 r, into its TMEM columns
+            const float2* Ig = a.Ip + (size_t)(s + 16 * q) * a.XP + group * 4 + c;
+#pragma unroll 1
+            for (int h = 0; h < 2; h++) {
+                float ib[16];
+#pragma unroll
+                for (int r = 0; r < 8; r++) {
+                    const float2 iv = __ldg(Ig + (size_t)(256 * (8 * h + r)) * a.XP);
+                    ib[2 * r] = iv.x;
+                    ib[2 * r + 1] = iv.y;
+                }
+                tmptx::tmem_st16(tmem + 16 * h, ib);
+            }
+            tmptx::tmem_wait_st();
+            cur_group = group;
+        }
+        // transposes: row rho (0..15) of this half-warp's 16 x 16 block sits in the
+        // final-phase ranges of this warp (columns c % 2 and c % 2 + 2, 8 rows of m' each)
+        float2* const scr = blk + (c & 1) * CS + 136 * (tid >> 5);
+#define TM_RG_ROW(rho) (scr + ((rho) >> 3) * (2 * CS) + ((rho) & 7) * RS)
+        float2 v[16];
+        // forward: b[n] = a[n] W4096^(-n s) for n = q + 16 r, 16-point DFT over r (-> k1)
+        {
+            const float2* ac = abuf + buf * (PB::W * AP) + c * AP + q;
+            const float2 w1 = tw(16 * s);
+            float2 w = tw(s * q);
+#pragma unroll
+            for (int r = 0; r < 16; r++) {
+                v[r] = cmul(ac[16 * r], w);
+                w = cmul(w, w1);
+            }
+        }
+        tmfft::dft16<-1>(v);
+        tmfft::apply_twiddles<16>(v, tw(16 * q));                       // W256^(-q k1)
+        __syncwarp();   // the warp's final-phase reads of the previous item are done
+#pragma unroll
+        for (int r = 0; r < 16; r++) TM_RG_ROW(q)[r] = v[r];           // row n1 = q, column k1 = r
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < 16; r++) v[r] = TM_RG_ROW(r)[q];           // thread k1 = q holds n1 = r
+        __syncwarp();
+        tmfft::dft16<-1>(v);                                           // -> k2: F[s + 16 q + 256 r]
+        // Z = I' conj(F)
+        {
+            float iv[16];
+            tmptx::tmem_ld16(tmem, iv);
+            tmptx::tmem_wait_ld16(iv);
+#pragma unroll
+            for (int r = 0; r < 8; r++) v[r] = cmul_conj(make_float2(iv[2 * r], iv[2 * r + 1]), v[r]);
+            tmptx::tmem_ld16(tmem + 16, iv);
+            tmptx::tmem_wait_ld16(iv);
+#pragma unroll
+            for (int r = 0; r < 8; r++) v[8 + r] = cmul_conj(make_float2(iv[2 * r], iv[2 * r + 1]), v[8 + r]);
+        }
+        // inverse, residue part: 16-point DFT over k2 (-> m1), W256^(m1 q), transpose,
+        // 16-point DFT over k1 (-> m2), then W4096^(s (m1 + 16 m2))
+        tmfft::dft16<+1>(v);
+        tmfft::apply_twiddles<16>(v, tmfft::conjf2(tw(16 * q)));
+#pragma unroll
+        for (int r = 0; r < 16; r++) TM_RG_ROW(q)[r] = v[r];           // row k1 = q, column m1 = r
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < 16; r++) v[r] = TM_RG_ROW(r)[q];           // thread m1 = q holds k1 = r
+#undef TM_RG_ROW
+        tmfft::dft16<+1>(v);                                           // -> m2
+        {
+            const float2 w1 = tmfft::conjf2(tw(16 * s));
+            float2 w = tmfft::conjf2(tw(s * q));
+#pragma unroll
+            for (int r = 0; r < 16; r++) {
+                v[r] = cmul(v[r], w);
+                w = cmul(w, w1);
+            }
+        }
+        // every warp is done with its transposes (which overlap other warps' final ranges)
+        __syncthreads();
+        {
+            float2* bw = blk + c * CS + q * RS + s;
+#pragma unroll
+            for (int r = 0; r < 16; r++) bw[16 * RS * r] = v[r];         // G_s[m' = q + 16 r]
+        }
+        tmptx::cp_async_wait<1>();   // the next item's rows (issued at the top of the previous item)
+        __syncthreads();
+        // final phase: thread holds row m' = tid / 4 of column tid % 4
+        {
+            const float2* br = blk + (tid & 3) * CS + (tid >> 2) * RS;
+#pragma unroll
+            for (int r = 0; r < 16; r++) v[r] = br[r];                  // residues s = r of row m'
+        }
+        tmfft::dft16<+1>(v);                                           // -> M
+        {
+            float2* Co = a.C + ((size_t)o * Y + (tid >> 2)) * a.XP + group * 4 + (tid & 3);
+            const size_t rstep = (size_t)256 * a.XP;
+#pragma unroll
+            for (int r = 0; r < 16; r++) {
+                *Co = v[r];
+                Co += rstep;
+            }
+        }
+        buf = buf == 2 ? 0 : buf + 1;
+    }
+    tmptx::cp_async_wait<0>();
+    tmptx::tmem_fence_before_sync();
+    __syncthreads();
+    tmptx::tmem_fence_after_sync();
+    if ((tid >> 5) == 0) tmptx::tmem_dealloc(*tmem_slot, PB::TMEM_COLS);
+}
+
+// --------------------------------------------------------------------------------------
 // k_pass_c: one block per row y; X/16 threads each own 16 pixels
 // (x = 2*(t + P*r) + h); loops over the batch keeping the per-pixel state in
 // registers.  The per-pixel sum and sum of squares are compensated (Kahan)
@@ -921,9 +1177,15 @@ struct Launch {
     using SC = SliceCol<T>;
     using RC = RowC2R<T>;
     static constexpr int pass_b_width = PB::WG;   // row pitch alignment (columns)
+    // 4096-high micrographs with 256-row pruned transforms: the residue-grouped column pass
+    static constexpr bool RG = (T == 256 && Y == 4096);
     static cudaError_t configure(int XP, int bins) {
         cudaError_t e = cudaFuncSetAttribute(k_pass_b<T, Y>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB::SMEM);
         if (e != cudaSuccess) return e;
+        if constexpr (RG) {
+            e = cudaFuncSetAttribute(k_pass_b_rg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PassBRg::SMEM);
+            if (e != cudaSuccess) return e;
+        }
         return cudaFuncSetAttribute(k_pass_c<X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PC::smem_bytes(XP, bins));
     }
     // slice, projection, normalisation and row transforms
@@ -935,7 +1197,11 @@ struct Launch {
     }
     static void pass_b(BatchArgs& a, cudaStream_t s, int nsm) {
         const int n_items = (a.XP / PB::WG) * a.nb;
-        k_pass_b<T, Y><<<n_items < nsm ? n_items : nsm, PB::NT, PB::SMEM, s>>>(a, n_items);
+        const int ngroups = a.XP / PB::WG;
+        if (RG && ColSchedule::max_items(ngroups, a.nb, nsm) <= PassBRg::MAX_ITEMS)
+            k_pass_b_rg<<<nsm, PassBRg::NT, PassBRg::SMEM, s>>>(a, ngroups);
+        else
+            k_pass_b<T, Y><<<n_items < nsm ? n_items : nsm, PB::NT, PB::SMEM, s>>>(a, n_items);
     }
     static void pass_c(BatchArgs& a, cudaStream_t s) {
         k_pass_c<X><<<Y, X / 16, PC::smem_bytes(a.XP, a.hist_bins), s>>>(a, Y);
