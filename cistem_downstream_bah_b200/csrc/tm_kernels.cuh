@@ -367,6 +367,65 @@ k_pass_a(BatchArgs a) {
 }
 
 // --------------------------------------------------------------------------------------
+// Work items of the column passes: (column group, orientation).  A block owns
+// whole column groups, every orientation of a group in turn (its micrograph
+// values stay in TMEM), and the blocks take adjacent groups in rounds: block b
+// has groups b, b + nblk, b + 2 nblk, ...  All blocks then write rows of the
+// same orientation at about the same time, into adjacent 32-byte sectors of
+// each row, which the L2 merges into whole lines before writing them back.
+// (With each block on a contiguous run of items, the blocks wrote rows of
+// unrelated orientations one sector at a time, and the 4096 x 4096 column pass
+// took 2.3 times as long as with its stores going to L2-resident addresses.)
+// Groups left over after the whole rounds are split by orientation ranges over
+// the blocks that would otherwise idle.
+struct ColSchedule {
+    int nb, nblk, b, rounds, tail_g, o_lo, n;
+    __host__ __device__ ColSchedule(int ngroups, int nbatch, int blk, int nblocks) : nb(nbatch), nblk(nblocks), b(blk) {
+        rounds = ngroups / nblk;
+        const int rem = ngroups % nblk;
+        const int parts = rem ? min(nb, nblk / rem) : 1;
+        int o_hi = 0;
+        tail_g = -1;
+        o_lo = 0;
+        if (rem && b < rem * parts) {
+            const int p = b / rem;
+            tail_g = rounds * nblk + b % rem;
+            o_lo = p * nb / parts;
+            o_hi = (p + 1) * nb / parts;
+        }
+        n = rounds * nb + (o_hi - o_lo);
+    }
+    // most items a block gets
+    __host__ __device__ static int max_items(int ngroups, int nbatch, int nblocks) {
+        return (ngroups + nblocks - 1) / nblocks * nbatch;
+    }
+    // (group, orientation) of the block's idx-th item.  k_pass_b keeps the schedule
+    // in shared memory (its fields cost no registers across the item loop);
+    // k_pass_b_rg expands it into a list of items there.
+    __host__ __device__ void locate(int idx, int& g, int& o) const {
+        if (idx < rounds * nb) {
+            g = (idx / nb) * nblk + b;
+            o = idx % nb;
+        } else {
+            g = tail_g;
+            o = o_lo + idx - rounds * nb;
+        }
+    }
+    // the same from the block's shared-memory copy, read afresh on every call
+    __device__ static void locate(const volatile ColSchedule* s, int idx, int& g, int& o) {
+        const int nb = s->nb, rounds = s->rounds;
+        if (idx < rounds * nb) {
+            g = (idx / nb) * s->nblk + s->b;
+            o = idx % nb;
+        } else {
+            g = s->tail_g;
+            o = s->o_lo + idx - rounds * nb;
+        }
+    }
+};
+static_assert(sizeof(ColSchedule) <= 48, "the schedule sits in the last 48 bytes of a column pass's shared memory");
+
+// --------------------------------------------------------------------------------------
 // k_pass_b: persistent; block = W columns x P threads (thread = c + W*j,
 // P = Y/V); work item = (group of G column chunks, orientation), orientation
 // fastest.  With 2-column chunks (tall micrographs, where 4 columns would need
@@ -451,7 +510,7 @@ __device__ __forceinline__ void tmem_put_values(uint32_t taddr, const float* f) 
 // block of RB rows with one bulk copy.
 template <int T, int Y, int RB = 0>
 __global__ void __launch_bounds__(PassB<T, Y>::NT, 1)
-k_pass_b(BatchArgs a, int n_items) {
+k_pass_b(BatchArgs a, int ngroups) {
     using PB = PassB<T, Y>;
     constexpr int W = PB::W, MY = PB::MY, PT = PB::PT, NT = PB::NT, V = PB::V, P = PB::P, L = PB::L;
     const int XP = a.XP;
@@ -459,6 +518,7 @@ k_pass_b(BatchArgs a, int n_items) {
     float2* exch = reinterpret_cast<float2*>(smem_b);
     float2* abuf = reinterpret_cast<float2*>(smem_b + PB::EXCH);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem_b + PB::EXCH + PB::ABUFS * PB::ASZ);
+    volatile ColSchedule* sch = reinterpret_cast<volatile ColSchedule*>(smem_b + PB::EXCH + PB::ABUFS * PB::ASZ + 16);
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const bool tmem_warp = warp < PB::FULL_WARPS;   // uniform per warp
@@ -473,10 +533,14 @@ k_pass_b(BatchArgs a, int n_items) {
         if constexpr (NH == 1) __syncthreads();
         else asm volatile("bar.sync %0, %1;" ::"r"(1 + h), "n"(NTH) : "memory");
     };
-    const int per = (n_items + gridDim.x - 1) / gridDim.x;
-    const int it0 = blockIdx.x * per;
-    const int it1 = min(n_items, it0 + per);
-    if (it0 >= it1) return;
+    if (tid == 0) {
+        const ColSchedule cs(ngroups, a.nb, blockIdx.x, gridDim.x);
+        sch->nb = cs.nb; sch->nblk = cs.nblk; sch->b = cs.b; sch->rounds = cs.rounds;
+        sch->tail_g = cs.tail_g; sch->o_lo = cs.o_lo; sch->n = cs.n;
+    }
+    __syncthreads();
+    const int n_items = sch->n;
+    if (n_items == 0) return;
     if (warp == 0) {
         tmptx::tmem_alloc(tmem_slot, PB::TMEM_COLS);
         tmptx::tmem_relinquish();
@@ -489,7 +553,8 @@ k_pass_b(BatchArgs a, int n_items) {
     // reads) only its own columns
     constexpr int WGH = WG / NH;   // the item's columns per half
     auto issue_rows = [&](int it, float2* dst) {
-        const int grp = it / a.nb, oo = it % a.nb;
+        int grp, oo;
+        ColSchedule::locate(sch, it, grp, oo);
         const float2* src = a.A + (size_t)oo * T * XP + grp * WG + h * WGH;
         for (int e = loc; e < T * WGH; e += NTH) {
             const int row = e / WGH, cc = e % WGH;
@@ -497,15 +562,16 @@ k_pass_b(BatchArgs a, int n_items) {
         }
     };
     if (PB::ABUFS == 2) {
-        issue_rows(it0, abuf);
+        issue_rows(0, abuf);
         tmptx::cp_async_commit();
     }
     int cur_group = -1;
-    for (int it = it0; it < it1; it++) {
-        const int kk = it - it0;
+    for (int it = 0; it < n_items; it++) {
+        const int kk = it;
         const float2* acur = abuf + (PB::ABUFS == 2 ? (kk & 1) : 0) * (T * WG);
         float2* anext = abuf + (PB::ABUFS == 2 ? ((kk + 1) & 1) : 0) * (T * WG);
-        const int group = it / a.nb, o = it % a.nb;
+        int group, o;
+        ColSchedule::locate(sch, it, group, o);
         const int kx0 = group * WG;
         // twiddles of the pruned forward, W_Y^(s * (tp + PT*r)) = w0 * w1^r, loaded early
         // (with 32 values, from the table again every 8 values)
@@ -518,7 +584,7 @@ k_pass_b(BatchArgs a, int n_items) {
         // (Each half copies and reads only its own columns, so its own barrier suffices.)
         if (PB::ABUFS == 1) sync();
         if (PB::ABUFS == 2) {
-            if (it + 1 < it1) issue_rows(it + 1, anext);
+            if (it + 1 < n_items) issue_rows(it + 1, anext);
             tmptx::cp_async_commit();
             tmptx::cp_async_wait<1>();
         } else {
@@ -631,50 +697,6 @@ k_pass_b(BatchArgs a, int n_items) {
     tmptx::tmem_fence_after_sync();
     if (warp == 0) tmptx::tmem_dealloc(*tmem_slot, PB::TMEM_COLS);
 }
-
-// --------------------------------------------------------------------------------------
-// Work items of the column passes: (column group, orientation).  A block owns
-// whole column groups, every orientation of a group in turn (its micrograph
-// values stay in TMEM), and the blocks take adjacent groups in rounds: block b
-// has groups b, b + nblk, b + 2 nblk, ...  All blocks then write rows of the
-// same orientation at about the same time, into adjacent 32-byte sectors of
-// each row, which the L2 merges into whole lines before writing them back.
-// (With each block on a contiguous run of items, the blocks wrote rows of
-// unrelated orientations one sector at a time, and the 4096 x 4096 column pass
-// took 2.3 times as long as with its stores going to L2-resident addresses.)
-// Groups left over after the whole rounds are split by orientation ranges over
-// the blocks that would otherwise idle.
-struct ColSchedule {
-    int nb, nblk, b, rounds, tail_g, o_lo, n;
-    __host__ __device__ ColSchedule(int ngroups, int nbatch, int blk, int nblocks) : nb(nbatch), nblk(nblocks), b(blk) {
-        rounds = ngroups / nblk;
-        const int rem = ngroups % nblk;
-        const int parts = rem ? min(nb, nblk / rem) : 1;
-        int o_hi = 0;
-        tail_g = -1;
-        o_lo = 0;
-        if (rem && b < rem * parts) {
-            const int p = b / rem;
-            tail_g = rounds * nblk + b % rem;
-            o_lo = p * nb / parts;
-            o_hi = (p + 1) * nb / parts;
-        }
-        n = rounds * nb + (o_hi - o_lo);
-    }
-    // most items a block gets
-    __host__ __device__ static int max_items(int ngroups, int nbatch, int nblocks) {
-        return (ngroups + nblocks - 1) / nblocks * nbatch;
-    }
-    __host__ __device__ void locate(int idx, int& g, int& o) const {
-        if (idx < rounds * nb) {
-            g = (idx / nb) * nblk + b;
-            o = idx % nb;
-        } else {
-            g = tail_g;
-            o = o_lo + idx - rounds * nb;
-        }
-    }
-};
 
 // --------------------------------------------------------------------------------------
 // k_pass_b_rg: the column pass of 4096-high micrographs with 256-row pruned
@@ -1196,12 +1218,11 @@ struct Launch {
         k_pass_a<T, X><<<dim3(T, a.nb), X / 16, 0, s>>>(a);
     }
     static void pass_b(BatchArgs& a, cudaStream_t s, int nsm) {
-        const int n_items = (a.XP / PB::WG) * a.nb;
         const int ngroups = a.XP / PB::WG;
         if (RG && ColSchedule::max_items(ngroups, a.nb, nsm) <= PassBRg::MAX_ITEMS)
             k_pass_b_rg<<<nsm, PassBRg::NT, PassBRg::SMEM, s>>>(a, ngroups);
         else
-            k_pass_b<T, Y><<<n_items < nsm ? n_items : nsm, PB::NT, PB::SMEM, s>>>(a, n_items);
+            k_pass_b<T, Y><<<nsm, PB::NT, PB::SMEM, s>>>(a, ngroups);
     }
     static void pass_c(BatchArgs& a, cudaStream_t s) {
         k_pass_c<X><<<Y, X / 16, PC::smem_bytes(a.XP, a.hist_bins), s>>>(a, Y);
@@ -1241,13 +1262,10 @@ struct LaunchTc {
     }
     static void pass_b(BatchArgs& a, cudaStream_t s, int nsm, const uint4* tabs) {
         if constexpr (COL_TC) {
-            // items = (group of 4 columns, orientation); two CTAs (the group's two column pairs) per item range
-            const int n_items = (a.XP / 4) * a.nb;
-            k_pass_b_tc<T, R><<<2 * (n_items < nsm ? n_items : nsm), PBT::NT, PBT::SMEM, s>>>(a, n_items,
-                                                                                          tabs + rows_tab_bytes / 16);
+            // items = (group of 4 columns, orientation); two blocks per SM
+            k_pass_b_tc<T, R><<<2 * nsm, PBT::NT, PBT::SMEM, s>>>(a, a.XP / 4, tabs + rows_tab_bytes / 16);
         } else {
-            const int n_items = (a.XP / PB::WG) * a.nb;
-            k_pass_b<T, Y, R><<<n_items < nsm ? n_items : nsm, PB::NT, PB::SMEM, s>>>(a, n_items);
+            k_pass_b<T, Y, R><<<nsm, PB::NT, PB::SMEM, s>>>(a, a.XP / PB::WG);
         }
     }
     static void pass_c(BatchArgs& a, cudaStream_t s, const uint4* dft) {

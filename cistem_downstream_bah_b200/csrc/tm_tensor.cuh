@@ -564,7 +564,7 @@ __device__ __forceinline__ float2 h2f(uint32_t bits) {
 
 template <int T, int RB>
 __global__ void __launch_bounds__(512, 1)
-k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
+k_pass_b_tc(BatchArgs a, int ngroups, const uint4* __restrict__ tabs) {
     using PB = PassBTc<T, RB>;
     constexpr int Y = PB::Y;
     constexpr uint32_t kWaitLimit = 1u << 24;
@@ -580,10 +580,10 @@ k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int q = warp & 3, sub = warp >> 2;
     const int m = 32 * q + lane;            // TMEM lane of this thread
-    const int per = (n_items + gridDim.x - 1) / gridDim.x;
-    const int it0 = blockIdx.x * per;
-    const int it1 = min(n_items, it0 + per);
-    if (it0 >= it1) return;
+    // the items of this block, as in k_pass_b (adjacent column groups per round)
+    const ColSchedule sch(ngroups, a.nb, blockIdx.x, gridDim.x);
+    const int it1 = sch.n;
+    if (it1 == 0) return;
     if (t == 0) {
         tmptx::mbar_init(&mbar[0], 1);
         tmptx::mbar_init(&mbar[1], 1);
@@ -651,7 +651,8 @@ k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
     constexpr int NPF = (4 * T + PB::NT - 1) / PB::NT;
     float2 pf[NPF];
     auto prefetch = [&](int itn) {
-        const int gn = itn / a.nb, on = itn % a.nb;
+        int gn, on;
+        sch.locate(itn, gn, on);
         const float2* Ao = a.A + (size_t)on * T * XP + gn * 4;
 #pragma unroll
         for (int q = 0; q < NPF; q++) {
@@ -659,9 +660,10 @@ k_pass_b_tc(BatchArgs a, int n_items, const uint4* __restrict__ tabs) {
             pf[q] = i < 4 * T ? __ldg(Ao + (size_t)(i >> 2) * XP + (i & 3)) : make_float2(0.f, 0.f);
         }
     };
-    prefetch(it0);
-    for (int it = it0; it < it1; it++) {
-        const int group = it / a.nb, o = it % a.nb;
+    prefetch(0);
+    for (int it = 0; it < it1; it++) {
+        int group, o;
+        sch.locate(it, group, o);
         const int kx0 = group * 4;
         // every thread is done with the previous item's staging tile and I'
         if (__syncthreads_or(timed_out)) break;

@@ -149,3 +149,35 @@ def test_shared_memory_budget():
     twiddles = 8 * Y
     assert exch + 3 * staging + twiddles + 64 <= 232448
     assert CS % 16 == 4 and RS % 2 == 1
+
+
+def _col_schedule(ngroups, nb, b, nblk):
+    """ColSchedule of tm_kernels.cuh: a block's (group, orientation) items in order."""
+    rounds, rem = divmod(ngroups, nblk)
+    parts = min(nb, nblk // rem) if rem else 1
+    items = [(r * nblk + b, o) for r in range(rounds) for o in range(nb)]
+    if rem and b < rem * parts:
+        p = b // rem
+        g = rounds * nblk + b % rem
+        items += [(g, o) for o in range(p * nb // parts, (p + 1) * nb // parts)]
+    return items
+
+
+def test_column_schedule_covers_every_item_once():
+    """Every (column group, orientation) item goes to exactly one block, blocks
+    of one round hold adjacent groups at the same orientation step, and no block
+    has more than a round's work beyond the average."""
+    for ngroups, nb, nblk in [(513, 128, 148), (513, 32, 148), (513, 128, 296), (129, 256, 148), (5, 16, 148),
+                              (1025, 64, 148), (17, 1, 148)]:
+        lists = [_col_schedule(ngroups, nb, b, nblk) for b in range(nblk)]
+        seen = [it for lst in lists for it in lst]
+        assert len(seen) == len(set(seen)) == ngroups * nb
+        longest = max(len(lst) for lst in lists)
+        assert longest <= -(-ngroups // nblk) * nb
+        # within the whole rounds, step i of every block is the same orientation on adjacent groups
+        rounds = ngroups // nblk
+        for i in range(0, rounds * nb, max(1, nb // 3)):
+            step = sorted(lists[b][i] for b in range(nblk))
+            assert {o for _, o in step} == {i % nb}
+            gs = [g for g, _ in step]
+            assert gs == list(range(gs[0], gs[0] + nblk))
