@@ -421,4 +421,64 @@ __device__ __forceinline__ void fft(float2 (&v)[R], int t, float2* buf, const Tw
     });
 }
 
+// The same transform with the twiddle multipliers of every stage supplied by
+// the caller instead of a table lookup and a power tree:
+// src.template issue<s>() starts fetching stage s's multipliers and is called
+// before the stage's barrier, so that the fetch overlaps the barrier and the
+// shared-memory loads; src.template get<s>(u, p) then fills p[1 .. RS-1] with
+// w^1 .. w^(RS-1) of the thread's butterfly u (w as in fft above, DIR applied).
+// Used where the multipliers are per-thread constants held in tensor memory.
+template <int L, int R, int DIR, bool FIRST_SYNC = true, class Src, class Sync>
+__device__ __forceinline__ void fft_pre(float2 (&v)[R], int t, float2* buf, Src& src, Sync sync) {
+    using PL = Plan<L, R>;
+    constexpr int P = PL::P;
+    sfor<PL::stages>([&](auto sc) {
+        constexpr int s = decltype(sc)::value;
+        constexpr int RS = PL::radix(s);
+        constexpr int Ns = PL::ns(s);
+        constexpr bool last = (s == PL::stages - 1);
+        if constexpr (s > 0) {
+            src.template issue<s>();
+            sync();
+            if constexpr (P % 16 == 0 || 16 % P == 0) {
+                const float2* rb = buf + rd_base<P>(t);
+#pragma unroll
+                for (int r = 0; r < R; r++) v[r] = rb[rd_off<P>(r)];
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; r++) v[r] = buf[pad16(t + P * r)];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < R / RS; u++) {
+            const int b = t + P * u;
+            float2 e[RS];
+#pragma unroll
+            for (int r = 0; r < RS; r++) e[r] = v[u + r * (R / RS)];
+            if constexpr (s > 0) {
+                float2 pw[RS];
+                src.template get<s>(u, pw);
+#pragma unroll
+                for (int r = 1; r < RS; r++) e[r] = cmul(e[r], pw[r]);
+            }
+            dft<RS, DIR>(e);
+            if constexpr (last) {
+#pragma unroll
+                for (int r = 0; r < RS; r++) v[u + r * (R / RS)] = e[r];
+            } else {
+                if (u == 0 && (FIRST_SYNC || s > 0)) sync();
+                if constexpr (RS == R && ((Ns == 1 && 16 % R == 0) || Ns % 16 == 0)) {
+                    float2* wb = buf + wr_base<R>(b, Ns);
+#pragma unroll
+                    for (int r = 0; r < RS; r++) wb[wr_off(r, Ns)] = e[r];
+                } else {
+                    const int idxD = (b / Ns) * Ns * RS + (b % Ns);
+#pragma unroll
+                    for (int r = 0; r < RS; r++) buf[pad16(idxD + r * Ns)] = e[r];
+                }
+            }
+        }
+    });
+}
+
 }  // namespace tmfft

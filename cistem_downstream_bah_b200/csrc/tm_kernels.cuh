@@ -936,13 +936,60 @@ struct PassC {
     static constexpr int P = H / R;                 // X/16 threads
     static constexpr int RSF = tmfft::padded_len(H);
     static constexpr bool COMP_IN_TMEM = X >= 4096 && P % 32 == 0;
-    static constexpr uint32_t TMEM_COLS = 64 * ((P / 32 + 3) / 4);   // warps of a lane quadrant side by side
+    // with the compensation terms in TMEM, a thread also keeps its twiddle
+    // multipliers there (the c2r packing's 8 and the transform's stages 1-3):
+    // 128 columns per warp, columns 0-47 sums, 48-63 packing, 64 + 16 (s - 1) stage s
+    static constexpr int WCOLS = COMP_IN_TMEM ? 128 : 64;
+    static constexpr uint32_t TMEM_COLS = WCOLS * ((P / 32 + 3) / 4);   // warps of a lane quadrant side by side
     // one histogram copy: measured at X = 4096, 16 lane-striped copies (32 KB
     // more shared memory per block, less L1) made this pass 5 % slower
     static constexpr int HIST_COPIES = 1;
     // dynamic shared memory for a row pitch XP and `bins` histogram bins
     static size_t smem_bytes(int XP, int bins) {
         return 128 + sizeof(float2) * (2 * (size_t)XP + RSF) + 4 * (size_t)bins * hist_copies(bins, HIST_COPIES);
+    }
+};
+
+// Stage multipliers of pass C's H-point inverse transform (8 values per thread),
+// parked in the thread's TMEM columns 64 + 16 (s - 1) for stage s: the R/RS
+// butterflies' RS - 1 powers each, as float pairs (tmfft::fft_pre's source).
+template <int H>
+struct PassCStageTw {
+    using PL = tmfft::Plan<H, 8>;
+    static_assert(PL::stages <= 4, "three twiddled stages fit columns 64-111");
+    uint32_t col64;
+    float tb[16];
+    template <int s>
+    __device__ __forceinline__ void issue() { tmptx::tmem_ld16(col64 + 16 * (s - 1), tb); }
+    template <int s>
+    __device__ __forceinline__ void get(int u, float2* p) {
+        constexpr int RS = PL::radix(s);
+        if (u == 0) tmptx::tmem_wait_ld16(tb);
+#pragma unroll
+        for (int r = 1; r < RS; r++) p[r] = make_float2(tb[2 * (u * (RS - 1) + r - 1)], tb[2 * (u * (RS - 1) + r - 1) + 1]);
+    }
+    // the multipliers of thread t, from the twiddle table, into its columns
+    __device__ static void fill(uint32_t col64, int t, const tmfft::Twiddles& tw) {
+        tmfft::sfor<PL::stages>([&](auto sc) {
+            constexpr int s = decltype(sc)::value;
+            if constexpr (s > 0) {
+                constexpr int RS = PL::radix(s), Ns = PL::ns(s), R = 8, P = PL::P;
+                float g[16];
+#pragma unroll
+                for (int i = 0; i < 16; i++) g[i] = 0.f;
+#pragma unroll
+                for (int u = 0; u < R / RS; u++) {
+                    const int jm = (t + P * u) % Ns;
+#pragma unroll
+                    for (int r = 1; r < RS; r++) {
+                        const float2 w = tw.template w<+1>(jm * (H / (Ns * RS)) * r, H);
+                        g[2 * (u * (RS - 1) + r - 1)] = w.x;
+                        g[2 * (u * (RS - 1) + r - 1) + 1] = w.y;
+                    }
+                }
+                tmptx::tmem_st16(col64 + 16 * (s - 1), g);
+            }
+        });
     }
 };
 
@@ -984,8 +1031,8 @@ k_pass_c(BatchArgs a, int Y) {
     if constexpr (kTm) tmptx::tmem_fence_before_sync();
     __syncthreads();
     if constexpr (kTm) tmptx::tmem_fence_after_sync();
-    // this thread's 64 TMEM columns (lane quadrant warp % 4)
-    const uint32_t tcomp = kTm ? *tmem_slot + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(64 * (warp >> 2)) : 0u;
+    // this thread's TMEM columns (lane quadrant warp % 4)
+    const uint32_t tcomp = kTm ? *tmem_slot + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(PC::WCOLS * (warp >> 2)) : 0u;
     if (t == 0 && a.nb > 0) {
         tmptx::mbar_arrive_expect_tx(&mbar[0], row_bytes);
         tmptx::bulk_g2s(rows, a.C + (size_t)y * XP, row_bytes, &mbar[0]);
@@ -1017,6 +1064,15 @@ k_pass_c(BatchArgs a, int Y) {
         tmptx::tmem_st16(tcomp, z);
         tmptx::tmem_st16(tcomp + 16, z);
         tmptx::tmem_st16(tcomp + 32, z);
+        // the packing's multipliers W_X^k, k = t + P r, and the transform's stage multipliers
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const float2 w = a.tw.template w<+1>(t + P * r, X);
+            z[2 * r] = w.x;
+            z[2 * r + 1] = w.y;
+        }
+        tmptx::tmem_st16(tcomp + 48, z);
+        PassCStageTw<H>::fill(tcomp + 64, t, a.tw);
         tmptx::tmem_wait_st();
     } else {
 #pragma unroll
@@ -1025,6 +1081,8 @@ k_pass_c(BatchArgs a, int Y) {
         for (int i = 0; i < (kTm ? 1 : 16); i++) fq_regs[i] = 0.f;
     }
     auto sync = [] __device__() { __syncthreads(); };
+    // histogram bin int((v - min) / step) as one multiply-add: (v - min) / step = v / step + hoff
+    const float hoff = -a.hist_min * a.hist_inv_step;
     // Copy o goes to buffer o & 1 and completes phase o >> 1 of that buffer's
     // mbarrier.  After a wait runs out the block stops issuing copies and, before
     // it exits, waits for the copies still in flight at the parity of the phase
@@ -1043,10 +1101,13 @@ k_pass_c(BatchArgs a, int Y) {
             tmptx::mbar_arrive_expect_tx(&mbar[buf ^ 1], row_bytes);
             tmptx::bulk_g2s(rows + (buf ^ 1) * XP, a.C + ((size_t)(o + 1) * Y + y) * XP, row_bytes, &mbar[buf ^ 1]);
         }
+        float pk[kTm ? 16 : 1];   // the packing's multipliers, from TMEM
+        if constexpr (kTm) tmptx::tmem_ld16(tcomp + 48, pk);
         if (!tmptx::mbar_wait_bounded(&mbar[buf], (o >> 1) & 1, kWaitLimit)) {
             timed_out = true;
             atomicExch(a.err, 1);
         }
+        if constexpr (kTm) tmptx::tmem_wait_ld16(pk);
         const float2* rb = rows + buf * XP;
         float2 v[8];
 #pragma unroll
@@ -1057,11 +1118,16 @@ k_pass_c(BatchArgs a, int Y) {
             if (k == 0) { hk.y = 0.f; hm.y = 0.f; }
             const float2 e = make_float2(hk.x + hm.x, hk.y - hm.y);
             const float2 d = make_float2(hk.x - hm.x, hk.y + hm.y);
-            const float2 od = cmul(d, a.tw.template w<+1>(k, X));
+            const float2 od = cmul(d, kTm ? make_float2(pk[2 * r], pk[2 * r + 1]) : a.tw.template w<+1>(k, X));
             v[r] = make_float2(e.x - od.y, e.y + od.x);
         }
         // the barrier at the top of the iteration follows the last reads of fbuf
-        tmfft::fft<H, 8, +1, false>(v, t, fbuf, a.tw, sync);
+        if constexpr (kTm) {
+            PassCStageTw<H> stw{tcomp + 64, {}};
+            tmfft::fft_pre<H, 8, +1, false>(v, t, fbuf, stw, sync);
+        } else {
+            tmfft::fft<H, 8, +1, false>(v, t, fbuf, a.tw, sync);
+        }
         const int g = (int)(a.gidx0 + o);
         // epilogue in two sweeps over the 16 values, so that only one sum's 16
         // compensation terms are live at a time: (1) MIP / argmax, histogram and
@@ -1092,8 +1158,8 @@ k_pass_c(BatchArgs a, int Y) {
                         const float ts = fs[pi] + ys;
                         comp[pi] = (ts - fs[pi]) - ys;
                         fs[pi] = ts;
-                        const int bin = __float2int_rz((val - a.hist_min) * a.hist_inv_step);
-                        if (bin >= 0 && bin < a.hist_bins) atomicAdd(&shist[bin * hcopies + hcopy], 1u);
+                        const int bin = __float2int_rz(fmaf(val, a.hist_inv_step, hoff));
+                        if ((unsigned)bin < (unsigned)a.hist_bins) atomicAdd(&shist[bin * hcopies + hcopy], 1u);
                     } else {
                         const float yq = fmaf(val, val, -comp[pi]);
                         const float tq = fq[pi] + yq;
