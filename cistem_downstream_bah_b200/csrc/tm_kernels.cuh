@@ -731,11 +731,13 @@ struct PassBRg {
     static constexpr size_t EXCH = sizeof(float2) * W * CS;
     static constexpr size_t ASZ = sizeof(float2) * W * APITCH;
     static constexpr int ABUFS = 3;                     // rows of A prefetched two items ahead
-    static constexpr size_t TWB = sizeof(float2) * Y;   // W4096^m, m = 0..4095
+    static constexpr size_t TWB = sizeof(float2) * NT;   // per-thread twiddle W256^(-q)
     static constexpr int MAX_ITEMS = 2048;              // a block's item list (group << 16 | orientation)
     static constexpr size_t LIST = sizeof(int) * MAX_ITEMS;
     static constexpr size_t SMEM = EXCH + ABUFS * ASZ + TWB + LIST + 64;
-    static constexpr uint32_t TMEM_COLS = 256;          // 8 warps per lane quadrant x 32 columns
+    // 8 warps per lane quadrant x 32 columns of I' (columns 0-255), and x 32 columns of
+    // the thread's twiddles W4096^(-(q + 16 r) s) (columns 256-511)
+    static constexpr uint32_t TMEM_COLS = 512;
     static_assert(SMEM <= 232448, "pass B block exceeds shared memory");
 };
 
@@ -746,7 +748,7 @@ k_pass_b_rg(BatchArgs a, int ngroups) {
     extern __shared__ __align__(16) unsigned char smem_b[];
     float2* const blk = reinterpret_cast<float2*>(smem_b);
     float2* const abuf = reinterpret_cast<float2*>(smem_b + PB::EXCH);
-    float2* const tws = reinterpret_cast<float2*>(smem_b + PB::EXCH + PB::ABUFS * PB::ASZ);
+    float2* const twt = reinterpret_cast<float2*>(smem_b + PB::EXCH + PB::ABUFS * PB::ASZ);
     int* const items = reinterpret_cast<int*>(smem_b + PB::EXCH + PB::ABUFS * PB::ASZ + PB::TWB);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem_b + PB::EXCH + PB::ABUFS * PB::ASZ + PB::TWB + PB::LIST);
     const int tid = threadIdx.x;
@@ -776,9 +778,8 @@ k_pass_b_rg(BatchArgs a, int ngroups) {
                      "l"(Asrc + (size_t)oo * T * a.XP + grp * 4)
                      : "memory");
     };
-    // twiddle table in shared memory: tw(m) = W4096^(-m)
-    for (int m = tid; m < Y; m += PB::NT) tws[m] = __ldg(a.twy.tab + m);
-    auto tw = [tws](int m) { return tws[m & (Y - 1)]; };
+    // this thread's W256^(-q) in shared memory, indexed by thread (conflict-free reads)
+    twt[tid] = a.twy.template w<-1>(16 * (tid & 15), Y);
     __syncthreads();   // the item list
     issue_rows(items[0] >> 16, items[0] & 0xffff, 0);
     tmptx::cp_async_commit();
@@ -789,6 +790,22 @@ k_pass_b_rg(BatchArgs a, int ngroups) {
     __syncthreads();
     tmptx::tmem_fence_after_sync();
     const uint32_t tmem = *tmem_slot + ((uint32_t)(32 * ((tid >> 5) & 3)) << 16) + (uint32_t)(32 * (tid >> 7));
+    const uint32_t tmw = tmem + 256;   // the twiddles W4096^(-(q + 16 r) s) of the residue phases
+    {
+        const int s = tid >> 6, q = tid & 15;
+#pragma unroll 1
+        for (int h = 0; h < 2; h++) {
+            float wb[16];
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                const float2 w = a.twy.template w<-1>((q + 16 * (8 * h + r)) * s, Y);
+                wb[2 * r] = w.x;
+                wb[2 * r + 1] = w.y;
+            }
+            tmptx::tmem_st16(tmw + 16 * h, wb);
+        }
+        tmptx::tmem_wait_st();
+    }
     int cur_group = -1;
     int buf = 0;
 #pragma unroll 1
@@ -826,16 +843,17 @@ k_pass_b_rg(BatchArgs a, int ngroups) {
         // forward: b[n] = a[n] W4096^(-n s) for n = q + 16 r, 16-point DFT over r (-> k1)
         {
             const float2* ac = abuf + buf * (PB::W * AP) + c * AP + q;
-            const float2 w1 = tw(16 * s);
-            float2 w = tw(s * q);
+            float wb[16];
 #pragma unroll
-            for (int r = 0; r < 16; r++) {
-                v[r] = cmul(ac[16 * r], w);
-                w = cmul(w, w1);
+            for (int h = 0; h < 2; h++) {
+                tmptx::tmem_ld16(tmw + 16 * h, wb);
+                tmptx::tmem_wait_ld16(wb);
+#pragma unroll
+                for (int r = 0; r < 8; r++) v[8 * h + r] = cmul(ac[16 * (8 * h + r)], make_float2(wb[2 * r], wb[2 * r + 1]));
             }
         }
         tmfft::dft16<-1>(v);
-        tmfft::apply_twiddles<16>(v, tw(16 * q));                       // W256^(-q k1)
+        tmfft::apply_twiddles<16>(v, twt[tid]);                         // W256^(-q k1)
         __syncwarp();   // the warp's final-phase reads of the previous item are done
 #pragma unroll
         for (int r = 0; r < 16; r++) TM_RG_ROW(q)[r] = v[r];           // row n1 = q, column k1 = r
@@ -859,7 +877,7 @@ k_pass_b_rg(BatchArgs a, int ngroups) {
         // inverse, residue part: 16-point DFT over k2 (-> m1), W256^(m1 q), transpose,
         // 16-point DFT over k1 (-> m2), then W4096^(s (m1 + 16 m2))
         tmfft::dft16<+1>(v);
-        tmfft::apply_twiddles<16>(v, tmfft::conjf2(tw(16 * q)));
+        tmfft::apply_twiddles<16>(v, tmfft::conjf2(twt[tid]));
 #pragma unroll
         for (int r = 0; r < 16; r++) TM_RG_ROW(q)[r] = v[r];           // row k1 = q, column m1 = r
         __syncwarp();
@@ -868,12 +886,13 @@ k_pass_b_rg(BatchArgs a, int ngroups) {
 #undef TM_RG_ROW
         tmfft::dft16<+1>(v);                                           // -> m2
         {
-            const float2 w1 = tmfft::conjf2(tw(16 * s));
-            float2 w = tmfft::conjf2(tw(s * q));
+            float wb[16];
 #pragma unroll
-            for (int r = 0; r < 16; r++) {
-                v[r] = cmul(v[r], w);
-                w = cmul(w, w1);
+            for (int h = 0; h < 2; h++) {
+                tmptx::tmem_ld16(tmw + 16 * h, wb);
+                tmptx::tmem_wait_ld16(wb);
+#pragma unroll
+                for (int r = 0; r < 8; r++) v[8 * h + r] = cmul_conj(v[8 * h + r], make_float2(wb[2 * r], wb[2 * r + 1]));
             }
         }
         // every warp is done with its transposes (which overlap other warps' final ranges)
@@ -914,10 +933,11 @@ k_pass_b_rg(BatchArgs a, int ngroups) {
 // k_pass_c: one block per row y; X/16 threads each own 16 pixels
 // (x = 2*(t + P*r) + h); loops over the batch keeping the per-pixel state in
 // registers.  The per-pixel sum and sum of squares are compensated (Kahan)
-// FP32 sums over the batch, added to the FP64 running sums once per batch; at
-// X = 4096 (256 threads, two blocks per SM, 128 registers) a thread parks the
-// compensation terms of both sums and its sums of squares in its TMEM lane
-// between orientations (columns 0-15, 16-31 and 32-47 of its 64).
+// FP32 sums over the batch, added to the FP64 running sums once per batch.  At
+// X = 4096 (256 threads, two blocks per SM, 128 registers) a thread keeps plain
+// FP32 partial sums over at most 8 orientations in registers and adds them
+// (Kahan) into compensated sums parked in its TMEM lane (columns 0-63 of its
+// 128), beside its twiddle multipliers (columns 64-127).
 // Copies of a block's shared-memory histogram: lane l counts into copy
 // l % n, bin b of copy c at word b * n + c, so that lanes of one warp whose
 // values fall in the same bin (the bins near zero take most of them) rarely
@@ -1040,11 +1060,15 @@ k_pass_c(BatchArgs a, int Y) {
     float mip[16];
     int best[16];
     // per-pixel sum and sum of squares over the batch: compensated (Kahan) FP32,
-    // added to the FP64 running sums once per batch.  comp_regs[0..15] and
-    // comp_regs[16..31] are the compensation terms of the two sums (registers
-    // only when they are not parked in TMEM, as is fq_regs).
+    // added to the FP64 running sums once per batch.  Without TMEM: fs, fq_regs
+    // and the compensation terms comp_regs[0..15] / [16..31] in registers, updated
+    // per orientation.  With TMEM (X = 4096): fs and pq are plain FP32 partial sums
+    // over at most 8 orientations, added every 8 orientations (Kahan) into the
+    // compensated sums held in TMEM columns 0-15 (sum), 16-31 (its compensation),
+    // 32-47 (sum of squares), 48-63 (its compensation).
     float fs[16];
     float fq_regs[kTm ? 1 : 16];
+    float pq[kTm ? 16 : 1];
     const size_t rowoff = (size_t)y * X;
 #pragma unroll
     for (int r = 0; r < 8; r++) {
@@ -1054,6 +1078,7 @@ k_pass_c(BatchArgs a, int Y) {
         mip[2 * r] = mv.x; mip[2 * r + 1] = mv.y;
         best[2 * r] = bv.x; best[2 * r + 1] = bv.y;
         fs[2 * r] = 0.f; fs[2 * r + 1] = 0.f;
+        if constexpr (kTm) { pq[2 * r] = 0.f; pq[2 * r + 1] = 0.f; }
     }
     // the compensation terms: in registers, or parked in TMEM between orientations
     float comp_regs[kTm ? 1 : 32];
@@ -1064,14 +1089,16 @@ k_pass_c(BatchArgs a, int Y) {
         tmptx::tmem_st16(tcomp, z);
         tmptx::tmem_st16(tcomp + 16, z);
         tmptx::tmem_st16(tcomp + 32, z);
-        // the packing's multipliers W_X^k, k = t + P r, and the transform's stage multipliers
+        tmptx::tmem_st16(tcomp + 48, z);
+        // the packing's multipliers W_X^k, k = t + P r (columns 112-127), and the
+        // transform's stage multipliers (64-111)
 #pragma unroll
         for (int r = 0; r < 8; r++) {
             const float2 w = a.tw.template w<+1>(t + P * r, X);
             z[2 * r] = w.x;
             z[2 * r + 1] = w.y;
         }
-        tmptx::tmem_st16(tcomp + 48, z);
+        tmptx::tmem_st16(tcomp + 112, z);
         PassCStageTw<H>::fill(tcomp + 64, t, a.tw);
         tmptx::tmem_wait_st();
     } else {
@@ -1102,7 +1129,7 @@ k_pass_c(BatchArgs a, int Y) {
             tmptx::bulk_g2s(rows + (buf ^ 1) * XP, a.C + ((size_t)(o + 1) * Y + y) * XP, row_bytes, &mbar[buf ^ 1]);
         }
         float pk[kTm ? 16 : 1];   // the packing's multipliers, from TMEM
-        if constexpr (kTm) tmptx::tmem_ld16(tcomp + 48, pk);
+        if constexpr (kTm) tmptx::tmem_ld16(tcomp + 112, pk);
         if (!tmptx::mbar_wait_bounded(&mbar[buf], (o >> 1) & 1, kWaitLimit)) {
             timed_out = true;
             atomicExch(a.err, 1);
@@ -1129,64 +1156,94 @@ k_pass_c(BatchArgs a, int Y) {
             tmfft::fft<H, 8, +1, false>(v, t, fbuf, a.tw, sync);
         }
         const int g = (int)(a.gidx0 + o);
-        // epilogue in two sweeps over the 16 values, so that only one sum's 16
-        // compensation terms are live at a time: (1) MIP / argmax, histogram and
-        // the sum, (2) the sum of squares
-        float comp_tm[kTm ? 32 : 1];
-#pragma unroll
-        for (int sweep = 0; sweep < 2; sweep++) {
-            float* comp = comp_regs + (kTm ? 0 : 16 * sweep);
-            float* fq = fq_regs;
-            if constexpr (kTm) {
-                // sweep 0: the sum's compensation; sweep 1: the sum of squares and its compensation
-                tmptx::tmem_ld16(tcomp + 16 * sweep, comp_tm);
-                if (sweep == 1) tmptx::tmem_ld16(tcomp + 32, comp_tm + 16);
-                tmptx::tmem_wait_ld32(comp_tm);
-                comp = comp_tm;
-                fq = comp_tm + 16;
-            }
+        if constexpr (kTm) {
+            // MIP / argmax, histogram and the plain partial sums of this orientation
 #pragma unroll
             for (int r = 0; r < 8; r++) {
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
                     const float val = h ? v[r].y : v[r].x;
                     const int pi = 2 * r + h;
-                    // Kahan: the compensation holds what the last addition added beyond its input
-                    if (sweep == 0) {
-                        if (val > mip[pi]) { mip[pi] = val; best[pi] = g; }
-                        const float ys = val - comp[pi];
-                        const float ts = fs[pi] + ys;
-                        comp[pi] = (ts - fs[pi]) - ys;
-                        fs[pi] = ts;
-                        const int bin = __float2int_rz(fmaf(val, a.hist_inv_step, hoff));
-                        if ((unsigned)bin < (unsigned)a.hist_bins) atomicAdd(&shist[bin * hcopies + hcopy], 1u);
-                    } else {
-                        const float yq = fmaf(val, val, -comp[pi]);
-                        const float tq = fq[pi] + yq;
-                        comp[pi] = (tq - fq[pi]) - yq;
-                        fq[pi] = tq;
+                    if (val > mip[pi]) { mip[pi] = val; best[pi] = g; }
+                    fs[pi] += val;
+                    pq[pi] = fmaf(val, val, pq[pi]);
+                    const int bin = __float2int_rz(fmaf(val, a.hist_inv_step, hoff));
+                    if ((unsigned)bin < (unsigned)a.hist_bins) atomicAdd(&shist[bin * hcopies + hcopy], 1u);
+                }
+            }
+            if ((o & 7) == 7 || o == a.nb - 1) {
+                // Kahan: the compensation holds what the last addition added beyond its input
+#pragma unroll
+                for (int sweep = 0; sweep < 4; sweep++) {   // 8 pixels of one sum at a time
+                    float* part = ((sweep >> 1) ? pq : fs) + 8 * (sweep & 1);
+                    const uint32_t col = tcomp + 32 * (sweep >> 1) + 8 * (sweep & 1);
+                    float sm[8], cm[8];   // sum, compensation
+                    tmptx::tmem_ld8(col, sm);
+                    tmptx::tmem_ld8(col + 16, cm);
+                    tmptx::tmem_wait_ld8x2(sm, cm);
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const float yv = part[i] - cm[i];
+                        const float tv = sm[i] + yv;
+                        cm[i] = (tv - sm[i]) - yv;
+                        sm[i] = tv;
+                        part[i] = 0.f;
+                    }
+                    tmptx::tmem_st8(col, sm);
+                    tmptx::tmem_st8(col + 16, cm);
+                }
+                tmptx::tmem_wait_st();
+            }
+        } else {
+            // epilogue in two sweeps over the 16 values, so that only one sum's 16
+            // compensation terms are live at a time: (1) MIP / argmax, histogram and
+            // the sum, (2) the sum of squares
+#pragma unroll
+            for (int sweep = 0; sweep < 2; sweep++) {
+                float* comp = comp_regs + 16 * sweep;
+#pragma unroll
+                for (int r = 0; r < 8; r++) {
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const float val = h ? v[r].y : v[r].x;
+                        const int pi = 2 * r + h;
+                        // Kahan: the compensation holds what the last addition added beyond its input
+                        if (sweep == 0) {
+                            if (val > mip[pi]) { mip[pi] = val; best[pi] = g; }
+                            const float ys = val - comp[pi];
+                            const float ts = fs[pi] + ys;
+                            comp[pi] = (ts - fs[pi]) - ys;
+                            fs[pi] = ts;
+                            const int bin = __float2int_rz(fmaf(val, a.hist_inv_step, hoff));
+                            if ((unsigned)bin < (unsigned)a.hist_bins) atomicAdd(&shist[bin * hcopies + hcopy], 1u);
+                        } else {
+                            const float yq = fmaf(val, val, -comp[pi]);
+                            const float tq = fq_regs[pi] + yq;
+                            comp[pi] = (tq - fq_regs[pi]) - yq;
+                            fq_regs[pi] = tq;
+                        }
                     }
                 }
             }
-            if constexpr (kTm) {
-                tmptx::tmem_st16(tcomp + 16 * sweep, comp_tm);
-                if (sweep == 1) tmptx::tmem_st16(tcomp + 32, comp_tm + 16);
-                tmptx::tmem_wait_st();
-            }
         }
     }
-    // the compensation terms (and sums of squares) for the FP64 flush
-    float comp_end[kTm ? 48 : 1];
+    // the sums and their compensation terms for the FP64 flush
+    float send[kTm ? 64 : 1];
+    const float* fsend = fs;
     const float* cend = comp_regs;
     const float* fqend = fq_regs;
+    const float* cqend = comp_regs + (kTm ? 0 : 16);
     if constexpr (kTm) {
-        tmptx::tmem_ld16(tcomp, comp_end);
-        tmptx::tmem_ld16(tcomp + 16, comp_end + 16);
-        tmptx::tmem_wait_ld32(comp_end);
-        tmptx::tmem_ld16(tcomp + 32, comp_end + 32);
-        tmptx::tmem_wait_ld16(comp_end + 32);
-        cend = comp_end;
-        fqend = comp_end + 32;
+        tmptx::tmem_ld16(tcomp, send);
+        tmptx::tmem_ld16(tcomp + 16, send + 16);
+        tmptx::tmem_wait_ld32(send);
+        tmptx::tmem_ld16(tcomp + 32, send + 32);
+        tmptx::tmem_ld16(tcomp + 48, send + 48);
+        tmptx::tmem_wait_ld32(send + 32);
+        fsend = send;
+        cend = send + 16;
+        fqend = send + 32;
+        cqend = send + 48;
         tmptx::tmem_fence_before_sync();
     }
     const bool failed = __syncthreads_or(timed_out);
@@ -1207,10 +1264,10 @@ k_pass_c(BatchArgs a, int Y) {
         *reinterpret_cast<int2*>(a.best + rowoff + x) = make_int2(best[2 * r], best[2 * r + 1]);
         double2 sv = *reinterpret_cast<const double2*>(a.sum + rowoff + x);
         double2 qv = *reinterpret_cast<const double2*>(a.sumsq + rowoff + x);
-        sv.x += (double)fs[2 * r] - (double)cend[2 * r];
-        sv.y += (double)fs[2 * r + 1] - (double)cend[2 * r + 1];
-        qv.x += (double)fqend[2 * r] - (double)cend[16 + 2 * r];
-        qv.y += (double)fqend[2 * r + 1] - (double)cend[16 + 2 * r + 1];
+        sv.x += (double)fsend[2 * r] - (double)cend[2 * r];
+        sv.y += (double)fsend[2 * r + 1] - (double)cend[2 * r + 1];
+        qv.x += (double)fqend[2 * r] - (double)cqend[2 * r];
+        qv.y += (double)fqend[2 * r + 1] - (double)cqend[2 * r + 1];
         *reinterpret_cast<double2*>(a.sum + rowoff + x) = sv;
         *reinterpret_cast<double2*>(a.sumsq + rowoff + x) = qv;
     }

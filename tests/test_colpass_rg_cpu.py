@@ -146,8 +146,9 @@ def test_shared_memory_ranges_and_banks():
 def test_shared_memory_budget():
     exch = 8 * 4 * CS
     staging = 8 * 4 * AP
-    twiddles = 8 * Y
-    assert exch + 3 * staging + twiddles + 64 <= 232448
+    twiddles = 8 * NT
+    item_list = 4 * 2048
+    assert exch + 3 * staging + twiddles + item_list + 64 <= 232448
     assert CS % 16 == 4 and RS % 2 == 1
 
 
