@@ -363,6 +363,9 @@ def _e2e_leg(sc, inp, args, world, local, chunk, precision):
     L = sc.L
     ptr = core._ptr
     n_ctx = max(1, min(args.e2e_contexts, args.steps))
+    # every host thread runs the same number of steps (the step count rounded up to a
+    # multiple of the threads), so that no thread's last step runs without overlap
+    n_steps = -(-args.steps // n_ctx) * n_ctx
     ctxs = [sc] + [core.SearchCore(X, Y, T, histogram_min_scaled=inp["hmin"], histogram_step_scaled=inp["hstep"],
                                    orientation_batch=sc.orientation_batch(), device=local) for _ in range(n_ctx - 1)]
     for c in ctxs[1:]:
@@ -379,7 +382,7 @@ def _e2e_leg(sc, inp, args, world, local, chunk, precision):
     def e2e_worker(k):
         try:
             c, outs = ctxs[k], bufs[k]
-            for i in range(k, args.steps, n_ctx):
+            for i in range(k, n_steps, n_ctx):
                 ang = chunk(args.warmup + i)
                 c._check(L.tm_set_image(c.h, ptr(ispec_h), X, Y))
                 c._check(L.tm_set_template(c.h, ptr(tspec_h), T))

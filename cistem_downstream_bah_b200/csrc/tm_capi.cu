@@ -446,6 +446,13 @@ const Variant kVariants[] = {
     TM_VARIANT_TC(64, 4096, 3888),
     TM_VARIANT(64, 4096, 5832),
     TM_VARIANT_TC(384, 4096, 3888),
+    // binned camera formats: K3 at 2x (2880 x 2046 -> 2048 x 2916 rotated), K2 at 2x
+    // (1919 x 1855 -> 2048 x 1944), 2560 x 1920 (-> 2048 x 2592), 5120 x 3840 (-> 4096 x 5184)
+    TM_VARIANT(256, 2048, 2916),
+    TM_VARIANT(128, 2048, 2916),
+    TM_VARIANT(256, 2048, 1944),
+    TM_VARIANT(256, 2048, 2592),
+    TM_VARIANT(256, 4096, 5184),
     // windows of the learned proposal's fine search (edge max(2T, 256))
     TM_VARIANT(64, 256, 256),
     TM_VARIANT(128, 256, 256),

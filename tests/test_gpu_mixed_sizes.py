@@ -42,7 +42,8 @@ def test_small_geometry_search_parity(geom):
 
 
 @pytest.mark.parametrize("geom", [(256, 4096, 3888), (256, 4096, 5832), (384, 4096, 5832), (384, 4096, 4096),
-                                  (256, 4096, 4096), (64, 4096, 4096)])
+                                  (256, 4096, 4096), (64, 4096, 4096), (256, 2048, 2916), (128, 2048, 2916),
+                                  (256, 2048, 1944), (256, 2048, 2592), (256, 4096, 5184)])
 def test_full_size_geometry_correlation_maps(geom):
     T, X, Y = geom
     case = make_case(T=T, X=X, Y=Y, pixel_size=1.0, n_particles=4, n_orient=40)
