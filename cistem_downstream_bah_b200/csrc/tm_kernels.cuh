@@ -674,7 +674,7 @@ k_pass_b(BatchArgs a, int ngroups) {
             } else if constexpr (G == 1) {
                 float2* Co = a.C + (size_t)o * Y * XP + kx0 + col;
 #pragma unroll
-                for (int r = 0; r < V; r++) Co[(size_t)(j + P * r) * XP] = v[r];
+                for (int r = 0; r < V; r++) __stcs(Co + (size_t)(j + P * r) * XP, v[r]);   // streaming
             } else {
                 sync();   // every thread has read its last-stage inputs from colbuf
 #pragma unroll
@@ -687,7 +687,7 @@ k_pass_b(BatchArgs a, int ngroups) {
             float2* Co = a.C + (size_t)o * Y * XP + kx0;
             for (int e = tid; e < Y * WG; e += NT) {
                 const int row = e / WG, cc = e % WG;
-                Co[(size_t)row * XP + cc] = exch[cc * PB::CS + tmfft::pad16(row)];
+                __stcs(Co + (size_t)row * XP + cc, exch[cc * PB::CS + tmfft::pad16(row)]);   // streaming
             }
         }
     }
@@ -912,11 +912,13 @@ k_pass_b_rg(BatchArgs a, int ngroups) {
         }
         tmfft::dft16<+1>(v);                                           // -> M
         {
+            // streaming stores (evict first): pass C reads the intermediate only after the
+            // whole launch, far more than L2 holds (4.17 -> 4.02 ms per 128 orientations)
             float2* Co = a.C + ((size_t)o * Y + (tid >> 2)) * a.XP + group * 4 + (tid & 3);
             const size_t rstep = (size_t)256 * a.XP;
 #pragma unroll
             for (int r = 0; r < 16; r++) {
-                *Co = v[r];
+                __stcs(Co, v[r]);
                 Co += rstep;
             }
         }
