@@ -69,6 +69,10 @@ WORKLOADS = {
     "stress384": dict(name="5760x4092 micrograph (padded 5832x4096, rotated), 384^3 template @0.8 A/px, C1 2.5/1.5 deg grid",
                       nx=5760, ny=4092, T=384, pixel_size=0.8, n_atoms=250000, radius_A=150.0, particles=40,
                       snr=0.03, defocus=12000.0, angular_step=2.5, psi_step=1.5),
+    # a binned camera format: K3 at 2x (2880 x 2046, padded 2916 x 2048 and rotated)
+    "binned2880": dict(name="2880x2046 micrograph (padded 2916x2048, rotated), 256^3 template @1.0 A/px, C1 3.0/2.0 deg grid",
+                       nx=2880, ny=2046, T=256, pixel_size=1.0, n_atoms=120000, radius_A=110.0, particles=30,
+                       snr=0.03, defocus=12000.0, angular_step=3.0, psi_step=2.0),
     # a size without compiled kernels (2700 = 2^2 3^3 5^2, kept by the factorisation): the
     # run-time-length kernels
     "generic2700": dict(name="2700x2700 micrograph (run-time-length kernels), 256^3 template @1.0 A/px, C1 3.0/2.0 deg grid",

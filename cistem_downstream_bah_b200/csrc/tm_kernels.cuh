@@ -936,7 +936,7 @@ k_pass_b_rg(BatchArgs a, int ngroups) {
 // (x = 2*(t + P*r) + h); loops over the batch keeping the per-pixel state in
 // registers.  The per-pixel sum and sum of squares are compensated (Kahan)
 // FP32 sums over the batch, added to the FP64 running sums once per batch.  At
-// X = 4096 (256 threads, two blocks per SM, 128 registers) a thread keeps plain
+// X = 4096 and 2048 (128 registers, two or four blocks per SM) a thread keeps plain
 // FP32 partial sums over at most 8 orientations in registers and adds them
 // (Kahan) into compensated sums parked in its TMEM lane (columns 0-63 of its
 // 128), beside its twiddle multipliers (columns 64-127).
@@ -957,7 +957,11 @@ struct PassC {
     static constexpr int R = 8;
     static constexpr int P = H / R;                 // X/16 threads
     static constexpr int RSF = tmfft::padded_len(H);
-    static constexpr bool COMP_IN_TMEM = X >= 4096 && P % 32 == 0;
+    // X = 4096 (256 threads, two blocks per SM) and X = 2048 (128 threads, four
+    // blocks per SM): every block's warps cover the four TMEM lane quadrants, and
+    // the blocks of an SM together take its 512 columns
+    static constexpr bool COMP_IN_TMEM = (X == 4096 || X == 2048) && P % 32 == 0;
+    static constexpr int MIN_BLOCKS = X == 2048 ? 4 : 2;
     // with the compensation terms in TMEM, a thread also keeps its twiddle
     // multipliers there (the c2r packing's 8 and the transform's stages 1-3):
     // 128 columns per warp, columns 0-47 sums, 48-63 packing, 64 + 16 (s - 1) stage s
@@ -1016,7 +1020,7 @@ struct PassCStageTw {
 };
 
 template <int X>
-__global__ void __launch_bounds__(X / 16, 2)
+__global__ void __launch_bounds__(X / 16, PassC<X>::MIN_BLOCKS)
 k_pass_c(BatchArgs a, int Y) {
     using PC = PassC<X>;
     constexpr int H = PC::H, P = PC::P;

@@ -55,3 +55,13 @@ def test_full_size_geometry_correlation_maps(geom):
             ref = O.correlate_one(case["tspec"], case["ispec"], case["filt"], case["angles"], o, X, Y)
             err = np.abs(got - ref).max() / np.abs(ref).max()
             assert err < 2e-5, (geom, o, err)
+
+
+@pytest.mark.parametrize("geom", [(128, 2048, 2048), (128, 2048, 2916)])
+def test_2048_wide_search_parity(geom):
+    """Whole-search parity (MIP, angles, sums, histogram) on 2048-wide micrographs, whose
+    row pass keeps its twiddles and compensated sums in tensor memory as at 4096,
+    over more orientations than one launch holds (ragged last batch)."""
+    T, X, Y = geom
+    case = make_case(T=T, X=X, Y=Y, angular_step=30.0, psi_step=30.0, n_orient=40)
+    _compare_search(case, batch=16)
