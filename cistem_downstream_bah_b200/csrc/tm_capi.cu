@@ -340,13 +340,18 @@ struct GenImpl {
     static int configure(tm_ctx* c) {
         TM_CUDA(c, cudaFuncSetAttribute(tmk::k_pass_a_gen<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)sizeof(float2) * 2 * c->X));
-        TM_CUDA(c, cudaFuncSetAttribute(tmk::k_pass_b_gen, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)sizeof(float2) * 2 * c->Y));
-        TM_CUDA(c, cudaFuncSetAttribute(tmk::k_pass_c_gen<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)sizeof(float2) * 2 * c->X + 4 * c->d.histogram_bins));
-        TM_CUDA(c, cudaFuncSetAttribute(tmk::k_pass_c_gen<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)sizeof(float2) * c->X + 4 * c->d.histogram_bins));
+        const int lw = tmk::gen_pass_b_lines(c->Y);
+        TM_CUDA(c, cudaFuncSetAttribute(lw == 4 ? tmk::k_pass_b_gen<4> : lw == 2 ? tmk::k_pass_b_gen<2> : tmk::k_pass_b_gen<1>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(float2) * 2 * lw * c->Y));
+        const int smem_c = (int)sizeof(float2) * (c->X % 2 ? 2 * c->X : c->X) + 4 * c->d.histogram_bins;
+        TM_CUDA(c, cudaFuncSetAttribute(pass_c_kernel(c->X), cudaFuncAttributeMaxDynamicSharedMemorySize, smem_c));
         return TM_OK;
+    }
+    // the row pass for a width X: odd or even rows, 4, 8 or 16 pixels per thread
+    static auto pass_c_kernel(int X) -> void (*)(tmk::BatchArgs, int, int, tmk::GenPlan) {
+        const int mp = X <= 4 * tmk::kGenNT ? 4 : X <= 8 * tmk::kGenNT ? 8 : 16;
+        if (X % 2) return mp == 4 ? tmk::k_pass_c_gen<true, 4> : mp == 8 ? tmk::k_pass_c_gen<true, 8> : tmk::k_pass_c_gen<true, 16>;
+        return mp == 4 ? tmk::k_pass_c_gen<false, 4> : mp == 8 ? tmk::k_pass_c_gen<false, 8> : tmk::k_pass_c_gen<false, 16>;
     }
     static void prep(tm_ctx* c, tmk::BatchArgs& a, cudaStream_t s) {
         using SC = tmk::SliceCol<T>;
@@ -357,15 +362,16 @@ struct GenImpl {
         tmk::k_pass_a_gen<T><<<dim3(T, a.nb), tmk::kGenNT, sizeof(float2) * 2 * c->X, s>>>(a, c->X, c->gen_px);
     }
     static void pass_b(tm_ctx* c, tmk::BatchArgs& a, cudaStream_t s) {
-        tmk::k_pass_b_gen<<<dim3(a.XP, a.nb), tmk::kGenNT, sizeof(float2) * 2 * c->Y, s>>>(a, T, c->Y, c->gen_py);
+        // the row pitch XP is a multiple of 4 columns (the variant's pass-B width)
+        const int lw = tmk::gen_pass_b_lines(c->Y);
+        const size_t smem = sizeof(float2) * 2 * lw * c->Y;
+        if (lw == 4) tmk::k_pass_b_gen<4><<<dim3(a.XP / 4, a.nb), tmk::kGenNT, smem, s>>>(a, T, c->Y, c->gen_py);
+        else if (lw == 2) tmk::k_pass_b_gen<2><<<dim3(a.XP / 2, a.nb), tmk::kGenNT, smem, s>>>(a, T, c->Y, c->gen_py);
+        else tmk::k_pass_b_gen<1><<<dim3(a.XP, a.nb), tmk::kGenNT, smem, s>>>(a, T, c->Y, c->gen_py);
     }
     static void pass_c(tm_ctx* c, tmk::BatchArgs& a, cudaStream_t s) {
-        if (c->X % 2)
-            tmk::k_pass_c_gen<true><<<c->Y, tmk::kGenNT, sizeof(float2) * 2 * c->X + 4 * a.hist_bins, s>>>(a, c->X, c->Y,
-                                                                                                      c->gen_ph);
-        else
-            tmk::k_pass_c_gen<false><<<c->Y, tmk::kGenNT, sizeof(float2) * c->X + 4 * a.hist_bins, s>>>(a, c->X, c->Y,
-                                                                                                       c->gen_ph);
+        const size_t smem = sizeof(float2) * (c->X % 2 ? 2 * c->X : c->X) + 4 * a.hist_bins;
+        pass_c_kernel(c->X)<<<c->Y, tmk::kGenNT, smem, s>>>(a, c->X, c->Y, c->gen_ph);
     }
     static int done(tm_ctx* c) {
         cudaError_t e = cudaGetLastError();
@@ -467,7 +473,7 @@ const Variant* find_variant(int T, int X, int Y) {
 
 // the run-time-length variants, one per template box (X = Y = 0: any size with radix plans)
 #define TM_GENERIC(T)                                                                                  \
-    {T, 0, 0, 2, &GenImpl<T>::run_batch, &GenImpl<T>::configure, &GenImpl<T>::run_stages, &whiten_generic, \
+    {T, 0, 0, 4, &GenImpl<T>::run_batch, &GenImpl<T>::configure, &GenImpl<T>::run_stages, &whiten_generic, \
      &GenImpl<T>::run_batch_images, nullptr}
 const Variant kGenericVariants[] = {TM_GENERIC(32), TM_GENERIC(48), TM_GENERIC(64), TM_GENERIC(128), TM_GENERIC(256),
                                     TM_GENERIC(384)};

@@ -155,20 +155,40 @@ __global__ void __launch_bounds__(kGenNT) k_pass_a_gen(BatchArgs a, int X, GenPl
     for (int k = threadIdx.x; k <= X / 2; k += kGenNT) out[k] = f[k];
 }
 
-// k_pass_b_gen: block per (column, orientation).
+// k_pass_b_gen: block per (group of LW adjacent columns, orientation), the LW
+// columns transformed together (LW lines per Stockham stage, so that a stage
+// has LW times the butterflies for the block's threads) and written as whole
+// row segments (LW = 4: 32-byte sectors).  Streaming stores, as the compiled
+// column passes.
+template <int LW>
 __global__ void __launch_bounds__(kGenNT) k_pass_b_gen(BatchArgs a, int T, int Y, GenPlan py) {
-    extern __shared__ float2 gbuf[];   // 2 x Y
-    const int kx = blockIdx.x, o = blockIdx.y;
+    extern __shared__ float2 gbuf[];   // 2 x LW x Y, line c at c * Y
+    const int kx0 = blockIdx.x * LW, o = blockIdx.y;
     const int XP = a.XP;
-    const float2* Ao = a.A + (size_t)o * T * XP + kx;
-    for (int n = threadIdx.x; n < Y; n += kGenNT) gbuf[n] = n < T ? Ao[(size_t)n * XP] : make_float2(0.f, 0.f);
+    const float2* Ao = a.A + (size_t)o * T * XP + kx0;
+    for (int e = threadIdx.x; e < LW * Y; e += kGenNT) {
+        const int n = e / LW, c = e - n * LW;
+        gbuf[c * Y + n] = n < T ? Ao[(size_t)n * XP + c] : make_float2(0.f, 0.f);
+    }
     __syncthreads();
-    float2* f = fft_gen<-1>(gbuf, gbuf + Y, Y, 1, py, a.twy);
-    for (int k = threadIdx.x; k < Y; k += kGenNT) f[k] = cmul_conj(__ldg(a.Ip + (size_t)k * XP + kx), f[k]);
+    float2* f = fft_gen<-1>(gbuf, gbuf + LW * Y, Y, LW, py, a.twy);
+    for (int e = threadIdx.x; e < LW * Y; e += kGenNT) {
+        const int k = e / LW, c = e - k * LW;
+        f[c * Y + k] = cmul_conj(__ldg(a.Ip + (size_t)k * XP + kx0 + c), f[c * Y + k]);
+    }
     __syncthreads();
-    const float2* z = fft_gen<+1>(f, f == gbuf ? gbuf + Y : gbuf, Y, 1, py, a.twy);
-    float2* Co = a.C + (size_t)o * Y * XP + kx;
-    for (int yy = threadIdx.x; yy < Y; yy += kGenNT) Co[(size_t)yy * XP] = z[yy];
+    const float2* z = fft_gen<+1>(f, f == gbuf ? gbuf + LW * Y : gbuf, Y, LW, py, a.twy);
+    float2* Co = a.C + (size_t)o * Y * XP + kx0;
+    for (int e = threadIdx.x; e < LW * Y; e += kGenNT) {
+        const int yy = e / LW, c = e - yy * LW;
+        __stcs(Co + (size_t)yy * XP + c, z[c * Y + yy]);
+    }
+}
+// columns per block of k_pass_b_gen for a height Y (two buffers of LW x Y in shared memory)
+inline int gen_pass_b_lines(int Y) {
+    if (2 * 4 * (size_t)Y * sizeof(float2) <= 232448) return 4;
+    if (2 * 2 * (size_t)Y * sizeof(float2) <= 232448) return 2;
+    return 1;
 }
 
 // k_pass_c_gen: block per row y; thread t owns the pixels x = t + kGenNT j and
@@ -177,9 +197,12 @@ __global__ void __launch_bounds__(kGenNT) k_pass_b_gen(BatchArgs a, int T, int Y
 // outputs hold pixel pairs); an odd width (the reference's factorisation can
 // give one, e.g. 3^8) the full X-point inverse of the Hermitian extension,
 // the imaginary part of the DC term ignored as FFTW's c2r does.
-template <bool ODD>
-__global__ void __launch_bounds__(kGenNT, 1) k_pass_c_gen(BatchArgs a, int X, int Y, GenPlan ph) {
-    constexpr int MAXP = kGenMaxLen / kGenNT;   // pixels per thread
+// MAXP pixels per thread (kGenNT * MAXP >= X): 4, 8 or 16, the smaller the
+// fewer registers and the more blocks per SM.
+template <bool ODD, int MAXP>
+__global__ void __launch_bounds__(kGenNT, MAXP == 4 ? 3 : MAXP == 8 ? 2 : 1)
+k_pass_c_gen(BatchArgs a, int X, int Y, GenPlan ph) {
+    static_assert(kGenNT * 16 >= kGenMaxLen, "16 pixels per thread cover the longest rows");
     extern __shared__ float2 gbuf[];             // 2 x L (L = X/2 or X), then the histogram
     const int L = ODD ? X : X / 2, HC = X / 2 + 1, XP = a.XP, y = blockIdx.x, t = threadIdx.x;
     unsigned int* shist = reinterpret_cast<unsigned int*>(gbuf + 2 * L);

@@ -670,7 +670,10 @@ k_pass_b(BatchArgs a, int ngroups) {
                 __half2* Co = reinterpret_cast<__half2*>(a.C) + (size_t)o * Y * XP +
                               ((size_t)(j / RB) * XP + kx0 + col) * RB + (j % RB);
 #pragma unroll
-                for (int r = 0; r < V; r++) Co[(size_t)r * P * XP] = __floats2half2_rn(v[r].x * sc, v[r].y * sc);
+                for (int r = 0; r < V; r++) {   // streaming stores, as the FP32 output
+                    const __half2 hv = __floats2half2_rn(v[r].x * sc, v[r].y * sc);
+                    __stcs(reinterpret_cast<unsigned int*>(Co + (size_t)r * P * XP), *reinterpret_cast<const unsigned int*>(&hv));
+                }
             } else if constexpr (G == 1) {
                 float2* Co = a.C + (size_t)o * Y * XP + kx0 + col;
 #pragma unroll

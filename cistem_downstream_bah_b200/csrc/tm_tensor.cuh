@@ -829,7 +829,8 @@ k_pass_b_tc(BatchArgs a, int ngroups, const uint4* __restrict__ tabs) {
                     const int c = (e0 + e) / RB, r = (e0 + e) % RB;
                     w4[e] = ((c >> 1) ? st1 : st0)[(c & 1) * Y + rb * RB + r];
                 }
-                *reinterpret_cast<uint4*>(C16 + ((size_t)rb * XP + kx0) * RB + e0) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+                // streaming store: the row pass reads the intermediate only after the whole launch
+                __stcs(reinterpret_cast<uint4*>(C16 + ((size_t)rb * XP + kx0) * RB + e0), make_uint4(w4[0], w4[1], w4[2], w4[3]));
             }
         }
     }
