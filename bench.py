@@ -567,6 +567,16 @@ def run_ours(args):
     else:
         ach = alg_c / (c_launch_ms * 1e-3) / 1e9
         traffic = args.traffic_c if args.traffic_c is not None else (prof["k_pass_c"] if prof else None)
+    # both search passes against the same HBM peak (the row pass is bound by its FP32
+    # issue rather than by HBM, so its fraction is low at any speed)
+    by_kernel = {}
+    for name, alg, ms, tr in ((b_name, alg_b, b_launch_ms, args.traffic_b if args.traffic_b is not None else
+                               (prof["k_pass_b"] if prof else None)),
+                              ("k_pass_c", alg_c, c_launch_ms, args.traffic_c if args.traffic_c is not None else
+                               (prof["k_pass_c"] if prof else None))):
+        gbs = alg / (max(ms, 1e-9) * 1e-3) / 1e9
+        by_kernel[name] = {"achieved": gbs, "frac": gbs / hbm_peak, "ms_per_launch": ms,
+                           "algorithmic_bytes_per_launch": alg, "traffic": tr}
 
     # ---- the FP16 tensor-core form on the same workload and orientation chunks
     fp16 = None
@@ -660,7 +670,8 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
                          "frac": ach / hbm_peak, "traffic": traffic, "peak_source": peak_kind,
                          "ms_per_launch": {b_name: b_launch_ms, "k_pass_c": c_launch_ms,
-                                           "prep_kernels": dev["prep_ms"] / max(n_launch, 1)}},
+                                           "prep_kernels": dev["prep_ms"] / max(n_launch, 1)},
+                         "by_kernel": by_kernel},
             "clocks": dev["clocks"],
             "wall_ms_timed_region": dev["wall_ms"],
         }
